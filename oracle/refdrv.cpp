@@ -1,0 +1,140 @@
+// Oracle driver — TEST INFRASTRUCTURE ONLY.
+//
+// Runs the reference FastBit library (built from source by
+// oracle/Makefile.ref into oracle/_ref/) on requests read from a binary file
+// and writes the reference's answers to another binary file.  It is used to
+// make the golden fixtures under tests/golden/ and to pin the C restatement
+// in oracle/wah_oracle.c against the reference itself.
+//
+// Request stream (all little-endian uint32 unless stated):
+//   1 op inplace compress na a[na] nb b[nb]   -> ibis::bitvector a OP b
+//        (operator& | ^ - , bitvector.cpp:1292-1838, or the OP= forms),
+//        operands built with the array_t constructor (bitvector.cpp:54);
+//        reply: status cnt len words[len]   (serialized result, write(array_t&))
+//   2 na a[na]                                -> compress(); reply like 1
+//   3 na a[na]                                -> firstIndexSet walk (rids);
+//        reply: status n rids[n]
+//   4 nruns(u64) runs[nruns](u64)             -> appendFill-built bitvector
+//        (alternating 0/1 runs, 0 first); reply like 1
+//   5 nrows vals[nrows] nq (lo hi)(f64 x2)[nq] -> ibis::relic over the uint32
+//        column (construct(array_t), irelic.cpp:879) + evaluate of
+//        qContinuousRange(lo <= x < hi) (irelic.cpp:1827) for each query;
+//        reply: nkeys keys(f64)[nkeys] noffs offs(i64)[noffs] nbms bms[nbms]
+//               then per query: status count nrids rids[nrids]
+//   6 na a[na] -> decompress(); reply like 1
+//   7 na a[na] -> flip(); reply like 1
+#include "ibis.h"
+#include "irelic.h"
+#include "bitvector.h"
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+#include <stdint.h>
+
+static FILE *fin, *fout;
+static uint32_t rd32() { uint32_t v; if (fread(&v, 4, 1, fin) != 1) exit(3); return v; }
+static uint64_t rd64() { uint64_t v; if (fread(&v, 8, 1, fin) != 1) exit(3); return v; }
+static double rdf64() { double v; if (fread(&v, 8, 1, fin) != 1) exit(3); return v; }
+static void wr32(uint32_t v) { fwrite(&v, 4, 1, fout); }
+static void wrv(const std::vector<uint32_t>& v) { wr32((uint32_t)v.size()); if (!v.empty()) fwrite(&v[0], 4, v.size(), fout); }
+static std::vector<uint32_t> rdvec() {
+    uint32_t n = rd32(); std::vector<uint32_t> v(n);
+    if (n && fread(&v[0], 4, n, fin) != n) exit(3);
+    return v;
+}
+static ibis::bitvector* from_serial(const std::vector<uint32_t>& w) {
+    ibis::array_t<uint32_t> arr(w.size());
+    for (size_t i = 0; i < w.size(); ++i) arr[i] = w[i];
+    return new ibis::bitvector(arr);
+}
+static void reply_bv(int status, ibis::bitvector* r) {
+    wr32((uint32_t)status);
+    if (status != 0 || r == 0) { wr32(0); wr32(0); return; }
+    uint32_t cnt = r->cnt();
+    ibis::array_t<uint32_t> out;
+    r->write(out);
+    wr32(cnt);
+    std::vector<uint32_t> v(out.begin(), out.end());
+    wrv(v);
+}
+static void rids_of(const ibis::bitvector& bv, std::vector<uint32_t>& rids) {
+    for (ibis::bitvector::indexSet is = bv.firstIndexSet(); is.nIndices() > 0; ++is) {
+        const ibis::bitvector::word_t* ii = is.indices();
+        if (is.isRange()) { for (uint32_t j = ii[0]; j < ii[1]; ++j) rids.push_back(j); }
+        else { for (uint32_t j = 0; j < is.nIndices(); ++j) rids.push_back(ii[j]); }
+    }
+}
+
+int main(int argc, char** argv) {
+    if (argc != 3) { fprintf(stderr, "usage: refdrv in out\n"); return 2; }
+    ibis::init();
+    fin = fopen(argv[1], "rb"); fout = fopen(argv[2], "wb");
+    if (!fin || !fout) return 2;
+    uint32_t kind;
+    while (fread(&kind, 4, 1, fin) == 1) {
+        if (kind == 1) {
+            uint32_t op = rd32(), inplace = rd32(), comp = rd32();
+            std::vector<uint32_t> a = rdvec(), b = rdvec();
+            ibis::bitvector *A = from_serial(a), *B = from_serial(b), *R = 0;
+            int st = 0;
+            try {
+                if (inplace) {
+                    switch (op) { case 0: *A &= *B; break; case 1: *A |= *B; break;
+                                  case 2: *A ^= *B; break; default: *A -= *B; }
+                    R = A; A = 0;
+                } else {
+                    switch (op) { case 0: R = *A & *B; break; case 1: R = *A | *B; break;
+                                  case 2: R = *A ^ *B; break; default: R = *A - *B; }
+                }
+                if (comp) R->compress();
+            } catch (...) { st = 1; }
+            reply_bv(st, R);
+            delete A; delete B; delete R;
+        } else if (kind == 2 || kind == 6 || kind == 7) {
+            std::vector<uint32_t> a = rdvec();
+            ibis::bitvector* A = from_serial(a);
+            if (kind == 2) A->compress(); else if (kind == 6) A->decompress(); else A->flip();
+            reply_bv(0, A);
+            delete A;
+        } else if (kind == 3) {
+            std::vector<uint32_t> a = rdvec();
+            ibis::bitvector* A = from_serial(a);
+            std::vector<uint32_t> rids;
+            rids_of(*A, rids);
+            wr32(0); wrv(rids);
+            delete A;
+        } else if (kind == 4) {
+            uint64_t n = rd64();
+            ibis::bitvector A;
+            for (uint64_t i = 0; i < n; ++i) A.appendFill((int)(i & 1), (uint32_t)rd64());
+            reply_bv(0, &A);
+        } else if (kind == 5) {
+            uint32_t nrows = rd32();
+            ibis::array_t<uint32_t> vals(nrows);
+            for (uint32_t i = 0; i < nrows; ++i) vals[i] = rd32();
+            ibis::relic rel(0);
+            rel.construct(vals);
+            ibis::array_t<double> keys; ibis::array_t<int64_t> offs; ibis::array_t<uint32_t> bms;
+            rel.write(keys, offs, bms);
+            wr32((uint32_t)keys.size()); fwrite(keys.begin(), 8, keys.size(), fout);
+            wr32((uint32_t)offs.size()); fwrite(offs.begin(), 8, offs.size(), fout);
+            wr32((uint32_t)bms.size()); fwrite(bms.begin(), 4, bms.size(), fout);
+            uint32_t nq = rd32();
+            for (uint32_t q = 0; q < nq; ++q) {
+                double lo = rdf64(), hi = rdf64();
+                ibis::qContinuousRange expr(lo, ibis::qExpr::OP_LE, "x", ibis::qExpr::OP_LT, hi);
+                ibis::bitvector hits;
+                long c = rel.evaluate(expr, hits);
+                hits.compress();
+                std::vector<uint32_t> rids;
+                rids_of(hits, rids);
+                wr32(c < 0 ? 1u : 0u); wr32((uint32_t)c); wrv(rids);
+            }
+        } else {
+            fprintf(stderr, "refdrv: unknown request %u\n", kind);
+            return 4;
+        }
+    }
+    fclose(fout);
+    return 0;
+}

@@ -1,0 +1,437 @@
+"""Benchmark: WAH bitvector operators on B200 (raw-WAH workload).
+
+Workload (one step): for each set-bit density d in {1e-4, 1e-3, 1e-2, 0.1,
+0.5}, a pair of 2^28-bit bitvectors built from alternating geometric 0/1
+runs (appendFill form), and for each operator & | ^ - the result
+r = a OP b, compress()ed, with cnt() — 20 operator calls per step.  All
+operands together (~190 MB) exceed the 126 MB L2 and the step visits the
+pairs in turn, so each operand is evicted between its uses.
+
+Metric: WAH-op bandwidth in GB/s, counting 4 bytes per serialized word of
+both operands and of the result (the algorithmic bytes).  `value` is device
+time with operands resident in HBM; `e2e` goes through the C ABI with host
+buffers (pinned), each call uploading its operands and reading back the
+result words and cnt().
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With N > 1 (torchrun, one process per GPU) every rank processes its own
+independent pairs (weak scaling, no collective on the data path); the time is
+the maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DENSITIES = [1e-4, 1e-3, 1e-2, 0.1, 0.5]
+NBITS = 1 << 28
+OPS = [0, 1, 2, 3]
+OPNAMES = ["&", "|", "^", "-"]
+METRIC = "WAH-op HBM GB/s (raw WAH logic: & | ^ - + cnt on 2^28-bit pairs)"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def make_operands(rank: int, device: str):
+    from libfastlib_b200 import workloads as W
+    ops = []
+    for i, d in enumerate(DENSITIES):
+        a = W.raw_wah_operand(1000 * rank + 2 * i + 1, NBITS, d, device)
+        b = W.raw_wah_operand(1000 * rank + 2 * i + 2, NBITS, d, device)
+        ops.append((a, b))
+    return ops
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        try:
+            sm = [float(r[1]) for r in self.rows if len(r) >= 9]
+            if sm:
+                out["sm_mhz"] = statistics.median(sm)
+                out["sm_max_mhz"] = max(float(r[2]) for r in self.rows if len(r) >= 9)
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            reasons = set()
+            for r in self.rows:
+                for k, nm in enumerate(names):
+                    if len(r) >= 9 and r[5 + k].lower().startswith("active"):
+                        reasons.add(nm)
+            out["reasons"] = sorted(reasons)
+            out["samples"] = len(self.rows)
+        except Exception:
+            pass
+        return out
+
+
+def serial_bytes(words: int) -> int:
+    return 4 * words
+
+
+def cpu_reference(pairs, threads: int, reps: int):
+    """Times the reference library's own operators (oracle/_ref, built from
+    the reference sources) on `threads` host threads; returns (seconds,
+    per-op result lengths) or None when the reference build is absent."""
+    import struct
+    import tempfile
+    refdrv = os.path.join(ROOT, "oracle", "_ref", "refdrv")
+    if not os.path.exists(refdrv):
+        return None
+    reqs = [struct.pack("<IIII", 8, threads, reps, len(pairs) * len(OPS))]
+    for op in OPS:
+        for a, b in pairs:
+            reqs.append(struct.pack("<I", op) + struct.pack("<I", len(a)) + a.tobytes()
+                        + struct.pack("<I", len(b)) + b.tobytes())
+    with tempfile.TemporaryDirectory() as td:
+        fi, fo = os.path.join(td, "req.bin"), os.path.join(td, "rep.bin")
+        with open(fi, "wb") as f:
+            f.write(b"".join(reqs))
+        subprocess.run([refdrv, fi, fo], check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        data = open(fo, "rb").read()
+    secs = struct.unpack_from("<d", data, 0)[0]
+    lens = np.frombuffer(data, np.uint32, offset=8)
+    return secs, lens
+
+
+def cpu_port(pairs, reps: int):
+    """The oracle's C restatement, one thread (when the reference build is
+    absent)."""
+    import oracle
+    t0 = time.perf_counter()
+    lens = []
+    for _ in range(reps):
+        lens = []
+        for op in OPS:
+            for a, b in pairs:
+                w, _c = oracle.binop(op, a, b)
+                lens.append(len(w))
+    return time.perf_counter() - t0, np.array(lens)
+
+
+def algorithmic_bytes(pairs, res_lens):
+    tot = 0
+    k = 0
+    for op in OPS:
+        for a, b in pairs:
+            tot += 4 * (len(a) + len(b) + int(res_lens[k]))
+            k += 1
+    return tot
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    device = "cuda" if _cuda() else "cpu"
+    pairs = make_operands(0, device)
+    threads = os.cpu_count() or 1
+    threads = max(1, min(threads, len(pairs) * len(OPS)))
+    # one warm-up pass sizes the sample: K passes of the 20 operator calls,
+    # bounded to about a minute of host time
+    r = cpu_reference(pairs, threads, 1)
+    kind = "reference"
+    if r is None:
+        kind = "port"
+        threads = 1
+        t1, _l = cpu_port(pairs, 1)
+        passes = max(1, min(args.steps, int(60.0 / max(t1, 1e-3))))
+        secs, lens = cpu_port(pairs, passes)
+    else:
+        passes = max(1, min(args.steps, int(60.0 / max(r[0], 1e-3))))
+        secs, lens = cpu_reference(pairs, threads, passes)
+    args.steps = passes
+    nbytes = algorithmic_bytes(pairs, lens)
+    value = nbytes * passes / secs / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * secs / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic",
+        "config": _config(1),
+        "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": kind,
+                         "sample": f"{args.steps} passes of the 20 operator calls"},
+        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def _cuda():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def _config(n):
+    return {"workload": "raw WAH logic: pairs of 2^28-bit bitvectors (alternating geometric 0/1 runs, "
+                        "densities 1e-4..0.5), ops & | ^ - then compress() and cnt()",
+            "nbits": NBITS, "densities": DENSITIES, "ops_per_step": len(DENSITIES) * len(OPS),
+            "l2": "operands (~190 MB per rank) exceed L2; pairs visited in turn",
+            "parallelism": f"replicas x{n} (independent pairs per GPU)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--only", default=None,
+                    help="OP:DENSITY, e.g. '&:0.5' — one operator on one pair, no e2e / CPU legs (for ncu)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import libfastlib_b200 as L
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    pairs = make_operands(rank, f"cuda:{local}")
+    if args.only:
+        op_s, d_s = args.only.split(":")
+        keep = DENSITIES.index(float(d_s))
+        pairs = [pairs[keep]]
+        OPS[:] = [OPNAMES.index(op_s)]
+    ctx = L.Context(local)
+    # a dedicated stream: the legacy default stream (handle 0) cannot be
+    # handed to the library, which treats NULL as "its own stream"
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    dev = [(ctx.bitvector(a), ctx.bitvector(b)) for a, b in pairs]
+    for A, B in dev:
+        A.size(); B.size()
+    res = [{op: ctx.empty(len(a) + len(b)) for op in OPS} for a, b in pairs]
+
+    def step():
+        for op in OPS:
+            for i, (A, B) in enumerate(dev):
+                A.binop_into(op, B, res[i][op])
+
+    clk = ClockSampler(local)
+    if not args.only:
+        clk.start()
+        time.sleep(1.0)  # nvidia-smi needs a moment before its first sample
+    l_step0 = ctx.launches
+    step()
+    launches_per_step = ctx.launches - l_step0
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    res_lens = [res[i][op].nwords() + 1 + (1 if (NBITS % 31) else 0) for op in OPS for i in range(len(dev))]
+    nbytes = algorithmic_bytes(pairs, res_lens)
+
+    # the step as one CUDA graph (the library enqueues without host syncs once
+    # operand metadata is known and scratch is sized)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        step()
+    for _ in range(args.warmup):
+        graph.replay()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = ctx.launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        graph.replay()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    # kernels per step were counted while capturing; replays launch the same set
+    launches = (ctx.launches - l0) + args.steps * launches_per_step
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = world * nbytes * args.steps / (ms / 1e3) / 1e9
+    if args.only:
+        if rank == 0:
+            print(json.dumps({"only": args.only, "value": value, "unit": "GB/s", "ms_per_call": ms / args.steps,
+                              "bytes_per_call": nbytes}))
+        ctx.set_stream(None)
+        return
+
+    # per-call device time of each operator call (the merge kernel and its
+    # metadata memset): a graph of REPS back-to-back calls, timed by events
+    REPS = 10
+    call_ms = {}
+    tot_b = 0
+    tot_ms = 0.0
+    for op in OPS:
+        for i, (A, B) in enumerate(dev):
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=stream):
+                for _ in range(REPS):
+                    A.binop_into(op, B, res[i][op])
+            g.replay()
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            g.replay()
+            s1.record(stream)
+            torch.cuda.synchronize()
+            t = s0.elapsed_time(s1) / REPS
+            a, b = pairs[i]
+            byt = 4 * (len(a) + len(b) + res_lens[OPS.index(op) * len(dev) + i])
+            tot_b += byt
+            tot_ms += t
+            call_ms[f"{OPNAMES[op]} d={DENSITIES[i]:g}"] = {"ms": round(t, 5), "GBps": round(byt / t / 1e6, 1)}
+            del g
+    peak, peak_kind = peaks()
+    achieved = tot_b / (tot_ms / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "merge_traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get("bytes_per_launch_workload_avg")
+        except Exception:
+            traffic = None
+
+    # end to end through the C ABI with host (pinned) buffers
+    pinned = []
+    for a, b in pairs:
+        ta = torch.from_numpy(a).pin_memory()
+        tb = torch.from_numpy(b).pin_memory()
+        pinned.append((ta.numpy(), tb.numpy(), ta, tb))
+    outbufs = [torch.empty(len(a) + len(b) + 4, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+               for a, b in pairs]
+
+    def e2e_step():
+        h2d = d2h = 0
+        for op in OPS:
+            for i, (a, b, _ta, _tb) in enumerate(pinned):
+                A = ctx.bitvector(a)
+                B = ctx.bitvector(b)
+                R = A._binop(op, B, False)
+                n = ctx.check(ctx.lib.wahgpu_bv_write(R.h, outbufs[i].ctypes.data_as(
+                    __import__("ctypes").POINTER(__import__("ctypes").c_uint32)), len(outbufs[i])))
+                R.cnt()
+                h2d += 4 * (len(a) + len(b))
+                d2h += 4 * n
+                del A, B, R
+        return h2d, d2h
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record(stream)
+    for _ in range(args.e2e_steps):
+        h2d, d2h = e2e_step()
+    q1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max(q0.elapsed_time(q1), (time.perf_counter() - t0) * 1e3)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * nbytes * args.e2e_steps / (e2e_ms / 1e3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1:
+        host = [(a, b) for a, b in pairs]
+        threads = max(1, min(os.cpu_count() or 1, len(host) * len(OPS)))
+        r = cpu_reference(host, threads, 2)
+        if r is not None:
+            secs, lens = r
+            cpu = {"value": algorithmic_bytes(host, lens) * 2 / secs / 1e9, "unit": "GB/s",
+                   "cores": threads, "kind": "reference",
+                   "sample": "2 passes of the 20 operator calls (reference library, oracle/_ref)"}
+        else:
+            secs, lens = cpu_port(host, 1)
+            cpu = {"value": algorithmic_bytes(host, lens) / secs / 1e9, "unit": "GB/s", "cores": 1,
+                   "kind": "port", "sample": "1 pass of the 20 operator calls (C oracle)"}
+
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": _config(world),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "k_merge (+ its metadata memset), per-call CUDA events"},
+            "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": launches,
+            "detail_call_ms": call_ms,
+        }
+        print(json.dumps(line))
+    ctx.set_stream(None)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,131 @@
+/*
+ * libwahgpu — B200 (sm_100a) implementation of FastBit's WAH bitvector
+ * operators and relic/bin range evaluation, behind a C ABI.
+ *
+ * Every entry point returns an int (or int64_t) status: >= 0 on success,
+ * a negative WAHGPU_E* code on failure (the convention of the reference's
+ * in-memory C API, src/iapi.cpp:1383-1429).  The text of the last error of a
+ * context is available from wahgpu_last_error().  No C++ exception crosses
+ * this boundary and no call falls back to a CPU computation: without a
+ * usable sm_100 device every call fails with WAHGPU_ENODEV.
+ *
+ * Bitvectors use the reference's serialized layout (src/bitvector.cpp:
+ * 2283-2313, write(array_t<word_t>&)): the whole 32-bit WAH words of m_vec,
+ * then the active word's value if it holds any bits, then the active word's
+ * bit count.  Row ids are uint32 positions, ascending.
+ */
+#ifndef WAHGPU_H
+#define WAHGPU_H
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WAHGPU_OK 0
+#define WAHGPU_EINVAL (-1)     /* bad argument */
+#define WAHGPU_ENODEV (-2)     /* no usable CUDA device */
+#define WAHGPU_ECUDA (-3)      /* a CUDA call failed */
+#define WAHGPU_ENOMEM (-4)     /* device or host allocation failed */
+#define WAHGPU_EFORMAT (-5)    /* malformed serialized bitvector */
+#define WAHGPU_ERANGE (-6)     /* more bits than a 32-bit count holds */
+#define WAHGPU_ETIMEOUT (-7)   /* a bounded device-side wait gave up */
+#define WAHGPU_ESIZE (-8)      /* output buffer too small */
+#define WAHGPU_EDEGENERATE (-9) /* operand the reference would corrupt, see below */
+#define WAHGPU_EBUSY (-10)     /* admission refused: scratch budget exhausted */
+
+/* Operators, numbered as the oracle and the reference's operator order. */
+#define WAHGPU_AND 0   /* operator&  / &=  (src/bitvector.cpp:1194, 1292) */
+#define WAHGPU_OR 1    /* operator|  / |=  (src/bitvector.cpp:1413, 1488) */
+#define WAHGPU_XOR 2   /* operator^  / ^=  (src/bitvector.cpp:1557, 1624) */
+#define WAHGPU_MINUS 3 /* operator-  / -=  (src/bitvector.cpp:1685, 1768) */
+
+typedef struct wahgpu_ctx wahgpu_ctx; /* a device, a stream, scratch, a pool */
+typedef struct wahgpu_bv wahgpu_bv;   /* a device-resident ibis::bitvector */
+
+typedef struct {
+    uint64_t nwords;  /* m_vec.size() */
+    uint64_t nbits;   /* size(): bits in m_vec plus active bits */
+    uint64_t cnt;     /* cnt(): number of 1 bits */
+    uint32_t anb;     /* active.nbits */
+    uint32_t aval;    /* active.val */
+    uint32_t compressed_form; /* 1: words are as compress() leaves them */
+} wahgpu_bv_info;
+
+/* ---- context ---------------------------------------------------------- */
+/* Creates a context on CUDA device `device` with its own stream. */
+int wahgpu_ctx_create(int device, wahgpu_ctx** out);
+int wahgpu_ctx_destroy(wahgpu_ctx* ctx);
+/* Runs the context's work on `stream` (a cudaStream_t); NULL restores the
+ * context's own stream. */
+int wahgpu_ctx_set_stream(wahgpu_ctx* ctx, void* stream);
+void* wahgpu_ctx_stream(wahgpu_ctx* ctx);
+/* Waits for all work queued on the context's stream. */
+int wahgpu_ctx_sync(wahgpu_ctx* ctx);
+const char* wahgpu_last_error(wahgpu_ctx* ctx);
+/* Number of kernels this context has launched (diagnostics). */
+int64_t wahgpu_ctx_launches(wahgpu_ctx* ctx);
+
+/* ---- bitvectors ------------------------------------------------------- */
+/* Builds a device bitvector from a serialized host array, like the
+ * reference's constructor from array_t<word_t> (src/bitvector.cpp:54-105):
+ * the words are copied as given (not compressed). */
+int wahgpu_bv_from_serial(wahgpu_ctx* ctx, const uint32_t* words, uint64_t nwords,
+                          wahgpu_bv** out);
+/* Same from a serialized array already in device memory (read on the
+ * device; the trailer words are read back to the host). */
+int wahgpu_bv_from_device_serial(wahgpu_ctx* ctx, const uint32_t* dev_words, uint64_t nwords,
+                                 wahgpu_bv** out);
+/* An empty bitvector with room for `cap_words` whole words, for use as the
+ * destination of wahgpu_bv_binop_into. */
+int wahgpu_bv_create(wahgpu_ctx* ctx, uint64_t cap_words, wahgpu_bv** out);
+int wahgpu_bv_free(wahgpu_bv* bv);
+/* Metadata; waits for the kernel that produced the bitvector. */
+int wahgpu_bv_info_get(wahgpu_bv* bv, wahgpu_bv_info* info);
+/* size() (src/bitvector.h:647) and cnt() (src/bitvector.h:652). */
+int64_t wahgpu_bv_size(wahgpu_bv* bv);
+int64_t wahgpu_bv_cnt(wahgpu_bv* bv);
+/* Serialized length in words (getSerialSize()/4, src/bitvector.h:150). */
+int64_t wahgpu_bv_serial_size(wahgpu_bv* bv);
+/* write(array_t<word_t>&) (src/bitvector.cpp:2283): copies the serialized
+ * form to host memory; returns its length in words, WAHGPU_ESIZE if cap is
+ * too small. */
+int64_t wahgpu_bv_write(wahgpu_bv* bv, uint32_t* out, uint64_t cap);
+/* Device pointer to the whole words (m_vec) of a bitvector. */
+const uint32_t* wahgpu_bv_device_words(wahgpu_bv* bv);
+
+/* ---- operators --------------------------------------------------------- */
+/* *res = a OP b, or a OP= b when inplace != 0, followed by compress():
+ * the words equal the reference's operator output after compress()
+ * (src/bitvector.cpp:1194-1838, kernels 2419-4079, compress 378-469).
+ * For inplace the result is also returned in *res (a is not modified: the
+ * device keeps operands immutable).
+ *
+ * Operands whose every word covers one 31-bit group while some word is a
+ * fill (a count-1 fill word) make the reference take its uncompressed loops
+ * with the fill header combined as literal bits; such calls return
+ * WAHGPU_EDEGENERATE. */
+int wahgpu_bv_binop(wahgpu_ctx* ctx, int op, int inplace, wahgpu_bv* a, wahgpu_bv* b,
+                    wahgpu_bv** res);
+/* Same into an existing bitvector (its capacity must be at least
+ * nwords(a) + nwords(b)); allocation free when the capacity suffices. */
+int wahgpu_bv_binop_into(wahgpu_ctx* ctx, int op, int inplace, wahgpu_bv* a, wahgpu_bv* b,
+                         wahgpu_bv* res);
+/* compress() (src/bitvector.cpp:378): in place on the device. */
+int wahgpu_bv_compress(wahgpu_bv* bv);
+/* decompress() (src/bitvector.cpp:474): in place on the device. */
+int wahgpu_bv_decompress(wahgpu_bv* bv);
+/* flip() (src/bitvector.cpp:1128) followed by compress(). */
+int wahgpu_bv_flip(wahgpu_bv* bv);
+/* Row ids of the 1 bits in ascending order (firstIndexSet()/indexSet walk,
+ * src/bitvector.cpp:4524), into host memory; returns the count (cnt()),
+ * WAHGPU_ESIZE if cap is too small. */
+int64_t wahgpu_bv_rids(wahgpu_bv* bv, uint32_t* out, uint64_t cap);
+/* Same into device memory (dev_out holds cap uint32). */
+int64_t wahgpu_bv_rids_device(wahgpu_bv* bv, uint32_t* dev_out, uint64_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

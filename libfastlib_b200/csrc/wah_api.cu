@@ -1,0 +1,709 @@
+// C ABI of libwahgpu: contexts, device bitvectors, operators.
+// Declarations and the reference interfaces they replace: include/wahgpu.h.
+#include "../../include/wahgpu.h"
+#include "wah_plan.h"
+#include "wah_merge.cuh"
+#include "wah_kernels.cuh"
+#include "wah_dense.cuh"
+#include "wah_api_internal.h"
+
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstdarg>
+#include <cstring>
+#include <mutex>
+#include <map>
+#include <vector>
+#include <string>
+
+using namespace wah;
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_tls_err;
+
+int wg_fail(wahgpu_ctx* ctx, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (ctx) ctx->err = buf; else g_tls_err = buf;
+    return code;
+}
+#define CUDA_TRY(ctx, call)                                                            \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess)                                                         \
+            return wg_fail(ctx, WAHGPU_ECUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+// -------------------------------------------------------------- allocator
+static size_t size_class(size_t b) {
+    if (b < 256) return 256;
+    if (b <= (1u << 20)) { size_t c = 256; while (c < b) c <<= 1; return c; }
+    return (b + (1u << 20) - 1) & ~(size_t)((1u << 20) - 1);
+}
+void* wg_alloc(wahgpu_ctx* ctx, size_t bytes) {
+    size_t c = size_class(bytes);
+    {
+        std::lock_guard<std::mutex> g(ctx->mu);
+        auto it = ctx->pool.find(c);
+        if (it != ctx->pool.end() && !it->second.empty()) {
+            void* p = it->second.back();
+            it->second.pop_back();
+            return p;
+        }
+    }
+    void* p = nullptr;
+    if (cudaMalloc(&p, c) != cudaSuccess) {
+        // release cached blocks and retry once
+        cudaStreamSynchronize(ctx->stream);
+        std::lock_guard<std::mutex> g(ctx->mu);
+        for (auto& kv : ctx->pool) for (void* q : kv.second) cudaFree(q);
+        ctx->pool.clear();
+        cudaGetLastError();
+        if (cudaMalloc(&p, c) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+    }
+    std::lock_guard<std::mutex> g(ctx->mu);
+    ctx->sizes[p] = c;
+    ctx->bytes_allocated += c;
+    return p;
+}
+void wg_free(wahgpu_ctx* ctx, void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    auto it = ctx->sizes.find(p);
+    if (it == ctx->sizes.end()) return;
+    ctx->pool[it->second].push_back(p);
+}
+
+// Scratch for the look-back scans: tile records plus the launch sync words.
+int wg_scratch(wahgpu_ctx* ctx, uint32_t ntiles, TileRec** recs, LaunchSync** sync) {
+    if (ntiles > ctx->scratch_tiles) {
+        uint32_t want = ntiles < 1024 ? 1024 : ntiles + ntiles / 2;
+        CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        if (ctx->scratch) cudaFree(ctx->scratch);
+        ctx->scratch = nullptr;
+        size_t bytes = sizeof(LaunchSync) * 2 + (size_t)want * sizeof(TileRec);
+        if (cudaMalloc(&ctx->scratch, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            ctx->scratch_tiles = 0;
+            return wg_fail(ctx, WAHGPU_ENOMEM, "scratch allocation of %zu bytes failed", bytes);
+        }
+        CUDA_TRY(ctx, cudaMemsetAsync(ctx->scratch, 0, bytes, ctx->stream));
+        ctx->scratch_tiles = want;
+    }
+    *sync = reinterpret_cast<LaunchSync*>(ctx->scratch);
+    *recs = reinterpret_cast<TileRec*>(reinterpret_cast<char*>(ctx->scratch) + 2 * sizeof(LaunchSync));
+    return WAHGPU_OK;
+}
+
+// ------------------------------------------------------------------ context
+extern "C" int wahgpu_ctx_create(int device, wahgpu_ctx** out) {
+    if (!out) return wg_fail(nullptr, WAHGPU_EINVAL, "out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return wg_fail(nullptr, WAHGPU_ENODEV, "no CUDA device is available");
+    }
+    if (device < 0 || device >= ndev) return wg_fail(nullptr, WAHGPU_EINVAL, "bad device %d", device);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess)
+        return wg_fail(nullptr, WAHGPU_ENODEV, "cannot query device %d", device);
+    if (prop.major != 10)
+        return wg_fail(nullptr, WAHGPU_ENODEV, "device %d is sm_%d%d; this build runs on sm_100 only",
+                       device, prop.major, prop.minor);
+    wahgpu_ctx* c = new wahgpu_ctx();
+    c->device = device;
+    c->sm_count = prop.multiProcessorCount;
+    cudaSetDevice(device);
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return wg_fail(nullptr, WAHGPU_ECUDA, "stream creation failed");
+    }
+    c->stream = c->own_stream;
+    if (cudaMallocHost(&c->h_meta_stage, sizeof(DevMeta) * 4) != cudaSuccess) {
+        cudaStreamDestroy(c->own_stream);
+        delete c;
+        return wg_fail(nullptr, WAHGPU_ENOMEM, "pinned staging allocation failed");
+    }
+    // the merge kernel uses more than the default 48 KB of shared memory only
+    // when TILE_BLOCKS grows; the attribute is set once here
+    *out = c;
+    return WAHGPU_OK;
+}
+
+extern "C" int wahgpu_ctx_destroy(wahgpu_ctx* ctx) {
+    if (!ctx) return WAHGPU_EINVAL;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& kv : ctx->sizes) cudaFree(kv.first);
+    if (ctx->scratch) cudaFree(ctx->scratch);
+    if (ctx->h_meta_stage) cudaFreeHost(ctx->h_meta_stage);
+    cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return WAHGPU_OK;
+}
+
+extern "C" int wahgpu_ctx_set_stream(wahgpu_ctx* ctx, void* stream) {
+    if (!ctx) return WAHGPU_EINVAL;
+    ctx->stream = stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->own_stream;
+    return WAHGPU_OK;
+}
+extern "C" void* wahgpu_ctx_stream(wahgpu_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+extern "C" int wahgpu_ctx_sync(wahgpu_ctx* ctx) {
+    if (!ctx) return WAHGPU_EINVAL;
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return WAHGPU_OK;
+}
+extern "C" const char* wahgpu_last_error(wahgpu_ctx* ctx) {
+    return ctx ? ctx->err.c_str() : g_tls_err.c_str();
+}
+extern "C" int64_t wahgpu_ctx_launches(wahgpu_ctx* ctx) { return ctx ? (int64_t)ctx->launches : -1; }
+
+// --------------------------------------------------------------- bitvectors
+static int bv_reserve(wahgpu_bv* b, uint64_t cap) {
+    wahgpu_ctx* ctx = b->ctx;
+    if (cap < 1) cap = 1;
+    if (cap > 0xFFFFFFFFull) return wg_fail(ctx, WAHGPU_ERANGE, "capacity %llu words too large", (unsigned long long)cap);
+    if (b->words && b->cap >= cap) return WAHGPU_OK;
+    wg_free(ctx, b->words);
+    wg_free(ctx, b->bpos);
+    b->words = static_cast<uint32_t*>(wg_alloc(ctx, cap * 4));
+    b->bpos = static_cast<uint32_t*>(wg_alloc(ctx, ((cap + 31) / 32 + 2) * 4));
+    if (!b->words || !b->bpos) return wg_fail(ctx, WAHGPU_ENOMEM, "device allocation of %llu words failed", (unsigned long long)cap);
+    b->cap = (uint32_t)cap;
+    b->gt_valid = false;
+    return WAHGPU_OK;
+}
+
+wahgpu_bv* wg_bv_new(wahgpu_ctx* ctx) {
+    wahgpu_bv* b = new wahgpu_bv();
+    b->ctx = ctx;
+    b->meta = static_cast<DevMeta*>(wg_alloc(ctx, sizeof(DevMeta)));
+    if (!b->meta) { delete b; return nullptr; }
+    return b;
+}
+
+// Waits for the producer of b and copies its metadata to the host.
+int wg_bv_meta(wahgpu_bv* b) {
+    if (b->h_valid) return WAHGPU_OK;
+    wahgpu_ctx* ctx = b->ctx;
+    DevMeta* st = reinterpret_cast<DevMeta*>(ctx->h_meta_stage);
+    CUDA_TRY(ctx, cudaMemcpyAsync(st, b->meta, sizeof(DevMeta), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    b->h = *st;
+    b->h_valid = true;
+    switch (b->h.status) {
+    case 0: return WAHGPU_OK;
+    case DEV_ERR_TIMEOUT: return wg_fail(ctx, WAHGPU_ETIMEOUT, "a device-side look-back wait gave up");
+    case DEV_ERR_FORMAT: return wg_fail(ctx, WAHGPU_EFORMAT, "serialized bitvector holds a fill word of length 0");
+    case DEV_ERR_RANGE: return wg_fail(ctx, WAHGPU_ERANGE, "bitvector holds more than 2^32-1 bits");
+    default: return wg_fail(ctx, WAHGPU_ECUDA, "device status %u", b->h.status);
+    }
+}
+
+// Launches the upload scan over b->words[0..n) (device data already there).
+int wg_scan_meta(wahgpu_bv* b, uint32_t n, uint32_t anb, uint32_t aval) {
+    wahgpu_ctx* ctx = b->ctx;
+    CUDA_TRY(ctx, cudaMemsetAsync(b->meta, 0, sizeof(DevMeta), ctx->stream));
+    if (n == 0) {
+        k_small<<<1, 32, 0, ctx->stream>>>(0, 0, nullptr, nullptr, 0, 0, b->words, b->bpos, b->meta, anb, aval);
+    } else {
+        uint32_t ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+        TileRec* recs; LaunchSync* sync;
+        int rc = wg_scratch(ctx, ntiles, &recs, &sync);
+        if (rc) return rc;
+        k_meta<<<ntiles, SCAN_THREADS, 0, ctx->stream>>>(b->words, n, b->bpos, b->meta, anb, aval, recs, sync, ntiles);
+    }
+    ctx->launches++;
+    CUDA_TRY(ctx, cudaGetLastError());
+    b->h_valid = false;
+    return WAHGPU_OK;
+}
+
+static void parse_trailer(const uint32_t* tail2, uint64_t nwords, uint32_t& n, uint32_t& anb, uint32_t& aval) {
+    // src/bitvector.cpp:54-105: the last word is the active bit count when it
+    // is in 1..30 (then the word before is the active value); any other last
+    // word is dropped and the active word is empty
+    n = 0; anb = 0; aval = 0;
+    if (nwords <= 1) return;
+    const uint32_t last = tail2[1];
+    if (last > 0 && last < MAXBITS) { anb = last; aval = tail2[0]; n = (uint32_t)(nwords - 2); }
+    else n = (uint32_t)(nwords - 1);
+}
+
+extern "C" int wahgpu_bv_from_serial(wahgpu_ctx* ctx, const uint32_t* words, uint64_t nwords, wahgpu_bv** out) {
+    if (!ctx || !out || (nwords && !words)) return wg_fail(ctx, WAHGPU_EINVAL, "bad argument");
+    if (nwords > 0xFFFFFFFFull) return wg_fail(ctx, WAHGPU_ERANGE, "too many words");
+    *out = nullptr;
+    uint32_t n, anb, aval;
+    uint32_t tail[2] = {0, 0};
+    if (nwords >= 2) { tail[0] = words[nwords - 2]; tail[1] = words[nwords - 1]; }
+    parse_trailer(tail, nwords, n, anb, aval);
+    wahgpu_bv* b = wg_bv_new(ctx);
+    if (!b) return wg_fail(ctx, WAHGPU_ENOMEM, "allocation failed");
+    int rc = bv_reserve(b, n);
+    if (rc) { wahgpu_bv_free(b); return rc; }
+    if (n) {
+        cudaError_t e = cudaMemcpyAsync(b->words, words, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) { wahgpu_bv_free(b); return wg_fail(ctx, WAHGPU_ECUDA, "upload failed: %s", cudaGetErrorString(e)); }
+    }
+    rc = wg_scan_meta(b, n, anb, aval);
+    if (rc) { wahgpu_bv_free(b); return rc; }
+    b->compressed_form = false;
+    *out = b;
+    return WAHGPU_OK;
+}
+
+extern "C" int wahgpu_bv_from_device_serial(wahgpu_ctx* ctx, const uint32_t* dev_words, uint64_t nwords,
+                                            wahgpu_bv** out) {
+    if (!ctx || !out || (nwords && !dev_words)) return wg_fail(ctx, WAHGPU_EINVAL, "bad argument");
+    if (nwords > 0xFFFFFFFFull) return wg_fail(ctx, WAHGPU_ERANGE, "too many words");
+    *out = nullptr;
+    uint32_t tail[2] = {0, 0};
+    if (nwords >= 2) {
+        CUDA_TRY(ctx, cudaMemcpyAsync(tail, dev_words + nwords - 2, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    uint32_t n, anb, aval;
+    parse_trailer(tail, nwords, n, anb, aval);
+    wahgpu_bv* b = wg_bv_new(ctx);
+    if (!b) return wg_fail(ctx, WAHGPU_ENOMEM, "allocation failed");
+    int rc = bv_reserve(b, n);
+    if (rc) { wahgpu_bv_free(b); return rc; }
+    if (n) CUDA_TRY(ctx, cudaMemcpyAsync(b->words, dev_words, (size_t)n * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+    rc = wg_scan_meta(b, n, anb, aval);
+    if (rc) { wahgpu_bv_free(b); return rc; }
+    b->compressed_form = false;
+    *out = b;
+    return WAHGPU_OK;
+}
+
+extern "C" int wahgpu_bv_create(wahgpu_ctx* ctx, uint64_t cap_words, wahgpu_bv** out) {
+    if (!ctx || !out) return wg_fail(ctx, WAHGPU_EINVAL, "bad argument");
+    wahgpu_bv* b = wg_bv_new(ctx);
+    if (!b) return wg_fail(ctx, WAHGPU_ENOMEM, "allocation failed");
+    int rc = bv_reserve(b, cap_words);
+    if (rc) { wahgpu_bv_free(b); return rc; }
+    rc = wg_scan_meta(b, 0, 0, 0);
+    if (rc) { wahgpu_bv_free(b); return rc; }
+    *out = b;
+    return WAHGPU_OK;
+}
+
+extern "C" int wahgpu_bv_free(wahgpu_bv* b) {
+    if (!b) return WAHGPU_EINVAL;
+    wahgpu_ctx* ctx = b->ctx;
+    // buffers go back to the context's pool; the pool never hands a block
+    // to later work before earlier work on the same stream has used it
+    wg_free(ctx, b->words);
+    wg_free(ctx, b->bpos);
+    wg_free(ctx, b->meta);
+    wg_free(ctx, b->gt);
+    delete b;
+    return WAHGPU_OK;
+}
+
+extern "C" int wahgpu_bv_info_get(wahgpu_bv* b, wahgpu_bv_info* info) {
+    if (!b || !info) return WAHGPU_EINVAL;
+    int rc = wg_bv_meta(b);
+    if (rc) return rc;
+    info->nwords = b->h.n;
+    info->nbits = (uint64_t)b->h.groups * MAXBITS + b->h.anb;
+    info->cnt = (uint64_t)b->h.nset + __builtin_popcount(b->h.aval);
+    info->anb = b->h.anb;
+    info->aval = b->h.aval;
+    info->compressed_form = b->compressed_form ? 1u : 0u;
+    return WAHGPU_OK;
+}
+extern "C" int64_t wahgpu_bv_size(wahgpu_bv* b) {
+    wahgpu_bv_info i; int rc = wahgpu_bv_info_get(b, &i); return rc ? rc : (int64_t)i.nbits;
+}
+extern "C" int64_t wahgpu_bv_cnt(wahgpu_bv* b) {
+    wahgpu_bv_info i; int rc = wahgpu_bv_info_get(b, &i); return rc ? rc : (int64_t)i.cnt;
+}
+extern "C" int64_t wahgpu_bv_serial_size(wahgpu_bv* b) {
+    wahgpu_bv_info i; int rc = wahgpu_bv_info_get(b, &i);
+    return rc ? rc : (int64_t)(i.nwords + 1 + (i.anb > 0));
+}
+extern "C" int64_t wahgpu_bv_write(wahgpu_bv* b, uint32_t* out, uint64_t cap) {
+    if (!b || (cap && !out)) return WAHGPU_EINVAL;
+    int rc = wg_bv_meta(b);
+    if (rc) return rc;
+    wahgpu_ctx* ctx = b->ctx;
+    const uint64_t len = (uint64_t)b->h.n + 1 + (b->h.anb > 0);
+    if (cap < len) return wg_fail(ctx, WAHGPU_ESIZE, "need %llu words", (unsigned long long)len);
+    if (b->h.n) {
+        CUDA_TRY(ctx, cudaMemcpyAsync(out, b->words, (size_t)b->h.n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    uint64_t k = b->h.n;
+    if (b->h.anb > 0) out[k++] = b->h.aval;
+    out[k] = b->h.anb;
+    return (int64_t)len;
+}
+extern "C" const uint32_t* wahgpu_bv_device_words(wahgpu_bv* b) { return b ? b->words : nullptr; }
+
+// ---------------------------------------------------------------- operators
+static uint32_t combine_active(int op, uint32_t a, uint32_t b) {
+    switch (op) {
+    case OP_AND: return a & b;
+    case OP_OR: return a | b;
+    case OP_XOR: return a ^ b;
+    default: return a & ~b;
+    }
+}
+
+// Launches one instantiation of the merge kernel; its shared-memory opt-in
+// above 48 KB is made on first use.
+template <int OP, bool FSM, bool UNARY, bool FLIP>
+static void launch_k(dim3 g, size_t sm, cudaStream_t s, const MergeArgs& a) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_merge<OP, FSM, UNARY, FLIP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        attr = true;
+    }
+    k_merge<OP, FSM, UNARY, FLIP><<<g, MERGE_THREADS, sm, s>>>(a);
+}
+template <int OP>
+static void launch_merge_op(bool fsm, dim3 g, size_t sm, cudaStream_t s, const MergeArgs& a) {
+    if (fsm) launch_k<OP, true, false, false>(g, sm, s, a);
+    else launch_k<OP, false, false, false>(g, sm, s, a);
+}
+
+// Merge launch: x OP y, or a (complemented) copy of x when y == nullptr.
+int wg_launch_merge(wahgpu_ctx* ctx, int op, bool fsm, bool unary, bool flip,
+                    const wahgpu_bv* x, const wahgpu_bv* y, uint32_t groups,
+                    uint32_t anb, uint32_t aval, wahgpu_bv* res) {
+    const uint32_t nx = x->h.n, ny = y ? y->h.n : 0;
+    const uint32_t nbx = (nx + 31) / 32, nby = (ny + 31) / 32;
+    const uint32_t need = nx + ny;
+    int rc = bv_reserve(res, need);
+    if (rc) return rc;
+    uint32_t ntiles = unary ? (nbx + TILE_BLOCKS - 1) / TILE_BLOCKS : (nbx + nby + TILE_BLOCKS - 1) / TILE_BLOCKS;
+    if (ntiles == 0) ntiles = 1;
+    TileRec* recs; LaunchSync* sync;
+    rc = wg_scratch(ctx, ntiles, &recs, &sync);
+    if (rc) return rc;
+    MergeArgs a;
+    a.xw = x->words; a.xbp = x->bpos; a.nx = nx; a.nbx = nbx;
+    a.yw = y ? y->words : x->words; a.ybp = y ? y->bpos : x->bpos; a.ny = ny; a.nby = nby;
+    a.groups = groups;
+    a.out = res->words; a.obp = res->bpos; a.meta = res->meta;
+    a.recs = recs; a.sync = sync; a.ntiles = ntiles;
+    a.aval = aval; a.anb = anb;
+    CUDA_TRY(ctx, cudaMemsetAsync(res->meta, 0, sizeof(DevMeta), ctx->stream));
+    const size_t sm = sizeof(TileShared);
+    dim3 g(ntiles);
+    cudaStream_t s = ctx->stream;
+    if (unary) {
+        if (flip) launch_k<0, false, true, true>(g, sm, s, a);
+        else launch_k<0, false, true, false>(g, sm, s, a);
+    } else {
+        switch (op) {
+        case OP_AND: launch_merge_op<OP_AND>(fsm, g, sm, s, a); break;
+        case OP_OR: launch_merge_op<OP_OR>(fsm, g, sm, s, a); break;
+        case OP_XOR: launch_merge_op<OP_XOR>(fsm, g, sm, s, a); break;
+        default: launch_merge_op<OP_MINUS>(fsm, g, sm, s, a); break;
+        }
+    }
+    ctx->launches++;
+    CUDA_TRY(ctx, cudaGetLastError());
+    res->h_valid = false;
+    res->gt_valid = false;
+    res->compressed_form = true;
+    return WAHGPU_OK;
+}
+
+// Group-tile index of b (host metadata must be valid); built once.
+static int wg_gtile(wahgpu_bv* b) {
+    if (b->gt_valid) return WAHGPU_OK;
+    wahgpu_ctx* ctx = b->ctx;
+    const uint32_t nt = (b->h.groups + DT - 1) / DT;
+    if (!b->gt) {
+        b->gt = static_cast<uint32_t*>(wg_alloc(ctx, ((size_t)nt + 2) * 8));
+        if (!b->gt) return wg_fail(ctx, WAHGPU_ENOMEM, "allocation failed");
+    } else {
+        // reallocate when the current block may be too small
+        wg_free(ctx, b->gt);
+        b->gt = static_cast<uint32_t*>(wg_alloc(ctx, ((size_t)nt + 2) * 8));
+        if (!b->gt) return wg_fail(ctx, WAHGPU_ENOMEM, "allocation failed");
+    }
+    const uint32_t threads = 128, blocks = (nt + 1 + threads - 1) / threads;
+    k_gtile<<<blocks, threads, 0, ctx->stream>>>(b->words, b->bpos, b->h.n, b->h.groups, nt, b->gt);
+    ctx->launches++;
+    CUDA_TRY(ctx, cudaGetLastError());
+    b->gt_valid = true;
+    return WAHGPU_OK;
+}
+
+template <int OP>
+static void launch_dense_op(dim3 g, size_t sm, cudaStream_t s, const DenseArgs& a) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_dense<OP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        attr = true;
+    }
+    k_dense<OP><<<g, DTHREADS, sm, s>>>(a);
+}
+
+// Canonical-result operators over dense operands: group-space tiles.
+int wg_launch_dense(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t groups,
+                    uint32_t anb, uint32_t aval, wahgpu_bv* res) {
+    int rc = bv_reserve(res, (uint64_t)x->h.n + y->h.n);
+    if (rc) return rc;
+    rc = wg_gtile(x);
+    if (rc) return rc;
+    rc = wg_gtile(y);
+    if (rc) return rc;
+    const uint32_t ntiles = (groups + DT - 1) / DT;
+    TileRec* recs; LaunchSync* sync;
+    rc = wg_scratch(ctx, ntiles, &recs, &sync);
+    if (rc) return rc;
+    DenseArgs a;
+    a.xw = x->words; a.xgt = x->gt; a.nx = x->h.n;
+    a.yw = y->words; a.ygt = y->gt; a.ny = y->h.n;
+    a.groups = groups;
+    a.out = res->words; a.obp = res->bpos; a.meta = res->meta;
+    a.recs = recs; a.sync = sync; a.ntiles = ntiles;
+    a.aval = aval; a.anb = anb;
+    CUDA_TRY(ctx, cudaMemsetAsync(res->meta, 0, sizeof(DevMeta), ctx->stream));
+    const size_t sm = sizeof(DenseShared);
+    dim3 g(ntiles);
+    switch (op) {
+    case OP_AND: launch_dense_op<OP_AND>(g, sm, ctx->stream, a); break;
+    case OP_OR: launch_dense_op<OP_OR>(g, sm, ctx->stream, a); break;
+    case OP_XOR: launch_dense_op<OP_XOR>(g, sm, ctx->stream, a); break;
+    default: launch_dense_op<OP_MINUS>(g, sm, ctx->stream, a); break;
+    }
+    ctx->launches++;
+    CUDA_TRY(ctx, cudaGetLastError());
+    res->h_valid = false;
+    res->gt_valid = false;
+    res->compressed_form = true;
+    return WAHGPU_OK;
+}
+
+// A one-word device bitvector holding the collapsed form of an all-zero
+// operand (do_cnt(), src/bitvector.cpp:601-604).
+static int collapsed_copy(wahgpu_ctx* ctx, const wahgpu_bv* src, wahgpu_bv** out) {
+    wahgpu_bv* b = wg_bv_new(ctx);
+    if (!b) return wg_fail(ctx, WAHGPU_ENOMEM, "allocation failed");
+    int rc = bv_reserve(b, 1);
+    if (rc) { wahgpu_bv_free(b); return rc; }
+    uint32_t* st = reinterpret_cast<uint32_t*>(ctx->h_meta_stage) + 16;
+    st[0] = HEADER0 | src->h.groups;
+    st[1] = 0;
+    st[2] = src->h.groups;
+    CUDA_TRY(ctx, cudaMemcpyAsync(b->words, st, 4, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(b->bpos, st + 1, 8, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    b->h = src->h;
+    b->h.n = 1;
+    b->h.w0 = st[0];
+    b->h.nfill = 1;
+    b->h_valid = true;
+    // device meta mirrors the host copy
+    CUDA_TRY(ctx, cudaMemcpyAsync(b->meta, &b->h, sizeof(DevMeta), cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    *out = b;
+    return WAHGPU_OK;
+}
+
+static OperandMeta opmeta(const wahgpu_bv* b) {
+    OperandMeta m;
+    m.n = b->h.n; m.groups = b->h.groups; m.anb = b->h.anb; m.aval = b->h.aval;
+    m.nset = b->h.nset; m.w0 = b->h.w0;
+    return m;
+}
+
+extern "C" int wahgpu_bv_binop_into(wahgpu_ctx* ctx, int op, int inplace, wahgpu_bv* a, wahgpu_bv* b,
+                                    wahgpu_bv* res) {
+    if (!ctx || !a || !b || !res || op < 0 || op > 3) return wg_fail(ctx, WAHGPU_EINVAL, "bad argument");
+    if (res == a || res == b) return wg_fail(ctx, WAHGPU_EINVAL, "result must differ from the operands");
+    int rc = wg_bv_meta(a);
+    if (rc) return rc;
+    rc = wg_bv_meta(b);
+    if (rc) return rc;
+    OperandMeta ma = effective(opmeta(a)), mb = effective(opmeta(b));
+    Plan p = plan_binop(op, inplace != 0, ma, mb);
+    if (p.kind == PK_UNEQUAL)
+        return wg_fail(ctx, WAHGPU_EINVAL, "operands of different sizes (%llu, %llu bits) are not supported",
+                       (unsigned long long)a->h.groups * 31 + a->h.anb, (unsigned long long)b->h.groups * 31 + b->h.anb);
+    const uint32_t G = ma.groups;
+    if (G >= 2 && ((ma.n == G && a->h.nfill && ma.n == a->h.n) || (mb.n == G && b->h.nfill && mb.n == b->h.n)))
+        return wg_fail(ctx, WAHGPU_EDEGENERATE,
+                       "an operand has one word per group and count-1 fill words; the reference "
+                       "combines such fill headers as literal bits");
+    const uint32_t aval = combine_active(op, a->h.aval, b->h.aval);
+    const uint32_t anb = a->h.anb;
+    wahgpu_bv* ca = a;
+    wahgpu_bv* cb = b;
+    wahgpu_bv* tmpa = nullptr;
+    wahgpu_bv* tmpb = nullptr;
+    if (ma.n != a->h.n) { rc = collapsed_copy(ctx, a, &tmpa); if (rc) return rc; ca = tmpa; }
+    if (mb.n != b->h.n) { rc = collapsed_copy(ctx, b, &tmpb); if (rc) { if (tmpa) wahgpu_bv_free(tmpa); return rc; } cb = tmpb; }
+    switch (p.kind) {
+    case PK_MERGE_FSM:
+        rc = wg_launch_merge(ctx, op, true, false, false, ca, cb, G, anb, aval, res);
+        break;
+    case PK_MERGE_CANON:
+        rc = wg_launch_dense(ctx, op, ca, cb, G, anb, aval, res);
+        break;
+    case PK_COPY:
+    case PK_COPY_FLIP:
+        rc = wg_launch_merge(ctx, 0, false, true, p.kind == PK_COPY_FLIP, p.src ? cb : ca, nullptr, G, anb, aval, res);
+        break;
+    default: {
+        rc = bv_reserve(res, 1);
+        if (rc) break;
+        int mode = p.kind == PK_EMPTY ? 0 : (p.kind == PK_RAW1 ? 1 : 2);
+        cudaError_t e = cudaMemsetAsync(res->meta, 0, sizeof(DevMeta), ctx->stream);
+        if (e != cudaSuccess) { rc = wg_fail(ctx, WAHGPU_ECUDA, "memset failed"); break; }
+        k_small<<<1, 32, 0, ctx->stream>>>(mode, op, ca->words, cb->words, p.fill_n, G, res->words, res->bpos,
+                                           res->meta, anb, aval);
+        ctx->launches++;
+        e = cudaGetLastError();
+        if (e != cudaSuccess) { rc = wg_fail(ctx, WAHGPU_ECUDA, "launch failed: %s", cudaGetErrorString(e)); break; }
+        res->h_valid = false;
+        res->gt_valid = false;
+        res->compressed_form = true;
+    }
+    }
+    if (tmpa || tmpb) {
+        cudaStreamSynchronize(ctx->stream);
+        if (tmpa) wahgpu_bv_free(tmpa);
+        if (tmpb) wahgpu_bv_free(tmpb);
+    }
+    return rc;
+}
+
+extern "C" int wahgpu_bv_binop(wahgpu_ctx* ctx, int op, int inplace, wahgpu_bv* a, wahgpu_bv* b,
+                               wahgpu_bv** res) {
+    if (!res) return wg_fail(ctx, WAHGPU_EINVAL, "res is NULL");
+    *res = nullptr;
+    wahgpu_bv* r = wg_bv_new(ctx);
+    if (!r) return wg_fail(ctx, WAHGPU_ENOMEM, "allocation failed");
+    int rc = wahgpu_bv_binop_into(ctx, op, inplace, a, b, r);
+    if (rc) { wahgpu_bv_free(r); return rc; }
+    *res = r;
+    return WAHGPU_OK;
+}
+
+// Replaces b's storage with that of tmp (both on the same context).
+static void bv_take(wahgpu_bv* b, wahgpu_bv* tmp) {
+    std::swap(b->words, tmp->words);
+    std::swap(b->bpos, tmp->bpos);
+    std::swap(b->meta, tmp->meta);
+    std::swap(b->cap, tmp->cap);
+    std::swap(b->h, tmp->h);
+    std::swap(b->h_valid, tmp->h_valid);
+    std::swap(b->gt, tmp->gt);
+    std::swap(b->gt_valid, tmp->gt_valid);
+    b->compressed_form = tmp->compressed_form;
+}
+
+static int unary_op(wahgpu_bv* b, bool flip) {
+    wahgpu_ctx* ctx = b->ctx;
+    int rc = wg_bv_meta(b);
+    if (rc) return rc;
+    wahgpu_bv* r = wg_bv_new(ctx);
+    if (!r) return wg_fail(ctx, WAHGPU_ENOMEM, "allocation failed");
+    const uint32_t aval = flip && b->h.anb ? (b->h.aval ^ ((1u << b->h.anb) - 1)) : b->h.aval;
+    if (b->h.n == 0) {
+        rc = bv_reserve(r, 1);
+        if (!rc) rc = wg_scan_meta(r, 0, b->h.anb, aval);
+    } else {
+        rc = wg_launch_merge(ctx, 0, false, true, flip, b, nullptr, b->h.groups, b->h.anb, aval, r);
+    }
+    if (rc) { wahgpu_bv_free(r); return rc; }
+    cudaStreamSynchronize(ctx->stream);
+    bv_take(b, r);
+    wahgpu_bv_free(r);
+    return WAHGPU_OK;
+}
+extern "C" int wahgpu_bv_compress(wahgpu_bv* b) {
+    if (!b) return WAHGPU_EINVAL;
+    if (b->compressed_form) return WAHGPU_OK;
+    return unary_op(b, false);
+}
+extern "C" int wahgpu_bv_flip(wahgpu_bv* b) {
+    if (!b) return WAHGPU_EINVAL;
+    return unary_op(b, true);
+}
+extern "C" int wahgpu_bv_decompress(wahgpu_bv* b) {
+    if (!b) return WAHGPU_EINVAL;
+    wahgpu_ctx* ctx = b->ctx;
+    int rc = wg_bv_meta(b);
+    if (rc) return rc;
+    const uint32_t G = b->h.groups;
+    if (b->h.n == G) return WAHGPU_OK;  // already uncompressed
+    wahgpu_bv* r = wg_bv_new(ctx);
+    if (!r) return wg_fail(ctx, WAHGPU_ENOMEM, "allocation failed");
+    rc = bv_reserve(r, G);
+    if (!rc && b->h.n) {
+        uint32_t nt = (b->h.n + SCAN_TILE - 1) / SCAN_TILE;
+        k_decompress<<<nt, SCAN_THREADS, 0, ctx->stream>>>(b->words, b->h.n, b->bpos, r->words);
+        ctx->launches++;
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = wg_fail(ctx, WAHGPU_ECUDA, "launch failed: %s", cudaGetErrorString(e));
+    }
+    if (!rc) rc = wg_scan_meta(r, G, b->h.anb, b->h.aval);
+    if (rc) { wahgpu_bv_free(r); return rc; }
+    cudaStreamSynchronize(ctx->stream);
+    bv_take(b, r);
+    b->compressed_form = false;
+    wahgpu_bv_free(r);
+    return WAHGPU_OK;
+}
+
+int64_t wg_rids_device(wahgpu_bv* b, uint32_t* dev_out, uint64_t cap, uint64_t* total) {
+    wahgpu_ctx* ctx = b->ctx;
+    int rc = wg_bv_meta(b);
+    if (rc) return rc;
+    const uint64_t cnt = (uint64_t)b->h.nset + __builtin_popcount(b->h.anb ? b->h.aval & ((1u << b->h.anb) - 1) : 0u);
+    *total = cnt;
+    if (cap < cnt) return wg_fail(ctx, WAHGPU_ESIZE, "need room for %llu row ids", (unsigned long long)cnt);
+    const uint32_t n = b->h.n;
+    const uint32_t ntiles = n ? (n + SCAN_TILE - 1) / SCAN_TILE : 1;
+    TileRec* recs; LaunchSync* sync;
+    rc = wg_scratch(ctx, ntiles, &recs, &sync);
+    if (rc) return rc;
+    unsigned long long* dtot = reinterpret_cast<unsigned long long*>(wg_alloc(ctx, 8));
+    if (!dtot) return wg_fail(ctx, WAHGPU_ENOMEM, "allocation failed");
+    k_rids<<<ntiles, SCAN_THREADS, 0, ctx->stream>>>(b->words, n, b->bpos, b->h.groups, b->h.anb, b->h.aval,
+                                                      dev_out, cap, dtot, b->meta, recs, sync, ntiles);
+    ctx->launches++;
+    CUDA_TRY(ctx, cudaGetLastError());
+    wg_free(ctx, dtot);
+    return (int64_t)cnt;
+}
+
+extern "C" int64_t wahgpu_bv_rids_device(wahgpu_bv* b, uint32_t* dev_out, uint64_t cap) {
+    if (!b || (cap && !dev_out)) return WAHGPU_EINVAL;
+    uint64_t total = 0;
+    return wg_rids_device(b, dev_out, cap, &total);
+}
+
+extern "C" int64_t wahgpu_bv_rids(wahgpu_bv* b, uint32_t* out, uint64_t cap) {
+    if (!b || (cap && !out)) return WAHGPU_EINVAL;
+    wahgpu_ctx* ctx = b->ctx;
+    int rc = wg_bv_meta(b);
+    if (rc) return rc;
+    const uint64_t cnt = (uint64_t)b->h.nset + __builtin_popcount(b->h.anb ? b->h.aval & ((1u << b->h.anb) - 1) : 0u);
+    if (cap < cnt) return wg_fail(ctx, WAHGPU_ESIZE, "need room for %llu row ids", (unsigned long long)cnt);
+    if (cnt == 0) return 0;
+    uint32_t* d = static_cast<uint32_t*>(wg_alloc(ctx, cnt * 4));
+    if (!d) return wg_fail(ctx, WAHGPU_ENOMEM, "allocation failed");
+    uint64_t total = 0;
+    int64_t r = wg_rids_device(b, d, cnt, &total);
+    if (r < 0) { wg_free(ctx, d); return r; }
+    cudaError_t e = cudaMemcpyAsync(out, d, cnt * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    wg_free(ctx, d);
+    if (e != cudaSuccess) return wg_fail(ctx, WAHGPU_ECUDA, "row-id copy failed: %s", cudaGetErrorString(e));
+    rc = wg_bv_meta(b);
+    return rc ? rc : (int64_t)cnt;
+}

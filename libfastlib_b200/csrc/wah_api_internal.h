@@ -1,0 +1,52 @@
+// Internal state behind the opaque handles of include/wahgpu.h.
+#ifndef WAH_API_INTERNAL_H
+#define WAH_API_INTERNAL_H
+#include <cuda_runtime.h>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+#include "wah_dev.cuh"
+
+struct wahgpu_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;      // where work is queued
+    cudaStream_t own_stream = nullptr;  // the context's own stream
+    std::string err;
+    std::mutex mu;
+    // caching device allocator: size class -> free blocks; block -> class
+    std::map<size_t, std::vector<void*>> pool;
+    std::map<void*, size_t> sizes;
+    size_t bytes_allocated = 0;
+    // look-back scratch: two LaunchSync words then TileRec records
+    void* scratch = nullptr;
+    uint32_t scratch_tiles = 0;
+    void* h_meta_stage = nullptr;  // pinned staging for metadata reads
+    uint64_t launches = 0;
+};
+
+struct wahgpu_bv {
+    wahgpu_ctx* ctx = nullptr;
+    uint32_t* words = nullptr;  // m_vec
+    uint32_t* bpos = nullptr;   // block positions: group where word 32k starts
+    wah::DevMeta* meta = nullptr;
+    uint32_t cap = 0;           // capacity in words
+    wah::DevMeta h{};           // host copy of *meta
+    bool h_valid = false;
+    uint32_t* gt = nullptr;     // group-tile index (k_gtile), built on first use
+    bool gt_valid = false;
+    bool compressed_form = false;  // words are as compress() leaves them
+};
+
+int wg_fail(wahgpu_ctx* ctx, int code, const char* fmt, ...);
+void* wg_alloc(wahgpu_ctx* ctx, size_t bytes);
+void wg_free(wahgpu_ctx* ctx, void* p);
+int wg_scratch(wahgpu_ctx* ctx, uint32_t ntiles, wah::TileRec** recs, wah::LaunchSync** sync);
+int wg_bv_meta(wahgpu_bv* b);
+wahgpu_bv* wg_bv_new(wahgpu_ctx* ctx);
+int wg_scan_meta(wahgpu_bv* b, uint32_t n, uint32_t anb, uint32_t aval);
+int wg_launch_merge(wahgpu_ctx* ctx, int op, bool fsm, bool unary, bool flip,
+                    const wahgpu_bv* x, const wahgpu_bv* y, uint32_t groups,
+                    uint32_t anb, uint32_t aval, wahgpu_bv* res);
+#endif

@@ -1,0 +1,90 @@
+"""Seeded synthetic inputs for the benchmark workloads.
+
+Raw-WAH workload: bitvectors of 2^28 bits made of alternating 0/1 runs (a
+0-run first) whose lengths are geometric — 1-runs with mean 8 bits, 0-runs
+with mean 8(1-d)/d for set-bit density d — built the way the reference's
+appendFill (src/bitvector.h:800) builds them: whole 31-bit groups become
+literal words, runs of two or more all-0 / all-1 groups become fill words,
+a single all-0 / all-1 group stays a literal, and the trailing bits form the
+active word.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+ALLONES = 0x7FFFFFFF
+
+
+def geometric_runs(seed: int, nbits: int, density: float, mean1: float = 8.0) -> np.ndarray:
+    """Alternating run lengths (0-run first) summing to nbits; PCG64 stream
+    per seed, so the inputs are the same on every platform."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    mean0 = max(mean1 * (1.0 - density) / density, 1.0)
+    parts = []
+    total = 0
+    chunk = max(1024, int(nbits / (mean0 + mean1)) + 1024)
+    while total < nbits:
+        inter = np.empty(2 * chunk, dtype=np.int64)
+        inter[0::2] = rng.geometric(1.0 / mean0, size=chunk)
+        inter[1::2] = rng.geometric(1.0 / mean1, size=chunk)
+        cs = np.cumsum(inter)
+        need = nbits - total
+        cut = int(np.searchsorted(cs, need, side="left"))
+        if cut < len(inter):
+            inter = inter[: cut + 1]
+            inter[-1] -= int(cs[cut]) - need
+            parts.append(inter)
+            total = nbits
+        else:
+            parts.append(inter)
+            total += int(cs[-1])
+    return np.concatenate(parts).astype(np.uint64)
+
+
+def groups_from_runs(runs: np.ndarray, device: str = "cpu"):
+    """Dense 31-bit group literals (first row = bit 30) and the trailing
+    (active) bits of the bit sequence described by alternating runs."""
+    import torch
+    r = torch.as_tensor(np.asarray(runs, dtype=np.int64), device=device)
+    nbits = int(r.sum().item())
+    ends = torch.cumsum(r, 0)
+    starts = ends - r
+    ones = torch.arange(len(r), device=device) % 2 == 1
+    delta = torch.zeros(nbits + 1, dtype=torch.int32, device=device)
+    s1, e1 = starts[ones], ends[ones]
+    delta.index_add_(0, s1, torch.ones_like(s1, dtype=torch.int32))
+    delta.index_add_(0, e1, -torch.ones_like(e1, dtype=torch.int32))
+    bits = torch.cumsum(delta[:nbits], 0, dtype=torch.int32)
+    G = nbits // 31
+    anb = nbits - 31 * G
+    w = torch.pow(2, torch.arange(30, -1, -1, device=device, dtype=torch.int64))
+    groups = (bits[: 31 * G].view(G, 31).to(torch.int64) * w).sum(1).to(torch.int64)
+    aval = 0
+    for k in range(anb):
+        aval = (aval << 1) | int(bits[31 * G + k].item())
+    return groups.cpu().numpy().astype(np.uint32), anb, aval
+
+
+def canonical_wah(groups: np.ndarray, anb: int = 0, aval: int = 0) -> np.ndarray:
+    """Serialized WAH of dense group literals in appendFill's form."""
+    g = np.asarray(groups, dtype=np.uint32)
+    if len(g) == 0:
+        body = np.zeros(0, np.uint32)
+    else:
+        cls = np.where(g == 0, 0, np.where(g == ALLONES, 1, 2)).astype(np.int8)
+        # a new run starts where the class changes or at every mixed group
+        head = np.ones(len(g), dtype=bool)
+        head[1:] = (cls[1:] != cls[:-1]) | (cls[1:] == 2)
+        hidx = np.flatnonzero(head)
+        lens = np.diff(np.append(hidx, len(g)))
+        hc = cls[hidx]
+        body = g[hidx].copy()
+        fill = (hc != 2) & (lens >= 2)
+        body[fill] = np.where(hc[fill] == 1, 0xC0000000, 0x80000000).astype(np.uint32) | lens[fill].astype(np.uint32)
+    tail = [aval & ((1 << anb) - 1), anb] if anb > 0 else [0]
+    return np.concatenate([body, np.asarray(tail, dtype=np.uint32)])
+
+
+def raw_wah_operand(seed: int, nbits: int, density: float, device: str = "cpu") -> np.ndarray:
+    groups, anb, aval = groups_from_runs(geometric_runs(seed, nbits, density), device)
+    return canonical_wah(groups, anb, aval)

@@ -23,6 +23,12 @@
 //               then per query: status count nrids rids[nrids]
 //   6 na a[na] -> decompress(); reply like 1
 //   7 na a[na] -> flip(); reply like 1
+//   8 nthreads reps nops (op na a[na] nb b[nb])[nops] -> times the reference's
+//        operators: each of nthreads threads builds its own operand copies,
+//        then runs its share of the ops (round robin) reps times, each as
+//        r = a OP b; r->compress(); r->cnt().  reply: seconds(f64) for the
+//        timed part (max over threads, after a barrier), then per op the
+//        serialized result length in words
 #include "ibis.h"
 #include "irelic.h"
 #include "bitvector.h"
@@ -30,6 +36,8 @@
 #include <cstdlib>
 #include <vector>
 #include <stdint.h>
+#include <pthread.h>
+#include <time.h>
 
 static FILE *fin, *fout;
 static uint32_t rd32() { uint32_t v; if (fread(&v, 4, 1, fin) != 1) exit(3); return v; }
@@ -50,9 +58,10 @@ static ibis::bitvector* from_serial(const std::vector<uint32_t>& w) {
 static void reply_bv(int status, ibis::bitvector* r) {
     wr32((uint32_t)status);
     if (status != 0 || r == 0) { wr32(0); wr32(0); return; }
-    uint32_t cnt = r->cnt();
+    // serialize first: cnt() may collapse an all-zero m_vec (do_cnt)
     ibis::array_t<uint32_t> out;
     r->write(out);
+    uint32_t cnt = r->cnt();
     wr32(cnt);
     std::vector<uint32_t> v(out.begin(), out.end());
     wrv(v);
@@ -63,6 +72,37 @@ static void rids_of(const ibis::bitvector& bv, std::vector<uint32_t>& rids) {
         if (is.isRange()) { for (uint32_t j = ii[0]; j < ii[1]; ++j) rids.push_back(j); }
         else { for (uint32_t j = 0; j < is.nIndices(); ++j) rids.push_back(ii[j]); }
     }
+}
+
+struct TimeJob {
+    std::vector<int> ops;
+    std::vector<ibis::bitvector*> a, b;
+    int reps;
+    pthread_barrier_t* bar;
+    double secs;
+    std::vector<uint32_t> lens;
+};
+static double now_s() { struct timespec t; clock_gettime(CLOCK_MONOTONIC, &t); return t.tv_sec + 1e-9 * t.tv_nsec; }
+static void* time_thread(void* p) {
+    TimeJob* j = (TimeJob*)p;
+    j->lens.assign(j->ops.size(), 0);
+    // warm the lazily counted members of the operands once, outside the timing
+    for (size_t k = 0; k < j->ops.size(); ++k) { j->a[k]->size(); j->b[k]->size(); j->a[k]->cnt(); j->b[k]->cnt(); }
+    pthread_barrier_wait(j->bar);
+    double t0 = now_s();
+    for (int r = 0; r < j->reps; ++r) {
+        for (size_t k = 0; k < j->ops.size(); ++k) {
+            ibis::bitvector* R;
+            switch (j->ops[k]) { case 0: R = *j->a[k] & *j->b[k]; break; case 1: R = *j->a[k] | *j->b[k]; break;
+                                 case 2: R = *j->a[k] ^ *j->b[k]; break; default: R = *j->a[k] - *j->b[k]; }
+            R->compress();
+            (void)R->cnt();
+            j->lens[k] = (uint32_t)(R->getSerialSize() / 4);
+            delete R;
+        }
+    }
+    j->secs = now_s() - t0;
+    return 0;
 }
 
 int main(int argc, char** argv) {
@@ -130,6 +170,36 @@ int main(int argc, char** argv) {
                 rids_of(hits, rids);
                 wr32(c < 0 ? 1u : 0u); wr32((uint32_t)c); wrv(rids);
             }
+        } else if (kind == 8) {
+            uint32_t nth = rd32(), reps = rd32(), nops = rd32();
+            std::vector<uint32_t> ops(nops);
+            std::vector<std::vector<uint32_t> > A(nops), B(nops);
+            for (uint32_t k = 0; k < nops; ++k) { ops[k] = rd32(); A[k] = rdvec(); B[k] = rdvec(); }
+            std::vector<TimeJob> jobs(nth);
+            std::vector<pthread_t> th(nth);
+            pthread_barrier_t bar;
+            pthread_barrier_init(&bar, 0, nth);
+            std::vector<uint32_t> lens(nops, 0);
+            for (uint32_t t = 0; t < nth; ++t) {
+                jobs[t].reps = reps; jobs[t].bar = &bar;
+                for (uint32_t k = t; k < nops; k += nth) {
+                    jobs[t].ops.push_back((int)ops[k]);
+                    jobs[t].a.push_back(from_serial(A[k]));
+                    jobs[t].b.push_back(from_serial(B[k]));
+                }
+            }
+            for (uint32_t t = 0; t < nth; ++t) pthread_create(&th[t], 0, time_thread, &jobs[t]);
+            double mx = 0;
+            for (uint32_t t = 0; t < nth; ++t) { pthread_join(th[t], 0); if (jobs[t].secs > mx) mx = jobs[t].secs; }
+            for (uint32_t t = 0; t < nth; ++t) {
+                for (size_t q = 0; q < jobs[t].ops.size(); ++q) {
+                    lens[t + q * nth] = jobs[t].lens[q];
+                    delete jobs[t].a[q]; delete jobs[t].b[q];
+                }
+            }
+            pthread_barrier_destroy(&bar);
+            fwrite(&mx, 8, 1, fout);
+            for (uint32_t k = 0; k < nops; ++k) wr32(lens[k]);
         } else {
             fprintf(stderr, "refdrv: unknown request %u\n", kind);
             return 4;

@@ -1090,16 +1090,16 @@ long wo_ser_binop(int op, int inplace, int do_compress,
     if (inplace) { if (wo_binop_inplace(op, &A, &B)) return -1; res = &A; }
     else { if (wo_binop(op, &A, &B, &R)) return -1; res = &R; }
     if (do_compress) wo_compress(res);
-    if (cnt) *cnt = wo_cnt(res);
     long len = (long)wo_serialize(res, out, cap);
+    if (cnt) *cnt = wo_cnt(res);
     wo_free(&A); wo_free(&B); wo_free(&R);
     return len;
 }
 long wo_ser_compress(const uint32_t *a, uint32_t na, uint32_t *out, uint32_t cap, uint32_t *cnt) {
     wo_bv A; wo_from_serial(&A, a, na);
     wo_compress(&A);
-    if (cnt) *cnt = wo_cnt(&A);
     long len = (long)wo_serialize(&A, out, cap);
+    if (cnt) *cnt = wo_cnt(&A);
     wo_free(&A);
     return len;
 }

@@ -125,6 +125,74 @@ int64_t wahgpu_bv_rids(wahgpu_bv* bv, uint32_t* out, uint64_t cap);
 /* Same into device memory (dev_out holds cap uint32). */
 int64_t wahgpu_bv_rids_device(wahgpu_bv* bv, uint32_t* dev_out, uint64_t cap);
 
+/* ---- indexes and range evaluation ------------------------------------- */
+#define WAHGPU_RELIC 1  /* ibis::relic: one bitmap per distinct value */
+#define WAHGPU_BIN 2    /* ibis::bin: one bitmap per value bin */
+/* comparison of a range term (qExpr::COMPARE subset) */
+#define WAHGPU_CMP_NONE 0
+#define WAHGPU_CMP_LT 1
+#define WAHGPU_CMP_LE 2
+/* value types of a raw column */
+#define WAHGPU_U32 0
+#define WAHGPU_F32 1
+#define WAHGPU_I32 2
+
+typedef struct wahgpu_index wahgpu_index; /* a device-resident relic / bin index */
+typedef struct wahgpu_batch wahgpu_batch; /* a prepared set of queries */
+
+/* One range term  `lo lop x rop hi`  on the column of `idx`
+ * (ibis::qContinuousRange, src/qExpr.h:259-280; CMP_NONE drops a side). */
+typedef struct {
+    wahgpu_index* idx;
+    int lop;
+    double lo;
+    int rop;
+    double hi;
+} wahgpu_term;
+
+/* Attaches an index given as the reference's serialized triple — keys
+ * (relic: the distinct values; bin: minval[nobs] then maxval[nobs]), word
+ * offsets of the nobs+1 bitmap boundaries, and the concatenated serialized
+ * bitmaps — as produced by relic::write / bin::write (src/irelic.cpp:644,
+ * src/ibin.cpp:5836) and fastbit_iapi_deconstruct_index (src/iapi.cpp:1915);
+ * the constructors from such a triple are relic(col, nb, keys, offs, bms)
+ * (src/irelic.h:30-34) and bin(col, nb, keys, offs) (src/ibin.cpp:432).
+ * The arrays are copied to the device; nrows is the column's row count. */
+int wahgpu_index_from_triple(wahgpu_ctx* ctx, int kind, uint64_t nrows, const double* keys,
+                             uint64_t nkeys, const int64_t* offsets, uint64_t noffsets,
+                             const uint32_t* bitmaps, uint64_t nbitmaps, wahgpu_index** out);
+/* The raw column (nrows values of type vtype) for the rows of edge bins that
+ * the reference checks value by value (bin::checkBin / part::doScan,
+ * src/ibin.cpp:2057-2304, src/part.cpp:4273). */
+int wahgpu_index_set_values(wahgpu_index* idx, int vtype, const void* values, uint64_t n);
+int wahgpu_index_free(wahgpu_index* idx);
+int64_t wahgpu_index_nbitmaps(wahgpu_index* idx);
+int64_t wahgpu_index_nrows(wahgpu_index* idx);
+/* estimate(count) without a range: all 1 bits (src/irelic.cpp:1843). */
+int64_t wahgpu_index_total_ones(wahgpu_index* idx);
+
+/* Evaluates the AND of nterms range terms (countQuery::evaluate,
+ * src/countQuery.cpp:292-332, whose terms go through relic::evaluate /
+ * bin::evaluate, src/irelic.cpp:1827, src/ibin.cpp:6614).  Returns the hit
+ * count (getNumHits, src/countQuery.cpp:376); writes the ascending row ids
+ * (getHitRows, src/countQuery.cpp:387) to rids when it is non-NULL, and the
+ * hit bitvector after compress() to *hits when hits is non-NULL. */
+int64_t wahgpu_evaluate(wahgpu_ctx* ctx, const wahgpu_term* terms, uint32_t nterms,
+                        uint32_t* rids, uint64_t cap, wahgpu_bv** hits);
+
+/* Batches: nq conjunctive queries, query q being terms
+ * [query_offsets[q], query_offsets[q+1]); all indexes of a batch share one
+ * row count.  The whole batch runs as one kernel launch (wahgpu_batch_run,
+ * capturable in a CUDA graph); rid_cap > 0 keeps the row ids of all queries
+ * back to back in device memory, rid_cap == 0 counts only. */
+int wahgpu_batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, const uint32_t* query_offsets,
+                        uint32_t nq, uint64_t rid_cap, int dense_first, wahgpu_batch** out);
+int wahgpu_batch_run(wahgpu_batch* batch);
+int wahgpu_batch_counts(wahgpu_batch* batch, uint64_t* counts);
+int64_t wahgpu_batch_rids(wahgpu_batch* batch, uint32_t q, uint32_t* out, uint64_t cap);
+const uint32_t* wahgpu_batch_device_rids(wahgpu_batch* batch);
+int wahgpu_batch_free(wahgpu_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

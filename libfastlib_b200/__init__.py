@@ -43,6 +43,15 @@ class _Info(ctypes.Structure):
                 ("compressed_form", ctypes.c_uint32)]
 
 
+class _Term(ctypes.Structure):
+    _fields_ = [("idx", ctypes.c_void_p), ("lop", ctypes.c_int), ("lo", ctypes.c_double),
+                ("rop", ctypes.c_int), ("hi", ctypes.c_double)]
+
+
+RELIC, BIN = 1, 2
+CMP_NONE, CMP_LT, CMP_LE = 0, 1, 2
+U32, F32, I32 = 0, 1, 2
+
 _lib = None
 
 
@@ -83,6 +92,23 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "wahgpu_bv_flip": (ctypes.c_int, [P]),
         "wahgpu_bv_rids": (ctypes.c_int64, [P, U32P, ctypes.c_uint64]),
         "wahgpu_bv_rids_device": (ctypes.c_int64, [P, P, ctypes.c_uint64]),
+        "wahgpu_index_from_triple": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double),
+                                                    ctypes.c_uint64, ctypes.POINTER(ctypes.c_int64), ctypes.c_uint64,
+                                                    U32P, ctypes.c_uint64, ctypes.POINTER(P)]),
+        "wahgpu_index_set_values": (ctypes.c_int, [P, ctypes.c_int, P, ctypes.c_uint64]),
+        "wahgpu_index_free": (ctypes.c_int, [P]),
+        "wahgpu_index_nbitmaps": (ctypes.c_int64, [P]),
+        "wahgpu_index_nrows": (ctypes.c_int64, [P]),
+        "wahgpu_index_total_ones": (ctypes.c_int64, [P]),
+        "wahgpu_evaluate": (ctypes.c_int64, [P, ctypes.POINTER(_Term), ctypes.c_uint32, U32P, ctypes.c_uint64,
+                                             ctypes.POINTER(P)]),
+        "wahgpu_batch_create": (ctypes.c_int, [P, ctypes.POINTER(_Term), U32P, ctypes.c_uint32, ctypes.c_uint64,
+                                               ctypes.c_int, ctypes.POINTER(P)]),
+        "wahgpu_batch_run": (ctypes.c_int, [P]),
+        "wahgpu_batch_counts": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_uint64)]),
+        "wahgpu_batch_rids": (ctypes.c_int64, [P, ctypes.c_uint32, U32P, ctypes.c_uint64]),
+        "wahgpu_batch_device_rids": (P, [P]),
+        "wahgpu_batch_free": (ctypes.c_int, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -247,3 +273,106 @@ class Bitvector:
     def __ior__(self, o): return self._binop(OR, o, True)
     def __ixor__(self, o): return self._binop(XOR, o, True)
     def __isub__(self, o): return self._binop(MINUS, o, True)
+
+
+class Index:
+    """A device-resident ``ibis::relic`` / ``ibis::bin`` index attached from
+    the reference's (keys, offsets, bitmaps) triple."""
+
+    def __init__(self, ctx: Context, kind: int, nrows: int, keys, offsets, bitmaps, values=None):
+        self.ctx = ctx
+        k = np.ascontiguousarray(keys, dtype=np.float64)
+        o = np.ascontiguousarray(offsets, dtype=np.int64)
+        b = np.ascontiguousarray(bitmaps, dtype=np.uint32)
+        h = ctypes.c_void_p()
+        ctx.check(ctx.lib.wahgpu_index_from_triple(
+            ctx.h, kind, nrows, k.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(k),
+            o.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), len(o),
+            b.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), len(b), ctypes.byref(h)))
+        self.h = h
+        self.nrows = nrows
+        if values is not None:
+            self.set_values(values)
+
+    def set_values(self, values):
+        v = np.ascontiguousarray(values)
+        vt = {np.dtype(np.uint32): U32, np.dtype(np.float32): F32, np.dtype(np.int32): I32}[v.dtype]
+        self.ctx.check(self.ctx.lib.wahgpu_index_set_values(self.h, vt, v.ctypes.data_as(ctypes.c_void_p), len(v)))
+        self._values = v
+
+    def term(self, lo=None, hi=None, lop=CMP_LE, rop=CMP_LT) -> _Term:
+        """lo lop x rop hi; a missing bound drops that side."""
+        return _Term(self.h, CMP_NONE if lo is None else lop, 0.0 if lo is None else float(lo),
+                     CMP_NONE if hi is None else rop, 0.0 if hi is None else float(hi))
+
+    def close(self):
+        if getattr(self, "h", None) and self.ctx.h:
+            self.ctx.lib.wahgpu_index_free(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def evaluate(ctx: Context, terms, want_rids: bool = True, want_hits: bool = False):
+    """AND of the terms: (count, row ids or None, hit Bitvector or None)."""
+    arr = (_Term * len(terms))(*terms)
+    nrows = None
+    cap = 0
+    rids = None
+    if want_rids:
+        # an upper bound without evaluating twice: the row count
+        nrows = int(ctx.lib.wahgpu_index_nrows(terms[0].idx))
+        cap = nrows
+        rids = np.empty(max(cap, 1), dtype=np.uint32)
+    hp = ctypes.c_void_p()
+    n = ctx.check(ctx.lib.wahgpu_evaluate(ctx.h, arr, len(terms),
+                                          rids.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)) if want_rids else None,
+                                          cap, ctypes.byref(hp) if want_hits else None))
+    hits = Bitvector(ctx, hp) if want_hits else None
+    return n, (rids[:n].copy() if want_rids else None), hits
+
+
+class Batch:
+    """Queries prepared once and run as one kernel launch (capturable in a
+    CUDA graph).  queries: list of lists of terms."""
+
+    def __init__(self, ctx: Context, queries, rid_cap: int = 0):
+        self.ctx = ctx
+        flat = [t for q in queries for t in q]
+        offs = np.zeros(len(queries) + 1, dtype=np.uint32)
+        offs[1:] = np.cumsum([len(q) for q in queries])
+        self._terms = (_Term * len(flat))(*flat)
+        self._offs = offs
+        h = ctypes.c_void_p()
+        ctx.check(ctx.lib.wahgpu_batch_create(ctx.h, self._terms, offs.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                              len(queries), rid_cap, 0, ctypes.byref(h)))
+        self.h = h
+        self.nq = len(queries)
+
+    def run(self):
+        self.ctx.check(self.ctx.lib.wahgpu_batch_run(self.h))
+
+    def counts(self) -> np.ndarray:
+        out = np.zeros(self.nq, dtype=np.uint64)
+        self.ctx.check(self.ctx.lib.wahgpu_batch_counts(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+        return out
+
+    def rids(self, q: int, count: int) -> np.ndarray:
+        out = np.empty(max(count, 1), dtype=np.uint32)
+        n = self.ctx.check(self.ctx.lib.wahgpu_batch_rids(self.h, q, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), count))
+        return out[:n]
+
+    def close(self):
+        if getattr(self, "h", None) and self.ctx.h:
+            self.ctx.lib.wahgpu_batch_free(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -169,5 +169,58 @@ __device__ __forceinline__ uint4 warp_lookback(const TileRec* recs, uint32_t t, 
     return acc;
 }
 
+// Block-wide exclusive scan of 64-bit values; returns the block total.
+// (blockDim.x threads, a multiple of 32; sh holds blockDim.x/32 + 1 values)
+__device__ __forceinline__ uint64_t block_exscan64(uint64_t v, uint64_t* sh, uint64_t& total) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint64_t x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        uint64_t t = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= (uint32_t)d) x += t;
+    }
+    if (lane == 31) sh[warp] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint64_t s = 0;
+        const uint32_t nw = blockDim.x / 32;
+        for (uint32_t w = 0; w < nw; ++w) { uint64_t t = sh[w]; sh[w] = s; s += t; }
+        sh[nw] = s;
+    }
+    __syncthreads();
+    total = sh[blockDim.x / 32];
+    return sh[warp] + x - v;
+}
+
+// 64-bit sums packed in uint4 {lo, hi, sum32, or32}
+struct Sum64Comb {
+    __device__ __forceinline__ uint4 operator()(uint4 a, uint4 b) const {
+        const uint64_t s = ((uint64_t)a.y << 32 | a.x) + ((uint64_t)b.y << 32 | b.x);
+        return make_uint4((uint32_t)s, (uint32_t)(s >> 32), a.z + b.z, a.w | b.w);
+    }
+};
+
+// Warp 0 only: publishes this tile's totals, looks back, publishes the
+// inclusive prefix; returns the exclusive prefix.
+__device__ __forceinline__ bool lookback64(TileRec* recs, uint32_t t, uint32_t epoch,
+                                           uint64_t tot, uint32_t aux, uint32_t aux2,
+                                           uint64_t& prefix, uint32_t& paux, uint32_t& paux2) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint4 mine = make_uint4((uint32_t)tot, (uint32_t)(tot >> 32), aux, aux2);
+    uint4 pre = make_uint4(0, 0, 0, 0);
+    bool ok = true;
+    if (t == 0) {
+        if (lane == 0) publish(&recs[0], epoch, REC_INCL, mine);
+    } else {
+        if (lane == 0) publish(&recs[t], epoch, REC_AGG, mine);
+        pre = warp_lookback(recs, t, epoch, make_uint4(0, 0, 0, 0), Sum64Comb(), &ok);
+        if (lane == 0) publish(&recs[t], epoch, REC_INCL, Sum64Comb()(pre, mine));
+    }
+    prefix = (uint64_t)pre.y << 32 | pre.x;
+    paux = pre.z;
+    paux2 = pre.w;
+    return ok;
+}
+
 }  // namespace wah
 #endif

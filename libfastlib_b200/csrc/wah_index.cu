@@ -1,2 +1,389 @@
-// Range evaluation of relic / bin indexes (filled in by the index kernels).
+// Index store and range evaluation behind the C ABI (include/wahgpu.h):
+// relic / bin indexes attached from the reference's (keys, offsets, bitmaps)
+// triple, the host-side locate (which bitmaps a range covers wholly and which
+// edge bitmaps need a row check), and batched evaluation through k_range.
 #include "../../include/wahgpu.h"
+#include "wah_range.cuh"
+#include "wah_api_internal.h"
+
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+
+using namespace wah;
+
+struct wahgpu_index {
+    wahgpu_ctx* ctx = nullptr;
+    int kind = 0;                 // WAHGPU_RELIC / WAHGPU_BIN
+    uint32_t nrows = 0, groups = 0, anb = 0, nobs = 0, ntiles = 0;
+    std::vector<double> keys;     // relic: distinct values; bin: minval then maxval
+    std::vector<uint64_t> bwords; // m_vec words per bitmap (for the complement choice)
+    std::vector<uint32_t> bones;  // 1 bits per bitmap
+    uint32_t* d_words = nullptr;
+    BitmapMeta* d_bm = nullptr;
+    uint32_t* d_tiles = nullptr;
+    void* d_values = nullptr;
+    uint32_t vtype = 0;
+    DevIndex dev{};
+};
+
+struct wahgpu_batch {
+    wahgpu_ctx* ctx = nullptr;
+    uint32_t nq = 0, nterms = 0, nidx = 0;
+    uint32_t groups = 0, anb = 0, ntiles = 0;
+    DevIndex* d_idx = nullptr;
+    DevTerm* d_terms = nullptr;
+    DevQuery* d_queries = nullptr;
+    unsigned long long* d_counts = nullptr;
+    unsigned long long* d_start = nullptr;
+    uint32_t* d_rids = nullptr;
+    uint64_t rid_cap = 0;
+    uint32_t* d_dense = nullptr;
+    DevMeta* d_status = nullptr;
+    std::vector<unsigned long long> h_counts, h_start;
+    bool h_valid = false;
+};
+
+#define CUDA_TRY(ctx, call)                                                            \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess)                                                         \
+            return wg_fail(ctx, WAHGPU_ECUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+// ------------------------------------------------------------------ attach
+extern "C" int wahgpu_index_from_triple(wahgpu_ctx* ctx, int kind, uint64_t nrows, const double* keys,
+                                        uint64_t nkeys, const int64_t* offsets, uint64_t noffsets,
+                                        const uint32_t* bitmaps, uint64_t nbitmaps, wahgpu_index** out) {
+    if (!ctx || !out || (kind != WAHGPU_RELIC && kind != WAHGPU_BIN) || noffsets < 1 || !offsets ||
+        (nbitmaps && !bitmaps) || nrows > 0xFFFFFFFFull)
+        return wg_fail(ctx, WAHGPU_EINVAL, "bad argument");
+    *out = nullptr;
+    const uint32_t nobs = (uint32_t)(noffsets - 1);
+    if ((kind == WAHGPU_RELIC && nkeys != nobs) || (kind == WAHGPU_BIN && nkeys != 2ull * nobs) || (nkeys && !keys))
+        return wg_fail(ctx, WAHGPU_EINVAL, "key count %llu does not match %u bitmaps", (unsigned long long)nkeys, nobs);
+    if (offsets[0] != 0 || (uint64_t)offsets[nobs] != nbitmaps)
+        return wg_fail(ctx, WAHGPU_EFORMAT, "offsets do not span the bitmap array");
+    wahgpu_index* x = new wahgpu_index();
+    x->ctx = ctx; x->kind = kind; x->nrows = (uint32_t)nrows;
+    x->groups = (uint32_t)(nrows / MAXBITS); x->anb = (uint32_t)(nrows % MAXBITS);
+    x->nobs = nobs;
+    x->ntiles = (x->groups + (x->anb ? 1 : 0) + RT - 1) / RT;
+    x->keys.assign(keys, keys + nkeys);
+    // per bitmap: the serialized trailer (src/bitvector.cpp:54-105)
+    std::vector<BitmapMeta> bm(nobs);
+    x->bwords.resize(nobs);
+    for (uint32_t j = 0; j < nobs; ++j) {
+        const int64_t a = offsets[j], b = offsets[j + 1];
+        if (b < a) { delete x; return wg_fail(ctx, WAHGPU_EFORMAT, "offsets decrease at bitmap %u", j); }
+        const uint64_t len = (uint64_t)(b - a);
+        BitmapMeta& m = bm[j];
+        m.wstart = (uint64_t)a; m.n = 0; m.anb = 0; m.aval = 0; m.groups = 0;
+        if (len > 1) {
+            const uint32_t last = bitmaps[b - 1];
+            if (last > 0 && last < MAXBITS) { m.anb = last; m.aval = bitmaps[b - 2]; m.n = (uint32_t)(len - 2); }
+            else m.n = (uint32_t)(len - 1);
+        }
+        x->bwords[j] = m.n;
+    }
+    int rc = WAHGPU_OK;
+    const size_t tiles_bytes = (size_t)nobs * (x->ntiles + 1) * 8;
+    x->d_words = static_cast<uint32_t*>(wg_alloc(ctx, std::max<uint64_t>(nbitmaps, 1) * 4));
+    x->d_bm = static_cast<BitmapMeta*>(wg_alloc(ctx, std::max<size_t>(nobs, 1) * sizeof(BitmapMeta)));
+    x->d_tiles = static_cast<uint32_t*>(wg_alloc(ctx, std::max<size_t>(tiles_bytes, 8)));
+    uint32_t* d_ones = static_cast<uint32_t*>(wg_alloc(ctx, std::max<size_t>(nobs, 1) * 4));
+    DevMeta* d_st = static_cast<DevMeta*>(wg_alloc(ctx, sizeof(DevMeta)));
+    if (!x->d_words || !x->d_bm || !x->d_tiles || !d_ones || !d_st) {
+        wahgpu_index_free(x);
+        return wg_fail(ctx, WAHGPU_ENOMEM, "index allocation failed");
+    }
+    CUDA_TRY(ctx, cudaMemcpyAsync(x->d_words, bitmaps, nbitmaps * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(x->d_bm, bm.data(), nobs * sizeof(BitmapMeta), cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaMemsetAsync(d_st, 0, sizeof(DevMeta), ctx->stream));
+    if (nobs) {
+        const uint32_t threads = 256, blocks = (nobs * 32 + threads - 1) / threads;
+        k_index_tiles<<<blocks, threads, 0, ctx->stream>>>(x->d_words, x->d_bm, nobs, x->ntiles, x->nrows,
+                                                           x->d_tiles, d_ones, d_st);
+        ctx->launches++;
+        CUDA_TRY(ctx, cudaGetLastError());
+    }
+    DevMeta st{};
+    x->bones.resize(nobs);
+    CUDA_TRY(ctx, cudaMemcpyAsync(&st, d_st, sizeof(DevMeta), cudaMemcpyDeviceToHost, ctx->stream));
+    if (nobs) CUDA_TRY(ctx, cudaMemcpyAsync(x->bones.data(), d_ones, nobs * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    wg_free(ctx, d_ones);
+    wg_free(ctx, d_st);
+    if (st.status == DEV_ERR_FORMAT) rc = wg_fail(ctx, WAHGPU_EFORMAT, "a bitmap holds a fill word of length 0");
+    else if (st.status) rc = wg_fail(ctx, WAHGPU_ERANGE, "a bitmap holds more bits than the index has rows");
+    if (rc) { wahgpu_index_free(x); return rc; }
+    x->dev.words = x->d_words; x->dev.bm = x->d_bm; x->dev.tiles = x->d_tiles;
+    x->dev.values = nullptr; x->dev.nobs = nobs; x->dev.vtype = 0; x->dev.ntiles = x->ntiles;
+    *out = x;
+    return WAHGPU_OK;
+}
+
+extern "C" int wahgpu_index_set_values(wahgpu_index* x, int vtype, const void* values, uint64_t n) {
+    if (!x || !values || vtype < 0 || vtype > 2) return WAHGPU_EINVAL;
+    wahgpu_ctx* ctx = x->ctx;
+    if (n != x->nrows) return wg_fail(ctx, WAHGPU_EINVAL, "%llu values for %u rows", (unsigned long long)n, x->nrows);
+    wg_free(ctx, x->d_values);
+    x->d_values = wg_alloc(ctx, std::max<uint64_t>(n, 1) * 4);
+    if (!x->d_values) return wg_fail(ctx, WAHGPU_ENOMEM, "allocation failed");
+    CUDA_TRY(ctx, cudaMemcpyAsync(x->d_values, values, n * 4, cudaMemcpyHostToDevice, ctx->stream));
+    x->vtype = (uint32_t)vtype;
+    x->dev.values = x->d_values;
+    x->dev.vtype = x->vtype;
+    return WAHGPU_OK;
+}
+
+extern "C" int wahgpu_index_free(wahgpu_index* x) {
+    if (!x) return WAHGPU_EINVAL;
+    wahgpu_ctx* ctx = x->ctx;
+    cudaStreamSynchronize(ctx->stream);
+    wg_free(ctx, x->d_words);
+    wg_free(ctx, x->d_bm);
+    wg_free(ctx, x->d_tiles);
+    wg_free(ctx, x->d_values);
+    delete x;
+    return WAHGPU_OK;
+}
+
+extern "C" int64_t wahgpu_index_nbitmaps(wahgpu_index* x) { return x ? (int64_t)x->nobs : WAHGPU_EINVAL; }
+extern "C" int64_t wahgpu_index_nrows(wahgpu_index* x) { return x ? (int64_t)x->nrows : WAHGPU_EINVAL; }
+
+// estimate(count) of relic / bin (src/irelic.cpp:1843, src/ibin.cpp:6832):
+// the 1 bits of all bitmaps.
+extern "C" int64_t wahgpu_index_total_ones(wahgpu_index* x) {
+    if (!x) return WAHGPU_EINVAL;
+    uint64_t s = 0;
+    for (uint32_t v : x->bones) s += v;
+    return (int64_t)s;
+}
+
+// ------------------------------------------------------------------ locate
+static bool pass_h(double v, int lop, double lo, int rop, double hi) {
+    const bool a = lop == 0 ? true : (lop == 1 ? lo < v : lo <= v);
+    const bool b = rop == 0 ? true : (rop == 1 ? v < hi : v <= hi);
+    return a && b;
+}
+
+// Which bitmaps a range covers: every value of bitmaps [h0, h1) passes, the
+// rows of the cand[] bitmaps must be checked, the others hold no passing
+// value.  relic (src/irelic.cpp:1416-1809): a bitmap per key; bin
+// (src/ibin.cpp:7596-8460): a bin whose [minval, maxval] lies inside the
+// range passes whole, one that straddles an end is checked.
+static int locate(wahgpu_ctx* ctx, const wahgpu_index* x, const wahgpu_term* t, DevTerm& out) {
+    out = DevTerm{};
+    out.lop = (uint32_t)t->lop; out.rop = (uint32_t)t->rop; out.lo = t->lo; out.hi = t->hi;
+    std::vector<uint8_t> cls(x->nobs);  // 0 none, 1 all, 2 some
+    for (uint32_t j = 0; j < x->nobs; ++j) {
+        if (x->kind == WAHGPU_RELIC) {
+            cls[j] = pass_h(x->keys[j], t->lop, t->lo, t->rop, t->hi) ? 1 : 0;
+        } else {
+            const double mn = x->keys[j], mx = x->keys[x->nobs + j];
+            if (x->bones[j] == 0 || !(mn <= mx)) { cls[j] = 0; continue; }
+            const bool pmn = pass_h(mn, t->lop, t->lo, t->rop, t->hi), pmx = pass_h(mx, t->lop, t->lo, t->rop, t->hi);
+            if (pmn && pmx) cls[j] = 1;
+            else {
+                // no value in [mn, mx] passes when the range lies wholly on one side
+                const bool below = t->rop != 0 && (t->rop == 1 ? !(mn < t->hi) : !(mn <= t->hi));
+                const bool above = t->lop != 0 && (t->lop == 1 ? !(t->lo < mx) : !(t->lo <= mx));
+                cls[j] = (below || above) ? 0 : 2;
+            }
+        }
+    }
+    uint32_t h0 = x->nobs, h1 = x->nobs, nc = 0;
+    for (uint32_t j = 0; j < x->nobs; ++j) {
+        if (cls[j] == 1) { if (h0 == x->nobs) h0 = j; h1 = j + 1; }
+        else if (cls[j] == 2) {
+            if (nc >= 2) return wg_fail(ctx, WAHGPU_EINVAL, "more than two bins straddle the range");
+            out.cand[nc++] = j;
+        }
+    }
+    if (h0 == x->nobs) { h0 = 0; h1 = 0; }
+    for (uint32_t j = h0; j < h1; ++j)
+        if (cls[j] != 1) return wg_fail(ctx, WAHGPU_EINVAL, "bitmaps wholly inside the range are not contiguous");
+    if (nc > 0 && !x->d_values)
+        return wg_fail(ctx, WAHGPU_EINVAL, "range needs row checks but the index has no raw values attached");
+    out.h0 = h0; out.h1 = h1; out.ncand = nc;
+    // sumBins reads the complement when the range holds more than half the
+    // index's words (src/index.cpp:6490); the bits are the same either way
+    uint64_t in = 0, all = 0;
+    for (uint32_t j = 0; j < x->nobs; ++j) { all += x->bwords[j]; if (j >= h0 && j < h1) in += x->bwords[j]; }
+    out.flip = (2 * in > all) ? 1u : 0u;
+    return WAHGPU_OK;
+}
+
+// ------------------------------------------------------------------ batches
+extern "C" int wahgpu_batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, const uint32_t* query_offsets,
+                                   uint32_t nq, uint64_t rid_cap, int dense_first, wahgpu_batch** out) {
+    if (!ctx || !out || !terms || !query_offsets || nq == 0) return wg_fail(ctx, WAHGPU_EINVAL, "bad argument");
+    *out = nullptr;
+    const uint32_t nt = query_offsets[nq];
+    if (query_offsets[0] != 0 || nt == 0) return wg_fail(ctx, WAHGPU_EINVAL, "bad query offsets");
+    const wahgpu_index* x0 = terms[0].idx;
+    if (!x0) return wg_fail(ctx, WAHGPU_EINVAL, "term without an index");
+    std::vector<const wahgpu_index*> idx;
+    std::vector<DevTerm> dt(nt);
+    for (uint32_t i = 0; i < nt; ++i) {
+        const wahgpu_index* x = terms[i].idx;
+        if (!x || x->nrows != x0->nrows) return wg_fail(ctx, WAHGPU_EINVAL, "term %u: indexes of one batch must share their row count", i);
+        int rc = locate(ctx, x, &terms[i], dt[i]);
+        if (rc) return rc;
+        auto it = std::find(idx.begin(), idx.end(), x);
+        dt[i].index = (uint32_t)(it - idx.begin());
+        if (it == idx.end()) idx.push_back(x);
+    }
+    std::vector<DevQuery> dq(nq);
+    for (uint32_t q = 0; q < nq; ++q) {
+        if (query_offsets[q + 1] <= query_offsets[q]) return wg_fail(ctx, WAHGPU_EINVAL, "query %u has no term", q);
+        dq[q].t0 = query_offsets[q]; dq[q].t1 = query_offsets[q + 1];
+    }
+    std::vector<DevIndex> di;
+    for (auto* x : idx) di.push_back(x->dev);
+    wahgpu_batch* B = new wahgpu_batch();
+    B->ctx = ctx; B->nq = nq; B->nterms = nt; B->nidx = (uint32_t)idx.size();
+    B->groups = x0->groups; B->anb = x0->anb; B->ntiles = x0->ntiles;
+    B->d_idx = static_cast<DevIndex*>(wg_alloc(ctx, di.size() * sizeof(DevIndex)));
+    B->d_terms = static_cast<DevTerm*>(wg_alloc(ctx, nt * sizeof(DevTerm)));
+    B->d_queries = static_cast<DevQuery*>(wg_alloc(ctx, nq * sizeof(DevQuery)));
+    B->d_counts = static_cast<unsigned long long*>(wg_alloc(ctx, nq * 8));
+    B->d_start = static_cast<unsigned long long*>(wg_alloc(ctx, nq * 8));
+    B->d_status = static_cast<DevMeta*>(wg_alloc(ctx, sizeof(DevMeta)));
+    B->rid_cap = rid_cap;
+    if (rid_cap) B->d_rids = static_cast<uint32_t*>(wg_alloc(ctx, rid_cap * 4));
+    if (dense_first) B->d_dense = static_cast<uint32_t*>(wg_alloc(ctx, ((size_t)x0->groups + 1) * 4));
+    if (!B->d_idx || !B->d_terms || !B->d_queries || !B->d_counts || !B->d_start || !B->d_status ||
+        (rid_cap && !B->d_rids) || (dense_first && !B->d_dense)) {
+        wahgpu_batch_free(B);
+        return wg_fail(ctx, WAHGPU_ENOMEM, "batch allocation failed");
+    }
+    CUDA_TRY(ctx, cudaMemcpyAsync(B->d_idx, di.data(), di.size() * sizeof(DevIndex), cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(B->d_terms, dt.data(), nt * sizeof(DevTerm), cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(B->d_queries, dq.data(), nq * sizeof(DevQuery), cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));  // host staging above is pageable
+    *out = B;
+    return WAHGPU_OK;
+}
+
+extern "C" int wahgpu_batch_run(wahgpu_batch* B) {
+    if (!B) return WAHGPU_EINVAL;
+    wahgpu_ctx* ctx = B->ctx;
+    const uint32_t nitems = B->nq * B->ntiles;
+    if (nitems == 0) return WAHGPU_OK;
+    TileRec* recs; LaunchSync* sync;
+    int rc = wg_scratch(ctx, nitems, &recs, &sync);
+    if (rc) return rc;
+    CUDA_TRY(ctx, cudaMemsetAsync(B->d_counts, 0, B->nq * 8, ctx->stream));
+    CUDA_TRY(ctx, cudaMemsetAsync(B->d_status, 0, sizeof(DevMeta), ctx->stream));
+    RangeArgs a;
+    a.idx = B->d_idx; a.terms = B->d_terms; a.queries = B->d_queries; a.nq = B->nq;
+    a.groups = B->groups; a.anb = B->anb; a.ntiles = B->ntiles;
+    a.counts = B->d_counts; a.rids = B->d_rids; a.rid_cap = B->rid_cap; a.rid_start = B->d_start;
+    a.dense = B->d_dense;
+    a.recs = recs; a.sync = sync; a.nitems = nitems; a.status = B->d_status;
+    static bool attr = false;
+    const size_t sm = sizeof(RangeShared);
+    if (!attr) { cudaFuncSetAttribute(k_range, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); attr = true; }
+    k_range<<<nitems, RTHREADS, sm, ctx->stream>>>(a);
+    ctx->launches++;
+    CUDA_TRY(ctx, cudaGetLastError());
+    B->h_valid = false;
+    return WAHGPU_OK;
+}
+
+static int batch_fetch(wahgpu_batch* B) {
+    if (B->h_valid) return WAHGPU_OK;
+    wahgpu_ctx* ctx = B->ctx;
+    B->h_counts.resize(B->nq);
+    B->h_start.resize(B->nq);
+    DevMeta st{};
+    CUDA_TRY(ctx, cudaMemcpyAsync(B->h_counts.data(), B->d_counts, B->nq * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(B->h_start.data(), B->d_start, B->nq * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(&st, B->d_status, sizeof(DevMeta), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (st.status == DEV_ERR_TIMEOUT) return wg_fail(ctx, WAHGPU_ETIMEOUT, "a device-side look-back wait gave up");
+    B->h_valid = true;
+    return WAHGPU_OK;
+}
+
+extern "C" int wahgpu_batch_counts(wahgpu_batch* B, uint64_t* counts) {
+    if (!B || !counts) return WAHGPU_EINVAL;
+    int rc = batch_fetch(B);
+    if (rc) return rc;
+    for (uint32_t q = 0; q < B->nq; ++q) counts[q] = B->h_counts[q];
+    return WAHGPU_OK;
+}
+
+extern "C" int64_t wahgpu_batch_rids(wahgpu_batch* B, uint32_t q, uint32_t* out, uint64_t cap) {
+    if (!B || q >= B->nq || (cap && !out)) return WAHGPU_EINVAL;
+    wahgpu_ctx* ctx = B->ctx;
+    int rc = batch_fetch(B);
+    if (rc) return rc;
+    const uint64_t n = B->h_counts[q], s = B->h_start[q];
+    if (!B->d_rids || s + n > B->rid_cap) return wg_fail(ctx, WAHGPU_ESIZE, "row ids exceed the batch's capacity");
+    if (cap < n) return wg_fail(ctx, WAHGPU_ESIZE, "need room for %llu row ids", (unsigned long long)n);
+    if (n) {
+        CUDA_TRY(ctx, cudaMemcpyAsync(out, B->d_rids + s, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    return (int64_t)n;
+}
+
+extern "C" const uint32_t* wahgpu_batch_device_rids(wahgpu_batch* B) { return B ? B->d_rids : nullptr; }
+
+extern "C" int wahgpu_batch_free(wahgpu_batch* B) {
+    if (!B) return WAHGPU_EINVAL;
+    wahgpu_ctx* ctx = B->ctx;
+    cudaStreamSynchronize(ctx->stream);
+    wg_free(ctx, B->d_idx); wg_free(ctx, B->d_terms); wg_free(ctx, B->d_queries);
+    wg_free(ctx, B->d_counts); wg_free(ctx, B->d_start); wg_free(ctx, B->d_status);
+    wg_free(ctx, B->d_rids); wg_free(ctx, B->d_dense);
+    delete B;
+    return WAHGPU_OK;
+}
+
+// One conjunctive query (countQuery::evaluate, src/countQuery.cpp:292):
+// returns the hit count; row ids into host memory when out is given; the hit
+// bitvector (compress()ed) when hits is given.
+extern "C" int64_t wahgpu_evaluate(wahgpu_ctx* ctx, const wahgpu_term* terms, uint32_t nterms,
+                                   uint32_t* rids, uint64_t cap, wahgpu_bv** hits) {
+    if (!ctx || !terms || nterms == 0 || (cap && !rids)) return wg_fail(ctx, WAHGPU_EINVAL, "bad argument");
+    const uint32_t qo[2] = {0, nterms};
+    wahgpu_batch* B = nullptr;
+    int rc = wahgpu_batch_create(ctx, terms, qo, 1, rids ? cap : 0, hits ? 1 : 0, &B);
+    if (rc) return rc;
+    rc = wahgpu_batch_run(B);
+    uint64_t cnt = 0;
+    if (!rc) rc = wahgpu_batch_counts(B, &cnt);
+    if (!rc && rids) {
+        int64_t n = wahgpu_batch_rids(B, 0, rids, cap);
+        if (n < 0) rc = (int)n;
+    }
+    if (!rc && hits) {
+        // the dense hit words become a bitvector; compress() gives the
+        // canonical words the reference holds after compress()
+        const wahgpu_index* x = terms[0].idx;
+        wahgpu_bv* hv = nullptr;
+        rc = wahgpu_bv_create(ctx, (uint64_t)x->groups + 1, &hv);
+        if (!rc) {
+            wahgpu_bv* b = hv;
+            uint32_t aval = 0;
+            if (x->anb) {
+                uint32_t last = 0;
+                cudaMemcpyAsync(&last, B->d_dense + x->groups, 4, cudaMemcpyDeviceToHost, ctx->stream);
+                cudaStreamSynchronize(ctx->stream);
+                aval = last >> (31u - x->anb);
+            }
+            cudaMemcpyAsync(b->words, B->d_dense, (size_t)x->groups * 4, cudaMemcpyDeviceToDevice, ctx->stream);
+            rc = wg_scan_meta(b, x->groups, x->anb, aval);
+            if (!rc) rc = wahgpu_bv_compress(b);
+            if (!rc) *hits = hv; else wahgpu_bv_free(hv);
+        }
+    }
+    wahgpu_batch_free(B);
+    return rc ? rc : (int64_t)cnt;
+}

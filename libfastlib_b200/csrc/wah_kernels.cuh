@@ -12,57 +12,6 @@ constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_WPT = 16;                              // words per thread
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_WPT;        // 4096 words, 128 blocks
 
-// Block-wide exclusive scan of 64-bit values; returns the block total.
-__device__ __forceinline__ uint64_t block_exscan64(uint64_t v, uint64_t* sh, uint64_t& total) {
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    uint64_t x = v;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        uint64_t t = __shfl_up_sync(0xffffffffu, x, d);
-        if (lane >= (uint32_t)d) x += t;
-    }
-    if (lane == 31) sh[warp] = x;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint64_t s = 0;
-        for (int w = 0; w < SCAN_THREADS / 32; ++w) { uint64_t t = sh[w]; sh[w] = s; s += t; }
-        sh[SCAN_THREADS / 32] = s;
-    }
-    __syncthreads();
-    total = sh[SCAN_THREADS / 32];
-    return sh[warp] + x - v;
-}
-
-// 64-bit sums packed in uint4 {lo, hi, sum32, or32}
-struct Sum64Comb {
-    __device__ __forceinline__ uint4 operator()(uint4 a, uint4 b) const {
-        const uint64_t s = ((uint64_t)a.y << 32 | a.x) + ((uint64_t)b.y << 32 | b.x);
-        return make_uint4((uint32_t)s, (uint32_t)(s >> 32), a.z + b.z, a.w | b.w);
-    }
-};
-
-// Warp 0 only: publishes this tile's totals, looks back, publishes the
-// inclusive prefix; returns the exclusive prefix.
-__device__ __forceinline__ bool lookback64(TileRec* recs, uint32_t t, uint32_t epoch,
-                                           uint64_t tot, uint32_t aux, uint32_t aux2,
-                                           uint64_t& prefix, uint32_t& paux, uint32_t& paux2) {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint4 mine = make_uint4((uint32_t)tot, (uint32_t)(tot >> 32), aux, aux2);
-    uint4 pre = make_uint4(0, 0, 0, 0);
-    bool ok = true;
-    if (t == 0) {
-        if (lane == 0) publish(&recs[0], epoch, REC_INCL, mine);
-    } else {
-        if (lane == 0) publish(&recs[t], epoch, REC_AGG, mine);
-        pre = warp_lookback(recs, t, epoch, make_uint4(0, 0, 0, 0), Sum64Comb(), &ok);
-        if (lane == 0) publish(&recs[t], epoch, REC_INCL, Sum64Comb()(pre, mine));
-    }
-    prefix = (uint64_t)pre.y << 32 | pre.x;
-    paux = pre.z;
-    paux2 = pre.w;
-    return ok;
-}
-
 // Upload scan: for words w[0..n) writes bpos[k] (k = 0..ceil(n/32)) and
 // meta {n, groups, nset, w0, nfill, status}.  A count-0 fill word is a
 // format error; more than 2^32-1 bits is a range error (the reference keeps

@@ -1,0 +1,326 @@
+// Range evaluation over equality-encoded indexes (relic: one bitmap per
+// distinct value; bin: one bitmap per value bin) and the AND across columns.
+//
+// The reference evaluates `lo <op> x <op> hi` as
+//   relic::evaluate  (src/irelic.cpp:1827): locate -> sumBins(h0, h1)
+//   bin::evaluate    (src/ibin.cpp:6614):   locate -> sumBins over the bins
+//                    wholly inside the range, plus the rows of the edge
+//                    bins whose values pass the comparison (checkBin /
+//                    doScan on the raw values, src/ibin.cpp:2057-2304)
+//   index::sumBins   (src/index.cpp:6450): OR of bitmaps [h0, h1), or the
+//                    complement OR'ed and flipped when that reads fewer bytes
+//   countQuery::doEvaluate (src/countQuery.cpp:953-1036): AND of the terms.
+// The hit set is exactly the rows whose value passes the comparison done in
+// double (qContinuousRange::inRange, src/qExpr.cpp:1647-1667); the reference's
+// OR order (a heap ordered by pointer values) changes only the words of its
+// intermediate results, never the bits.
+//
+// Work item = (query, tile of RT groups), claimed in order.  For each term
+// the warps of the CTA OR the covered bitmaps' words for the tile into a
+// shared-memory accumulator (bitmap b goes to warp b % warps; each warp walks
+// its bitmap's words 32 at a time, positions by ballot / scan), the edge bins'
+// rows are checked against the raw column, and the term result is AND'ed
+// into the query result.  Hit counts and row ids follow; row-id positions come
+// from one decoupled look-back over the items in claim order, so each query's
+// ids are contiguous and ascending.
+#ifndef WAH_RANGE_CUH
+#define WAH_RANGE_CUH
+#include "wah_dev.cuh"
+
+namespace wah {
+
+constexpr int RT = 4096;             // groups per tile
+constexpr int RTHREADS = 256;
+constexpr int RWARPS = RTHREADS / 32;
+constexpr int RGPT = RT / RTHREADS;  // groups per thread in the epilogue
+
+// per-bitmap metadata of an attached index
+struct BitmapMeta {
+    uint64_t wstart;  // first m_vec word in the index's word pool
+    uint32_t n;       // m_vec words
+    uint32_t anb;     // active bits
+    uint32_t aval;    // active value
+    uint32_t groups;  // groups covered by m_vec (set by k_index_tiles)
+};
+
+struct DevIndex {
+    const uint32_t* words;     // word pool (the bitmaps' serialized arrays)
+    const BitmapMeta* bm;      // nobs entries
+    const uint32_t* tiles;     // nobs x (ntiles+1) x {word index, first group}
+    const void* values;        // raw column (nrows), or null
+    uint32_t nobs;
+    uint32_t vtype;            // 0 uint32, 1 float32, 2 int32
+    uint32_t ntiles;
+    uint32_t pad;
+};
+
+// comparison ops (qExpr::COMPARE): 0 none, 1 <, 2 <=
+struct DevTerm {
+    uint32_t index;       // into the DevIndex table
+    uint32_t h0, h1;      // bitmaps wholly inside: [h0, h1)
+    uint32_t flip;        // OR the complement [0,h0) u [h1,nobs) and flip
+    uint32_t ncand;       // edge bitmaps to check row by row (0..2)
+    uint32_t cand[2];
+    uint32_t lop, rop;    // lo lop x rop hi
+    double lo, hi;
+};
+
+struct DevQuery {
+    uint32_t t0, t1;      // terms [t0, t1)
+};
+
+struct RangeArgs {
+    const DevIndex* idx;
+    const DevTerm* terms;
+    const DevQuery* queries;
+    uint32_t nq;
+    uint32_t groups;          // whole groups per column (nrows / 31)
+    uint32_t anb;             // rows past the last whole group
+    uint32_t ntiles;          // tiles per query
+    unsigned long long* counts;  // per query (zeroed by the caller)
+    uint32_t* rids;           // row ids, all queries back to back (or null)
+    uint64_t rid_cap;
+    unsigned long long* rid_start;  // per query: offset of its first row id
+    uint32_t* dense;          // dense hit words of query 0 (or null)
+    TileRec* recs; LaunchSync* sync; uint32_t nitems;
+    DevMeta* status;
+};
+
+struct RangeShared {
+    uint32_t acc[RT];
+    uint32_t tmp[RT];
+    uint64_t scan[RWARPS + 1];
+    uint32_t hdr[8];
+    unsigned long long base;
+};
+
+__device__ __forceinline__ bool pass_cmp(double v, uint32_t lop, double lo, uint32_t rop, double hi) {
+    const bool a = lop == 0 ? true : (lop == 1 ? lo < v : lo <= v);
+    const bool b = rop == 0 ? true : (rop == 1 ? v < hi : v <= hi);
+    return a && b;
+}
+__device__ __forceinline__ double col_value(const void* vals, uint32_t vtype, uint32_t row) {
+    if (vtype == 1) return (double)__ldg(reinterpret_cast<const float*>(vals) + row);
+    if (vtype == 2) return (double)__ldg(reinterpret_cast<const int32_t*>(vals) + row);
+    return (double)__ldg(reinterpret_cast<const uint32_t*>(vals) + row);
+}
+
+// One warp ORs bitmap b's words for the tile [g0, g1) into S.tmp.  With
+// check != nullptr the bitmap's rows are instead tested against the term's
+// comparison on the raw column and only passing rows are set.  The virtual
+// group G holds the active bits.
+__device__ __forceinline__ void warp_or_bitmap(RangeShared& S, const DevIndex& I, uint32_t b, uint32_t k,
+                                               uint32_t g0, uint32_t g1, uint32_t G, uint32_t anb,
+                                               const DevTerm* check) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const BitmapMeta m = I.bm[b];
+    const uint32_t* tix = I.tiles + ((size_t)b * (I.ntiles + 1) + k) * 2;
+    const uint32_t i0 = __ldg(tix), s0 = __ldg(tix + 1);
+    const uint32_t in1 = __ldg(tix + 2), sn1 = __ldg(tix + 3);
+    const uint32_t i1 = min(sn1 < g1 ? in1 + 1u : in1, m.n);  // words covering [g0, min(g1, G))
+    const uint32_t* w = I.words + m.wstart;
+    uint32_t carry = s0;
+    for (uint32_t base = i0; base < i1; base += 32) {
+        const uint32_t i = base + lane;
+        const bool in = i < i1;
+        const uint32_t wd = in ? __ldg(w + i) : 0u;
+        const uint32_t c = in ? wgroups(wd) : 0u;
+        uint32_t p;
+        const uint32_t fm = __ballot_sync(0xffffffffu, in && is_fill(wd));
+        if (fm == 0) {
+            p = carry + lane;
+            carry += __popc(__ballot_sync(0xffffffffu, in));
+        } else {
+            uint32_t x = c;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) { uint32_t t = __shfl_up_sync(0xffffffffu, x, d); if (lane >= (uint32_t)d) x += t; }
+            p = carry + x - c;
+            carry += __shfl_sync(0xffffffffu, x, 31);
+        }
+        if (in && wd != 0u && !(is_fill(wd) && wd < HEADER1)) {
+            const uint32_t a = max(p, g0), e = min(p + c, g1);
+            const uint32_t pat = wpattern(wd);
+            for (uint32_t g = a; g < e; ++g) {
+                if (!check) {
+                    if (pat == ALLONES) S.tmp[g - g0] = ALLONES;
+                    else atomicOr(&S.tmp[g - g0], pat);
+                } else {
+                    uint32_t bits = pat, set = 0;
+                    while (bits) {
+                        const uint32_t hb = 31u - __clz(bits);
+                        const uint32_t row = g * 31u + (30u - hb);
+                        if (pass_cmp(col_value(I.values, I.vtype, row), check->lop, check->lo, check->rop, check->hi))
+                            set |= 1u << hb;
+                        bits &= ~(1u << hb);
+                    }
+                    if (set) atomicOr(&S.tmp[g - g0], set);
+                }
+            }
+        }
+    }
+    // the bitmap's active bits form the group after its whole words (the
+    // virtual group G when the bitmap covers every row)
+    const uint32_t Gb = m.groups;
+    if (lane == 0 && m.anb > 0 && Gb >= g0 && Gb < g1) {
+        uint32_t pat = (m.aval & ((1u << m.anb) - 1u)) << (31u - m.anb);
+        if (check) {
+            uint32_t bits = pat, set = 0;
+            while (bits) {
+                const uint32_t hb = 31u - __clz(bits);
+                const uint32_t row = Gb * 31u + (30u - hb);
+                if (pass_cmp(col_value(I.values, I.vtype, row), check->lop, check->lo, check->rop, check->hi))
+                    set |= 1u << hb;
+                bits &= ~(1u << hb);
+            }
+            pat = set;
+        }
+        if (pat) atomicOr(&S.tmp[Gb - g0], pat);
+    }
+}
+
+__global__ void __launch_bounds__(RTHREADS) k_range(RangeArgs A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    RangeShared& S = *reinterpret_cast<RangeShared*>(smem_raw);
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    if (tid == 0) { S.hdr[0] = claim_tile(A.sync); S.hdr[1] = ld_cg(&A.sync->epoch); }
+    __syncthreads();
+    const uint32_t item = S.hdr[0], epoch = S.hdr[1];
+    const uint32_t q = item / A.ntiles, k = item % A.ntiles;
+    const uint32_t G = A.groups, anb = A.anb;
+    const uint32_t GX = G + (anb > 0 ? 1u : 0u);  // groups incl. the active one
+    const uint32_t g0 = k * (uint32_t)RT, g1 = min(g0 + (uint32_t)RT, GX);
+    const uint32_t ng = g1 > g0 ? g1 - g0 : 0u;
+    const uint32_t lastmask = anb > 0 ? (((1u << anb) - 1u) << (31u - anb)) : ALLONES;
+    const DevQuery Q = A.queries[q];
+
+    for (uint32_t l = tid; l < RT; l += RTHREADS) S.acc[l] = ALLONES;
+    for (uint32_t t = Q.t0; t < Q.t1; ++t) {
+        const DevTerm T = A.terms[t];
+        const DevIndex I = A.idx[T.index];
+        for (uint32_t l = tid; l < RT; l += RTHREADS) S.tmp[l] = 0u;
+        __syncthreads();
+        // wholly-inside bitmaps (or their complement)
+        const uint32_t nsel = T.flip ? (T.h0 + (I.nobs - T.h1)) : (T.h1 - T.h0);
+        for (uint32_t j = warp; j < nsel; j += RWARPS) {
+            uint32_t b;
+            if (T.flip) b = j < T.h0 ? j : T.h1 + (j - T.h0);
+            else b = T.h0 + j;
+            warp_or_bitmap(S, I, b, k, g0, g1, G, anb, nullptr);
+        }
+        __syncthreads();
+        if (T.flip) {
+            for (uint32_t l = tid; l < ng; l += RTHREADS) {
+                const uint32_t msk = (g0 + l == G && anb > 0) ? lastmask : ALLONES;
+                S.tmp[l] ^= msk;
+            }
+            __syncthreads();
+        }
+        // edge bitmaps: rows checked against the raw values
+        for (uint32_t c = warp; c < T.ncand; c += RWARPS)
+            warp_or_bitmap(S, I, T.cand[c], k, g0, g1, G, anb, &T);
+        __syncthreads();
+        for (uint32_t l = tid; l < RT; l += RTHREADS) S.acc[l] &= S.tmp[l];
+        __syncthreads();
+    }
+    // ---- counts and row ids
+    const uint32_t l0 = tid * RGPT;
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int j = 0; j < RGPT; ++j) {
+        const uint32_t l = l0 + j;
+        if (l < ng) {
+            uint32_t v = S.acc[l];
+            if (g0 + l == G && anb > 0) v &= lastmask;
+            S.acc[l] = v;
+            cnt += __popc(v);
+        } else if (l < RT) {
+            S.acc[l] = 0u;
+        }
+    }
+    uint64_t total;
+    const uint64_t ex = block_exscan64(cnt, S.scan, total);
+    if (warp == 0) {
+        uint64_t prefix; uint32_t pa, pb;
+        const bool ok = lookback64(A.recs, item, epoch, total, 0, 0, prefix, pa, pb);
+        if (lane == 0) {
+            if (!ok) atomicExch(&A.status->status, DEV_ERR_TIMEOUT);
+            S.base = prefix;
+            if (total) atomicAdd(&A.counts[q], (unsigned long long)total);
+            if (k == 0) A.rid_start[q] = prefix;
+        }
+    }
+    __syncthreads();
+    if (A.rids) {
+        uint64_t off = S.base + ex;
+        for (int j = 0; j < RGPT; ++j) {
+            const uint32_t l = l0 + j;
+            if (l >= ng) break;
+            uint32_t bits = S.acc[l];
+            const uint32_t rbase = (g0 + l) * 31u;
+            while (bits) {
+                const uint32_t hb = 31u - __clz(bits);
+                if (off < A.rid_cap) A.rids[off] = rbase + (30u - hb);
+                ++off;
+                bits &= ~(1u << hb);
+            }
+        }
+    }
+    if (A.dense && q == 0) {
+        for (uint32_t l = tid; l < ng; l += RTHREADS) A.dense[g0 + l] = S.acc[l];
+    }
+    __syncthreads();
+    if (tid == 0) finish_tile(A.sync, A.nitems);
+}
+
+// Per-bitmap group-tile index of an attached index: one warp per bitmap
+// walks its words, records the word covering every multiple of RT, checks
+// the words and counts groups and ones.
+__global__ void k_index_tiles(const uint32_t* __restrict__ words, BitmapMeta* __restrict__ bm,
+                              uint32_t nobs, uint32_t ntiles, uint32_t nrows, uint32_t* __restrict__ tiles,
+                              uint32_t* __restrict__ bones, DevMeta* status) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (b >= nobs) return;
+    const BitmapMeta m = bm[b];
+    const uint32_t* w = words + m.wstart;
+    uint32_t* tix = tiles + (size_t)b * (ntiles + 1) * 2;
+    uint32_t carry = 0, ones = 0, bad = 0;
+    uint32_t next_t = 0;  // next tile boundary not yet recorded
+    for (uint32_t base = 0; base < m.n; base += 32) {
+        const uint32_t i = base + lane;
+        const bool in = i < m.n;
+        const uint32_t wd = in ? __ldg(w + i) : 0u;
+        const uint32_t c = in ? wgroups(wd) : 0u;
+        if (in && is_fill(wd) && c == 0) bad = 1;
+        if (in) ones += wd > ALLONES ? (wd >= HEADER1 ? c * 31u : 0u) : __popc(wd);
+        uint32_t x = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) { uint32_t t = __shfl_up_sync(0xffffffffu, x, d); if (lane >= (uint32_t)d) x += t; }
+        const uint32_t p = carry + x - c;  // first group of word i
+        // word i covers boundaries t*RT in [p, p+c)
+        if (in && c > 0) {
+            uint32_t t = (p + RT - 1) / RT;
+            for (; (uint64_t)t * RT < (uint64_t)p + c && t <= ntiles; ++t) {
+                tix[2 * t] = i;
+                tix[2 * t + 1] = p;
+            }
+        }
+        carry += __shfl_sync(0xffffffffu, x, 31);
+    }
+    (void)next_t;
+    // boundaries at or past the end of the words
+    for (uint32_t t = lane; t <= ntiles; t += 32) {
+        if ((uint64_t)t * RT >= carry) { tix[2 * t] = m.n; tix[2 * t + 1] = carry; }
+    }
+    ones = __reduce_add_sync(0xffffffffu, ones);
+    bad = __reduce_or_sync(0xffffffffu, bad);
+    if (lane == 0) {
+        bm[b].groups = carry;
+        bones[b] = ones + __popc(m.anb ? (m.aval & ((1u << m.anb) - 1u)) : 0u);
+        if (bad) atomicExch(&status->status, DEV_ERR_FORMAT);
+        else if ((uint64_t)carry * 31u + m.anb > nrows) atomicExch(&status->status, DEV_ERR_RANGE);
+    }
+}
+
+}  // namespace wah
+#endif

@@ -23,6 +23,13 @@
 //               then per query: status count nrids rids[nrids]
 //   6 na a[na] -> decompress(); reply like 1
 //   7 na a[na] -> flip(); reply like 1
+//   9 nrows vals(f32)[nrows] nbins nq (lo hi)(f64 x2)[nq] -> ibis::bin index
+//        through the in-memory C API: fastbit_iapi_register_array +
+//        fastbit_iapi_build_index("<binning nbins=N equal_weight/>") +
+//        fastbit_iapi_deconstruct_index (src/iapi.cpp:1644, 1893, 1915), then
+//        per query osr(x >= lo) AND osr(x < hi), evaluate and
+//        get_coordinates (src/iapi.cpp:2062, 1285, 1383, 1517);
+//        reply: the triple like 5, then per query: status count nrids rids
 //   8 nthreads reps nops (op na a[na] nb b[nb])[nops] -> times the reference's
 //        operators: each of nthreads threads builds its own operand copies,
 //        then runs its share of the ops (round robin) reps times, each as
@@ -31,6 +38,7 @@
 //        serialized result length in words
 #include "ibis.h"
 #include "irelic.h"
+#include "iapi.h"
 #include "bitvector.h"
 #include <cstdio>
 #include <cstdlib>
@@ -200,6 +208,40 @@ int main(int argc, char** argv) {
             pthread_barrier_destroy(&bar);
             fwrite(&mx, 8, 1, fout);
             for (uint32_t k = 0; k < nops; ++k) wr32(lens[k]);
+        } else if (kind == 9) {
+            uint32_t nrows = rd32();
+            std::vector<float> vals(nrows);
+            if (nrows && fread(&vals[0], 4, nrows, fin) != nrows) exit(3);
+            uint32_t nbins = rd32();
+            fastbit_iapi_register_array("x", FastBitDataTypeFloat, &vals[0], nrows);
+            char spec[128];
+            snprintf(spec, sizeof spec, "<binning nbins=%u equal_weight/>", nbins);
+            int ierr = fastbit_iapi_build_index("x", spec);
+            double* keys = 0; int64_t* offs = 0; uint32_t* bms = 0;
+            uint64_t nk = 0, no = 0, nb = 0;
+            if (ierr >= 0) ierr = fastbit_iapi_deconstruct_index("x", &keys, &nk, &offs, &no, &bms, &nb);
+            if (ierr < 0) { nk = no = nb = 0; }
+            wr32((uint32_t)nk); if (nk) fwrite(keys, 8, nk, fout);
+            wr32((uint32_t)no); if (no) fwrite(offs, 8, no, fout);
+            wr32((uint32_t)nb); if (nb) fwrite(bms, 4, nb, fout);
+            uint32_t nq = rd32();
+            for (uint32_t q = 0; q < nq; ++q) {
+                double lo = rdf64(), hi = rdf64();
+                FastBitSelectionHandle a = fastbit_selection_osr("x", FastBitCompareGreaterEqual, lo);
+                FastBitSelectionHandle b = fastbit_selection_osr("x", FastBitCompareLess, hi);
+                FastBitSelectionHandle c = fastbit_selection_combine(a, FastBitCombineAnd, b);
+                int64_t cnt = fastbit_selection_evaluate(c);
+                std::vector<uint32_t> rids;
+                if (cnt > 0) {
+                    std::vector<uint64_t> co(cnt);
+                    int64_t got = fastbit_selection_get_coordinates(c, &co[0], cnt, 0);
+                    for (int64_t i = 0; i < got; ++i) rids.push_back((uint32_t)co[i]);
+                }
+                wr32(cnt < 0 ? 1u : 0u); wr32((uint32_t)(cnt < 0 ? 0 : cnt)); wrv(rids);
+                fastbit_selection_free(c);
+            }
+            delete [] keys; delete [] offs; delete [] bms;
+            fastbit_iapi_free_all();
         } else {
             fprintf(stderr, "refdrv: unknown request %u\n", kind);
             return 4;

@@ -18,6 +18,12 @@ Outputs (all seeded, compressed .npz):
                     ranges lo <= x < hi: the index triple (keys, offsets,
                     bitmaps) from relic::write and hit counts + row ids from
                     relic::evaluate
+  bin_small.npz     bin index (<binning nbins=100 equal_weight/>) over
+                    200000 float32 values (70% normal(0,1), 30% Zipf(1.2)
+                    ranks) built through the in-memory C API, its triple from
+                    fastbit_iapi_deconstruct_index, and 30 ranges
+                    lo <= x < hi evaluated by the reference (counts and row
+                    ids from get_coordinates)
 """
 import os
 import sys
@@ -143,6 +149,27 @@ def main():
     np.savez_compressed(os.path.join(HERE, "relic_small.npz"), vals=vals, queries=np.array(qs),
                         keys=keys, offsets=offs, bitmaps=bms, counts=np.array(qc, np.uint64),
                         rids=fr, rids_off=orr)
+    # ---- bin, small
+    import struct
+    rng = np.random.default_rng(43)
+    n = 200000
+    z = rng.zipf(1.2, size=n) % 100000
+    vals = np.where(rng.random(n) < 0.7, rng.normal(size=n), z).astype(np.float32)
+    qv = np.sort(rng.choice(vals, size=60).astype(np.float64)).reshape(30, 2)
+    qv[:5, 0] -= 0.25  # a few ranges starting between values
+    req = (struct.pack("<II", 9, n) + vals.tobytes() + struct.pack("<II", 100, len(qv)) + qv.tobytes())
+    R = G.run_refdrv(oracle.REFDRV, [req], td)
+    nk = R.u32(); keys = np.frombuffer(R.d, np.float64, nk, R.p).copy(); R.p += 8 * nk
+    no = R.u32(); offs = np.frombuffer(R.d, np.int64, no, R.p).copy(); R.p += 8 * no
+    bms = R.vec()
+    qc, qr = [], []
+    for _ in range(len(qv)):
+        s_ = R.u32(); c = R.u32(); r = R.vec()
+        assert s_ == 0
+        qc.append(c); qr.append(r)
+    fr, orr = pack(qr)
+    np.savez_compressed(os.path.join(HERE, "bin_small.npz"), vals=vals, queries=qv, keys=keys, offsets=offs,
+                        bitmaps=bms, counts=np.array(qc, np.uint64), rids=fr, rids_off=orr)
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

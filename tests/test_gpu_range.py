@@ -1,0 +1,181 @@
+"""GPU parity of relic / bin range evaluation and of conjunctive queries,
+through the C ABI: hit counts and row ids against the reference's own
+answers (golden fixtures, and the reference library run through
+oracle/refdrv at the relic workload's full size) and against brute-force
+scans of the raw values."""
+import ctypes
+import struct
+import tempfile
+
+import numpy as np
+import pytest
+
+import oracle
+from oracle import wahgen as G
+from conftest import load_golden, unpack
+
+pytestmark = pytest.mark.gpu
+
+
+def _scan(vals, lo, hi):
+    v = vals.astype(np.float64)
+    return np.flatnonzero((v >= lo) & (v < hi)).astype(np.uint32)
+
+
+def _relic_ref(vals, queries):
+    """Reference relic over vals: triple, counts, row ids."""
+    with tempfile.TemporaryDirectory() as td:
+        R = G.run_refdrv(oracle.REFDRV, [G.req_relic(vals, queries)], td)
+        nk = R.u32(); keys = np.frombuffer(R.d, np.float64, nk, R.p).copy(); R.p += 8 * nk
+        no = R.u32(); offs = np.frombuffer(R.d, np.int64, no, R.p).copy(); R.p += 8 * no
+        bms = R.vec()
+        res = []
+        for _ in queries:
+            st = R.u32(); c = R.u32(); r = R.vec()
+            res.append((c, r))
+    return keys, offs, bms, res
+
+
+def _bin_ref(vals, nbins, queries):
+    req = (struct.pack("<II", 9, len(vals)) + np.ascontiguousarray(vals, np.float32).tobytes()
+           + struct.pack("<II", nbins, len(queries)) + np.asarray(queries, np.float64).reshape(-1, 2).tobytes())
+    with tempfile.TemporaryDirectory() as td:
+        R = G.run_refdrv(oracle.REFDRV, [req], td)
+        nk = R.u32(); keys = np.frombuffer(R.d, np.float64, nk, R.p).copy(); R.p += 8 * nk
+        no = R.u32(); offs = np.frombuffer(R.d, np.int64, no, R.p).copy(); R.p += 8 * no
+        bms = R.vec()
+        res = []
+        for _ in range(len(queries)):
+            st = R.u32(); c = R.u32(); r = R.vec()
+            res.append((c, r))
+    return keys, offs, bms, res
+
+
+def test_relic_small_golden(gpu_ctx):
+    import libfastlib_b200 as L
+    g = load_golden("relic_small.npz")
+    idx = L.Index(gpu_ctx, L.RELIC, len(g["vals"]), g["keys"], g["offsets"], g["bitmaps"], values=g["vals"])
+    for q, (lo, hi) in enumerate(g["queries"]):
+        n, rids, _ = L.evaluate(gpu_ctx, [idx.term(lo, hi)])
+        assert n == int(g["counts"][q])
+        assert np.array_equal(rids, unpack(g, "rids", q)), q
+
+
+def test_bin_small_golden(gpu_ctx):
+    import libfastlib_b200 as L
+    g = load_golden("bin_small.npz")
+    idx = L.Index(gpu_ctx, L.BIN, len(g["vals"]), g["keys"], g["offsets"], g["bitmaps"], values=g["vals"])
+    for q, (lo, hi) in enumerate(g["queries"]):
+        n, rids, _ = L.evaluate(gpu_ctx, [idx.term(lo, hi)])
+        assert n == int(g["counts"][q]), q
+        assert np.array_equal(rids, unpack(g, "rids", q)), q
+
+
+def test_relic_full_size_against_reference(gpu_ctx):
+    """1M-row uint32 column in [0,100), 100 seeded ranges lo <= x < hi, one
+    batch: counts and row ids equal the reference's relic::evaluate."""
+    import libfastlib_b200 as L
+    rng = np.random.default_rng(42)
+    vals = rng.integers(0, 100, size=1 << 20).astype(np.uint32)
+    qs = []
+    qrng = np.random.default_rng(7)
+    while len(qs) < 100:
+        lo, hi = (int(v) for v in qrng.integers(0, 101, size=2))
+        if lo < hi:
+            qs.append((float(lo), float(hi)))
+    keys, offs, bms, ref = _relic_ref(vals, qs)
+    idx = L.Index(gpu_ctx, L.RELIC, len(vals), keys, offs, bms, values=vals)
+    total = sum(c for c, _ in ref)
+    B = L.Batch(gpu_ctx, [[idx.term(lo, hi)] for lo, hi in qs], rid_cap=total)
+    B.run()
+    counts = B.counts()
+    for q, (c, r) in enumerate(ref):
+        assert int(counts[q]) == c, q
+        assert np.array_equal(B.rids(q, c), r), q
+
+
+def test_bin_reduced_against_reference(gpu_ctx):
+    """Binned index (1000 equal-weight bins) over a 2M-row float32 mixture
+    column; ranges spanning 1..500 bins with both edges inside bins."""
+    import libfastlib_b200 as L
+    rng = np.random.default_rng(3)
+    n = 2 << 20
+    z = rng.zipf(1.2, size=n) % 100000
+    vals = np.where(rng.random(n) < 0.7, rng.normal(size=n), z).astype(np.float32)
+    sv = np.sort(vals.astype(np.float64))
+    qs = []
+    for _ in range(40):
+        span = int(rng.integers(1, 501)) / 1000.0
+        a = float(rng.random()) * (1.0 - span)
+        lo = sv[int(a * (n - 1))] + 1e-4
+        hi = sv[int((a + span) * (n - 1))] - 1e-4
+        if lo < hi:
+            qs.append((lo, hi))
+    keys, offs, bms, ref = _bin_ref(vals, 1000, qs)
+    idx = L.Index(gpu_ctx, L.BIN, n, keys, offs, bms, values=vals)
+    for q, (lo, hi) in enumerate(qs):
+        cnt, rids, _ = L.evaluate(gpu_ctx, [idx.term(lo, hi)])
+        assert cnt == ref[q][0], q
+        assert np.array_equal(rids, ref[q][1]), q
+        assert np.array_equal(rids, _scan(vals, lo, hi)), q
+
+
+def test_conjunctions_and_batch_equal_scan(gpu_ctx):
+    """AND of 1-4 range terms over four 1M-row columns (two relic, two
+    bin), as one batch and one query at a time."""
+    import libfastlib_b200 as L
+    rng = np.random.default_rng(11)
+    n = 1 << 20
+    c0 = rng.integers(0, 1000, size=n).astype(np.uint32)
+    c1 = (rng.zipf(1.1, size=n) % 5000).astype(np.uint32)
+    c2 = rng.normal(size=n).astype(np.float32)
+    c3 = np.where(rng.random(n) < 0.7, rng.normal(size=n), rng.zipf(1.2, size=n) % 100000).astype(np.float32)
+    k0 = _relic_ref(c0, [])[:3]
+    k1 = _relic_ref(c1, [])[:3]
+    k2 = _bin_ref(c2, 512, [])[:3]
+    k3 = _bin_ref(c3, 256, [])[:3]
+    cols = [(c0, L.RELIC, k0), (c1, L.RELIC, k1), (c2, L.BIN, k2), (c3, L.BIN, k3)]
+    idxs = [L.Index(gpu_ctx, kind, n, *k, values=c) for c, kind, k in cols]
+    queries, specs = [], []
+    for _ in range(60):
+        cs = rng.choice(4, size=int(rng.integers(1, 5)), replace=False)
+        terms, spec = [], []
+        for ci in cs:
+            v = cols[ci][0].astype(np.float64)
+            lo, hi = np.sort(rng.choice(v, size=2))
+            if lo == hi:
+                hi = lo + 1
+            terms.append(idxs[ci].term(lo, hi))
+            spec.append((ci, lo, hi))
+        queries.append(terms)
+        specs.append(spec)
+    expect = []
+    for spec in specs:
+        m = np.ones(n, dtype=bool)
+        for ci, lo, hi in spec:
+            v = cols[ci][0].astype(np.float64)
+            m &= (v >= lo) & (v < hi)
+        expect.append(np.flatnonzero(m).astype(np.uint32))
+    B = L.Batch(gpu_ctx, queries, rid_cap=sum(len(e) for e in expect))
+    B.run()
+    counts = B.counts()
+    for q, e in enumerate(expect):
+        assert int(counts[q]) == len(e), q
+        assert np.array_equal(B.rids(q, len(e)), e), q
+    for q in range(0, 60, 7):
+        cnt, rids, _ = L.evaluate(gpu_ctx, queries[q])
+        assert cnt == len(expect[q]) and np.array_equal(rids, expect[q])
+
+
+def test_hit_bitvector_is_compressed_result(gpu_ctx):
+    """The hit bitvector of an evaluation holds the hit rows, in the words
+    compress() gives for them."""
+    import libfastlib_b200 as L
+    g = load_golden("relic_small.npz")
+    idx = L.Index(gpu_ctx, L.RELIC, len(g["vals"]), g["keys"], g["offsets"], g["bitmaps"], values=g["vals"])
+    n, rids, hits = L.evaluate(gpu_ctx, [idx.term(10, 60)], want_hits=True)
+    assert hits.size() == len(g["vals"])
+    assert hits.cnt() == n
+    assert np.array_equal(hits.rids(), rids)
+    dense = oracle.decompress(hits.write())
+    assert np.array_equal(oracle.compress(dense)[0], hits.write())

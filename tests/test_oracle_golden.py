@@ -65,3 +65,12 @@ def test_relic_small_hits_match_scan():
                              out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), ctypes.c_uint64(len(vals)))
         assert n == int(g["counts"][q])
         assert np.array_equal(out[:n], unpack(g, "rids", q))
+
+
+def test_bin_small_hits_match_scan():
+    g = load_golden("bin_small.npz")
+    v = g["vals"].astype(np.float64)
+    for q, (lo, hi) in enumerate(g["queries"]):
+        e = np.flatnonzero((v >= lo) & (v < hi))
+        assert len(e) == int(g["counts"][q])
+        assert np.array_equal(e, unpack(g, "rids", q))

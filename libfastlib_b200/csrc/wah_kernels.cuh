@@ -200,7 +200,11 @@ k_rids(const uint32_t* __restrict__ w, uint32_t n, const uint32_t* __restrict__ 
                 const uint32_t c = x & MAXCNT;
                 if (x >= HEADER1) {
                     const uint32_t slot = atomicAdd(&fq_n, 1u);
-                    fq_off[slot] = off; fq_row[slot] = g * 31u; fq_len[slot] = c * 31u;
+                    if (slot < (uint32_t)(SCAN_TILE / 2)) {
+                        fq_off[slot] = off; fq_row[slot] = g * 31u; fq_len[slot] = c * 31u;
+                    } else {  // list full: this thread writes the fill
+                        for (uint32_t r = 0; r < c * 31u; ++r) if (off + r < cap) out[off + r] = g * 31u + r;
+                    }
                     off += (uint64_t)c * 31u;
                 }
                 g += c;
@@ -217,8 +221,9 @@ k_rids(const uint32_t* __restrict__ w, uint32_t n, const uint32_t* __restrict__ 
         }
     }
     __syncthreads();
-    // the CTA writes every 1-fill of the tile cooperatively
-    for (uint32_t k = 0; k < fq_n; ++k) {
+    // the CTA writes every listed 1-fill of the tile cooperatively
+    const uint32_t nfq = min(fq_n, (uint32_t)(SCAN_TILE / 2));
+    for (uint32_t k = 0; k < nfq; ++k) {
         const uint64_t o = fq_off[k];
         const uint32_t r0 = fq_row[k], len = fq_len[k];
         for (uint32_t r = threadIdx.x; r < len; r += SCAN_THREADS)
@@ -245,8 +250,13 @@ k_decompress(const uint32_t* __restrict__ w, uint32_t n, const uint32_t* __restr
             const uint32_t x = __ldg(w + base + q);
             if (x > ALLONES) {
                 const uint32_t c = x & MAXCNT;
+                const uint32_t val = (x >= HEADER1) ? ALLONES : 0u;
                 const uint32_t slot = atomicAdd(&fq_n, 1u);
-                fq_pos[slot] = g; fq_len[slot] = c; fq_val[slot] = (x >= HEADER1) ? ALLONES : 0u;
+                if (slot < (uint32_t)(SCAN_TILE / 2)) {
+                    fq_pos[slot] = g; fq_len[slot] = c; fq_val[slot] = val;
+                } else {  // list full: this thread writes the fill
+                    for (uint32_t r = 0; r < c; ++r) out[g + r] = val;
+                }
                 g += c;
             } else {
                 out[g] = x;
@@ -255,7 +265,8 @@ k_decompress(const uint32_t* __restrict__ w, uint32_t n, const uint32_t* __restr
         }
     }
     __syncthreads();
-    for (uint32_t k = 0; k < fq_n; ++k) {
+    const uint32_t nfq = min(fq_n, (uint32_t)(SCAN_TILE / 2));
+    for (uint32_t k = 0; k < nfq; ++k) {
         const uint32_t p = fq_pos[k], len = fq_len[k], val = fq_val[k];
         for (uint32_t r = threadIdx.x; r < len; r += SCAN_THREADS) out[p + r] = val;
     }

@@ -285,7 +285,6 @@ __global__ void k_index_tiles(const uint32_t* __restrict__ words, BitmapMeta* __
     const uint32_t* w = words + m.wstart;
     uint32_t* tix = tiles + (size_t)b * (ntiles + 1) * 2;
     uint32_t carry = 0, ones = 0, bad = 0;
-    uint32_t next_t = 0;  // next tile boundary not yet recorded
     for (uint32_t base = 0; base < m.n; base += 32) {
         const uint32_t i = base + lane;
         const bool in = i < m.n;
@@ -307,7 +306,6 @@ __global__ void k_index_tiles(const uint32_t* __restrict__ words, BitmapMeta* __
         }
         carry += __shfl_sync(0xffffffffu, x, 31);
     }
-    (void)next_t;
     // boundaries at or past the end of the words
     for (uint32_t t = lane; t <= ntiles; t += 32) {
         if ((uint64_t)t * RT >= carry) { tix[2 * t] = m.n; tix[2 * t + 1] = carry; }

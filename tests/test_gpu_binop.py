@@ -113,3 +113,15 @@ def test_rids_large(gpu_ctx):
     a = oracle.build_runs(G.geometric_runs(3, nbits, 0.3, mean1=200.0))
     A = gpu_ctx.bitvector(a)
     assert np.array_equal(A.rids(), oracle.rids(a))
+
+
+def test_many_one_fills_per_tile(gpu_ctx):
+    """Row ids and decompress of words that are all 1-fills (more per 4096-word
+    tile than the kernels' shared fill list holds)."""
+    words = [0xC0000002] * 9000 + [0x12345, 0x80000003] * 500
+    a = G.serialize(words, 5, 0b10110)
+    A = gpu_ctx.bitvector(a)
+    assert np.array_equal(A.rids(), oracle.rids(a))
+    B = gpu_ctx.bitvector(a)
+    B.decompress()
+    assert np.array_equal(B.write(), oracle.decompress(a))

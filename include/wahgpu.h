@@ -193,6 +193,25 @@ int64_t wahgpu_batch_rids(wahgpu_batch* batch, uint32_t q, uint32_t* out, uint64
 const uint32_t* wahgpu_batch_device_rids(wahgpu_batch* batch);
 int wahgpu_batch_free(wahgpu_batch* batch);
 
+/* ---- allocation-free row ids -------------------------------------------
+ * No counterpart in the reference: an addition for callers that cannot
+ * allocate device memory while they run — code issuing work during CUDA
+ * graph capture (cudaMalloc is not allowed there), pipelines driven from
+ * host callbacks, and runtimes that own all device memory through their own
+ * pool.  Computes the ascending row ids of the serialized bitvector at
+ * dev_serial (nwords words in device memory, the write(array_t&) layout)
+ * into dev_rids (room for cap ids) and its count into *dev_count (device
+ * memory; UINT64_MAX if a device-side wait gave up), on `stream`, without
+ * allocating anything: its scratch is a fixed area of about 197 KiB
+ * compiled into the library, held by every device that loads it.
+ * Limit: at most 16,777,216 whole words (WAHGPU_ESIZE beyond).  The first
+ * call on a device looks up the scratch area's device address
+ * (cudaGetSymbolAddress) — make it before any stream capture.  All calls
+ * share the scratch area: calls whose kernels overlap on the GPU race, so
+ * order them (one stream).  Errors: wahgpu_last_error(NULL). */
+int wahgpu_rids_noalloc(const uint32_t* dev_serial, uint64_t nwords, uint32_t* dev_rids,
+                        uint64_t cap, unsigned long long* dev_count, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

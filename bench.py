@@ -226,6 +226,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--dense-tile", type=int, default=2048, choices=[1024, 2048, 4096],
+                    help="groups per tile of the dense-path kernel")
     ap.add_argument("--only", default=None,
                     help="OP:DENSITY, e.g. '&:0.5' — one operator on one pair, no e2e / CPU legs (for ncu)")
     args = ap.parse_args()
@@ -254,6 +256,7 @@ def main():
         pairs = [pairs[keep]]
         OPS[:] = [OPNAMES.index(op_s)]
     ctx = L.Context(local)
+    ctx.set_tuning(L.TUNE_DENSE_TILE, args.dense_tile)
     # a dedicated stream: the legacy default stream (handle 0) cannot be
     # handed to the library, which treats NULL as "its own stream"
     stream = torch.cuda.Stream()

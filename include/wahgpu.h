@@ -67,6 +67,13 @@ const char* wahgpu_last_error(wahgpu_ctx* ctx);
 /* Number of kernels this context has launched (diagnostics). */
 int64_t wahgpu_ctx_launches(wahgpu_ctx* ctx);
 
+/* Launch-shape knobs, set by an autotuner (no counterpart in the reference;
+ * results never depend on them).  Values outside the listed set are
+ * rejected with WAHGPU_EINVAL. */
+#define WAHGPU_TUNE_DENSE_TILE 1  /* groups per tile of the dense-path kernel: 1024 | 2048 | 4096 */
+int wahgpu_ctx_set_tuning(wahgpu_ctx* ctx, int key, int64_t value);
+int64_t wahgpu_ctx_get_tuning(wahgpu_ctx* ctx, int key);
+
 /* ---- bitvectors ------------------------------------------------------- */
 /* Builds a device bitvector from a serialized host array, like the
  * reference's constructor from array_t<word_t> (src/bitvector.cpp:54-105):

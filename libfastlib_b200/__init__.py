@@ -49,6 +49,8 @@ class _Term(ctypes.Structure):
 
 
 RELIC, BIN = 1, 2
+TUNE_DENSE_TILE = 1
+DENSE_TILES = (1024, 2048, 4096)
 CMP_NONE, CMP_LT, CMP_LE = 0, 1, 2
 U32, F32, I32 = 0, 1, 2
 
@@ -75,6 +77,8 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "wahgpu_ctx_sync": (ctypes.c_int, [P]),
         "wahgpu_last_error": (ctypes.c_char_p, [P]),
         "wahgpu_ctx_launches": (ctypes.c_int64, [P]),
+        "wahgpu_ctx_set_tuning": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int64]),
+        "wahgpu_ctx_get_tuning": (ctypes.c_int64, [P, ctypes.c_int]),
         "wahgpu_bv_from_serial": (ctypes.c_int, [P, U32P, ctypes.c_uint64, ctypes.POINTER(P)]),
         "wahgpu_bv_from_device_serial": (ctypes.c_int, [P, P, ctypes.c_uint64, ctypes.POINTER(P)]),
         "wahgpu_bv_create": (ctypes.c_int, [P, ctypes.c_uint64, ctypes.POINTER(P)]),
@@ -144,6 +148,13 @@ class Context:
     @property
     def launches(self) -> int:
         return int(self.lib.wahgpu_ctx_launches(self.h))
+
+    def set_tuning(self, key: int, value: int) -> None:
+        """Launch-shape knob (TUNE_DENSE_TILE); results never depend on it."""
+        self.check(self.lib.wahgpu_ctx_set_tuning(self.h, key, value))
+
+    def get_tuning(self, key: int) -> int:
+        return self.check(int(self.lib.wahgpu_ctx_get_tuning(self.h, key)))
 
     def close(self) -> None:
         """Frees every bitvector still alive on this context, then the

@@ -8,6 +8,7 @@
 #include "wah_api_internal.h"
 
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdio>
 #include <cstdarg>
 #include <cstring>
@@ -84,7 +85,8 @@ int wg_scratch(wahgpu_ctx* ctx, uint32_t ntiles, TileRec** recs, LaunchSync** sy
         CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
         if (ctx->scratch) cudaFree(ctx->scratch);
         ctx->scratch = nullptr;
-        size_t bytes = sizeof(LaunchSync) * 2 + (size_t)want * sizeof(TileRec);
+        // sync words, TileRec records, then the dense kernel's 16-byte records
+        size_t bytes = sizeof(LaunchSync) * 2 + (size_t)want * (sizeof(TileRec) + sizeof(uint4));
         if (cudaMalloc(&ctx->scratch, bytes) != cudaSuccess) {
             cudaGetLastError();
             ctx->scratch_tiles = 0;
@@ -96,6 +98,10 @@ int wg_scratch(wahgpu_ctx* ctx, uint32_t ntiles, TileRec** recs, LaunchSync** sy
     *sync = reinterpret_cast<LaunchSync*>(ctx->scratch);
     *recs = reinterpret_cast<TileRec*>(reinterpret_cast<char*>(ctx->scratch) + 2 * sizeof(LaunchSync));
     return WAHGPU_OK;
+}
+// The dense kernel's records, after the TileRec array of the scratch block.
+static uint4* wg_dense_recs(wahgpu_ctx* ctx, TileRec* recs) {
+    return reinterpret_cast<uint4*>(recs + ctx->scratch_tiles);
 }
 
 // ------------------------------------------------------------------ context
@@ -150,6 +156,25 @@ extern "C" int wahgpu_ctx_set_stream(wahgpu_ctx* ctx, void* stream) {
     if (!ctx) return WAHGPU_EINVAL;
     ctx->stream = stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->own_stream;
     return WAHGPU_OK;
+}
+extern "C" int wahgpu_ctx_set_tuning(wahgpu_ctx* ctx, int key, int64_t value) {
+    if (!ctx) return WAHGPU_EINVAL;
+    switch (key) {
+    case WAHGPU_TUNE_DENSE_TILE:
+        if (value != 1024 && value != 2048 && value != 4096)
+            return wg_fail(ctx, WAHGPU_EINVAL, "dense tile must be 1024, 2048 or 4096 groups, not %lld", (long long)value);
+        ctx->dense_tile = (uint32_t)value;
+        return WAHGPU_OK;
+    default:
+        return wg_fail(ctx, WAHGPU_EINVAL, "unknown tuning key %d", key);
+    }
+}
+extern "C" int64_t wahgpu_ctx_get_tuning(wahgpu_ctx* ctx, int key) {
+    if (!ctx) return WAHGPU_EINVAL;
+    switch (key) {
+    case WAHGPU_TUNE_DENSE_TILE: return ctx->dense_tile;
+    default: return wg_fail(ctx, WAHGPU_EINVAL, "unknown tuning key %d", key);
+    }
 }
 extern "C" void* wahgpu_ctx_stream(wahgpu_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 extern "C" int wahgpu_ctx_sync(wahgpu_ctx* ctx) {
@@ -439,17 +464,26 @@ static int wg_gtile(wahgpu_bv* b) {
     return WAHGPU_OK;
 }
 
-template <int OP>
-static void launch_dense_op(dim3 g, size_t sm, cudaStream_t s, const DenseArgs& a) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_dense<OP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        attr = true;
+template <int OP, int TG, int NCW>
+static void launch_dense_op(const wahgpu_ctx* ctx, uint32_t ntiles, cudaStream_t s, const DenseArgs& a) {
+    static int per_sm = 0;
+    const size_t sm = sizeof(DShared<TG, NCW>);
+    if (!per_sm) {
+        cudaFuncSetAttribute(k_dense<OP, TG, NCW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense<OP, TG, NCW>, (NCW + 1) * 32, sm);
+        if (per_sm < 1) per_sm = 1;
     }
-    k_dense<OP><<<g, DTHREADS, sm, s>>>(a);
+    // persistent: at most one wave of resident CTAs
+    const uint32_t grid = std::min<uint32_t>(ntiles, (uint32_t)(per_sm * ctx->sm_count));
+    k_dense<OP, TG, NCW><<<grid, (NCW + 1) * 32, sm, s>>>(a);
+}
+template <int OP>
+static void launch_dense_tg(const wahgpu_ctx* ctx, uint32_t tg, uint32_t ntiles, cudaStream_t s, const DenseArgs& a) {
+    if (tg == 1024) launch_dense_op<OP, 1024, 4>(ctx, ntiles, s, a);
+    else if (tg == 4096) launch_dense_op<OP, 4096, 8>(ctx, ntiles, s, a);
+    else launch_dense_op<OP, 2048, 8>(ctx, ntiles, s, a);
 }
 
-// Canonical-result operators over dense operands: group-space tiles.
 int wg_launch_dense(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t groups,
                     uint32_t anb, uint32_t aval, wahgpu_bv* res) {
     int rc = bv_reserve(res, (uint64_t)x->h.n + y->h.n);
@@ -458,7 +492,8 @@ int wg_launch_dense(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_
     if (rc) return rc;
     rc = wg_gtile(y);
     if (rc) return rc;
-    const uint32_t ntiles = (groups + DT - 1) / DT;
+    const uint32_t tg = ctx->dense_tile;
+    const uint32_t ntiles = (groups + tg - 1) / tg;
     TileRec* recs; LaunchSync* sync;
     rc = wg_scratch(ctx, ntiles, &recs, &sync);
     if (rc) return rc;
@@ -467,16 +502,14 @@ int wg_launch_dense(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_
     a.yw = y->words; a.ygt = y->gt; a.ny = y->h.n;
     a.groups = groups;
     a.out = res->words; a.obp = res->bpos; a.meta = res->meta;
-    a.recs = recs; a.sync = sync; a.ntiles = ntiles;
+    a.drecs = wg_dense_recs(ctx, recs); a.sync = sync; a.ntiles = ntiles;
     a.aval = aval; a.anb = anb;
     CUDA_TRY(ctx, cudaMemsetAsync(res->meta, 0, sizeof(DevMeta), ctx->stream));
-    const size_t sm = sizeof(DenseShared);
-    dim3 g(ntiles);
     switch (op) {
-    case OP_AND: launch_dense_op<OP_AND>(g, sm, ctx->stream, a); break;
-    case OP_OR: launch_dense_op<OP_OR>(g, sm, ctx->stream, a); break;
-    case OP_XOR: launch_dense_op<OP_XOR>(g, sm, ctx->stream, a); break;
-    default: launch_dense_op<OP_MINUS>(g, sm, ctx->stream, a); break;
+    case OP_AND: launch_dense_tg<OP_AND>(ctx, tg, ntiles, ctx->stream, a); break;
+    case OP_OR: launch_dense_tg<OP_OR>(ctx, tg, ntiles, ctx->stream, a); break;
+    case OP_XOR: launch_dense_tg<OP_XOR>(ctx, tg, ntiles, ctx->stream, a); break;
+    default: launch_dense_tg<OP_MINUS>(ctx, tg, ntiles, ctx->stream, a); break;
     }
     ctx->launches++;
     CUDA_TRY(ctx, cudaGetLastError());

@@ -24,6 +24,7 @@ struct wahgpu_ctx {
     uint32_t scratch_tiles = 0;
     void* h_meta_stage = nullptr;  // pinned staging for metadata reads
     uint64_t launches = 0;
+    uint32_t dense_tile = 2048;         // WAHGPU_TUNE_DENSE_TILE
 };
 
 struct wahgpu_bv {

@@ -6,38 +6,80 @@
 // the operands hold more words than half their groups (the _d2 rule
 // (|a|+|b|)*31 > nbits) or one operand is uncompressed, i.e. for dense data.
 //
-// Tile t covers groups [t*DT, (t+1)*DT).  Its operands' words come from the
-// group-tile index gtile[k] = (index, first group) of the word covering group
-// k*DT, so no search is needed.  An operand whose words over the tile are one
-// per group ("pure") is read straight from global memory, lane = group;
-// otherwise it is first expanded into shared memory (fills longer than 32
-// groups are written by the whole CTA).  Each warp then walks 32 groups per
-// step: the elementwise result, its class, run heads by ballot, head indices
-// by popcount.  A run's word is written by the lane holding the next head
-// (its length is only known there) — consecutive indices, so the stores of a
-// warp are coalesced.  Head counts and the last run cross warps and tiles
-// through a block scan and the decoupled look-back of the merge kernel.
+// Structure: a persistent, warp-specialised pipeline.  Each CTA runs one
+// control warp and NCW compute warps.
+//
+//  * The control warp claims tiles of TG groups in order (atomic ticket),
+//    finds each tile's word ranges in the group-tile index, and prefetches
+//    the words of both operands into a ring of NI shared-memory slots with
+//    bulk copies (cp.async.bulk) that complete on the slot's mbarrier.  It
+//    also runs the decoupled look-back for every claimed tile as soon as the
+//    predecessors' records appear, so a tile's prefix is usually known
+//    before its words are even consumed.
+//  * The compute warps take the slots in order.  For an operand whose words
+//    over the tile are one per group ("pure") the patterns are read straight
+//    from the slot; otherwise each thread scans a contiguous run of words,
+//    a block scan places them, and a marker per word start plus one cover
+//    entry per 128-group step let every lane find the word of each of its
+//    groups by a warp max-scan — no loop over fill lengths.  Pass 1 gives
+//    per group the result, its class and the run heads (4 consecutive
+//    groups per lane; a step of 128 mixed results takes a branch-free
+//    path), kept in shared memory with the tile's aggregate (heads, last
+//    head, popcount), which is published as the tile's look-back record.
+//  * Pass 2 of a tile runs one tile later, after pass 1 of the next one, so
+//    the control warp's look-back has had a whole tile of time.  The lane of
+//    each head writes the word of the run before it (a uniform run's length
+//    is only known there) and, for a mixed group, its own literal.
+//
+// Every wait is bounded (WAIT_LIMIT_NS without progress); a timeout sets the
+// result's status word and all warps leave the pipeline.
 #ifndef WAH_DENSE_CUH
 #define WAH_DENSE_CUH
 #include "wah_merge.cuh"
 
 namespace wah {
 
-constexpr int DT = 2048;                  // groups per tile
-constexpr int DTHREADS = 128;
-constexpr int DWARPS = DTHREADS / 32;
-constexpr int DGPW = DT / DWARPS;         // 512 groups per warp
-constexpr int DSTEPS = DGPW / 32;         // 16 steps of 32 groups
-constexpr int DFILL_MAX = DT / 32 + 2;    // long fills per operand and tile
+constexpr int DT = 1024;                  // group-tile index stride (k_gtile)
+constexpr uint32_t DEND = 0xFFFFFFFFu;    // slot marker: no more tiles
+constexpr uint32_t DFAST = 0xFFFFFFFFu;   // step code: 128 mixed literals
 
-struct DenseShared {
-    uint32_t d[2][DT];      // expanded patterns of impure operands
-    uint32_t fl_pos[2][DFILL_MAX], fl_len[2][DFILL_MAX], fl_val[2][DFILL_MAX];
-    uint32_t fl_n[2];
-    uint32_t wsum[2][DWARPS];
-    uint32_t warp_agg[DWARPS][4];
-    uint32_t tile_prefix[4];
-    uint32_t hdr[8];
+template <int TG, int NCW>
+struct DCfg {
+    static constexpr int NI = 3;                  // prefetch slots
+    static constexpr int NP = NI + 2;             // prefix slots (tiles claimed ahead of pass 2)
+    static constexpr int CT = NCW * 32;           // compute threads
+    static constexpr int GPW = TG / NCW;          // groups per compute warp
+    static constexpr int STEPS = GPW / 128;       // steps of 4 groups per lane
+    static constexpr int NSTEP = TG / 128;        // steps per tile
+    static constexpr int BUFW = TG + 8;           // words per operand slot
+    static constexpr int WPT = ((TG + CT - 1) / CT) | 1;  // words per thread when expanding (odd)
+    static_assert(TG % DT == 0 && GPW % 128 == 0 && STEPS >= 1, "tile shape");
+};
+
+// Tile words as the control warp found them (indices into the slot buffer).
+struct DSlot {
+    uint32_t t, g0, ng, flags;                    // flags: 1 x pure, 2 y pure
+    uint32_t xlo, xhi, xs0, xprev;                // words [xlo, xhi) = [xi0, xi1); xs0 first group of xi0
+    uint32_t ylo, yhi, ys0, yprev;                // xprev: the word covering g0-1
+};
+
+template <int TG, int NCW>
+struct DShared {
+    using C = DCfg<TG, NCW>;
+    uint4 in[C::NI][2][C::BUFW / 4];              // prefetched words
+    uint4 res[2][TG / 4];                         // pass-1 results of the last two tiles
+    uint32_t code[2][C::NSTEP * 32];              // head flags | classes per lane and step, or DFAST
+    uint16_t mk[2][TG];                           // expansion: buffer index + 1 of the word starting here
+    uint32_t cov[2][C::NSTEP];                    // expansion: buffer index of the word covering step q
+    uint32_t xsum[2][NCW];
+    DSlot slot[C::NI];
+    uint4 prefix[C::NP];                          // look-back result per claimed tile
+    uint32_t lbt[C::NP];                          // tile of each claim awaiting its look-back (control)
+    uint4 wagg[2][NCW];                           // warp aggregates, then warp exclusive prefixes
+    uint4 tagg[2];                                // tile aggregate
+    uint32_t tinfo[2][4];                         // tile, g0, ng
+    uint64_t full[C::NI], empty[C::NI], pre[C::NP];
+    uint32_t epoch, abort, ok;
 };
 
 // Group-tile index of a bitvector: gt[2k] = index of the word covering group
@@ -67,342 +109,626 @@ struct DenseArgs {
     const uint32_t* yw; const uint32_t* ygt; uint32_t ny;
     uint32_t groups;
     uint32_t* out; uint32_t* obp; DevMeta* meta;
-    TileRec* recs; LaunchSync* sync; uint32_t ntiles;
+    uint4* drecs; LaunchSync* sync; uint32_t ntiles;
     uint32_t aval, anb;
 };
 
-// Expansion of impure operands in two halves so that the words of both
-// operands are requested in one batch: dense_load fetches a warp's chunk of
-// words [i0, i1) into registers and sums its groups; dense_place (after one
-// block barrier) writes the 31-bit patterns at their positions in S.d[side],
-// restricted to the tile [g0, g1).
-constexpr int DKMAX = (DT + 2 + DWARPS * 32 - 1) / (DWARPS * 32) + 1;  // words per lane
-struct Chunk {
-    uint32_t v[DKMAX];
-    uint32_t c0, c1;
-};
-__device__ __forceinline__ void dense_load(DenseShared& S, int side, const uint32_t* __restrict__ w,
-                                           uint32_t i0, uint32_t i1, Chunk& ch) {
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const uint32_t nw = i1 - i0;
-    const uint32_t chunk = ((nw + DWARPS - 1) / DWARPS + 31u) & ~31u;
-    ch.c0 = i0 + warp * chunk;
-    ch.c1 = min(ch.c0 + chunk, i1);
+// ---- tile aggregates: {popc, nheads | cls << 28 | has << 30, pos, -}.
+// The look-back record of tile t is drecs[t] = {popc, nheads|cls|has,
+// pos | state << 28, epoch}, written and read as one 16-byte access so that
+// a record is never seen half written; records of earlier launches carry an
+// older epoch.
+__device__ __forceinline__ uint4 dagg_comb(uint4 a, uint4 b) {  // a before b
+    const bool hb = (b.y >> 30) & 1u;
+    uint4 r;
+    r.x = a.x + b.x;
+    r.y = ((a.y & 0x0FFFFFFFu) + (b.y & 0x0FFFFFFFu)) | ((hb ? b.y : a.y) & 0x70000000u);
+    r.z = hb ? b.z : a.z;
+    r.w = 0;
+    return r;
+}
+__device__ __forceinline__ uint4 dagg_make(uint32_t nheads, uint32_t popc, uint32_t pos, uint32_t cls, bool has) {
+    return make_uint4(popc, nheads | (cls << 28) | (has ? (1u << 30) : 0u), pos, 0u);
+}
+__device__ __forceinline__ uint32_t dagg_n(uint4 a) { return a.y & 0x0FFFFFFFu; }
+__device__ __forceinline__ uint32_t dagg_cls(uint4 a) { return (a.y >> 28) & 3u; }
+__device__ __forceinline__ bool dagg_has(uint4 a) { return (a.y >> 30) & 1u; }
+__device__ __forceinline__ void drec_publish(uint4* recs4, uint32_t t, uint32_t epoch, uint32_t state, uint4 a) {
+    st_cg4(recs4 + t, make_uint4(a.x, a.y, a.z | (state << 28), epoch));
+}
+
+// One step of the warp-wide look-back: reads the records of up to 32 tiles
+// before `hi`; if every one of them up to the nearest inclusive record is
+// present, folds them into acc and moves hi.  Returns 2 when the prefix is
+// complete, 1 when a window was consumed, 0 when a record is not there yet.
+__device__ __forceinline__ int dlook_step(const uint4* recs4, uint32_t epoch, uint32_t& hi, uint4& acc) {
+    const uint32_t lane = threadIdx.x & 31u;
+    if (hi == 0) return 2;
+    const int64_t p = (int64_t)hi - 1 - lane;
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    bool valid = true, incl = true;
+    if (p >= 0) {
+        const uint4 r = ld_cg4(recs4 + p);
+        const uint32_t st = (r.z >> 28) & 3u;
+        valid = r.w == epoch && (st == REC_AGG || st == REC_INCL);
+        incl = valid && st == REC_INCL;
+        v = make_uint4(r.x, r.y, r.z & 0x0FFFFFFFu, 0u);
+    }
+    const uint32_t im = __ballot_sync(0xffffffffu, incl);
+    const uint32_t vm = __ballot_sync(0xffffffffu, valid);
+    const uint32_t L = im ? (uint32_t)(__ffs(im) - 1) : 31u;
+    const uint32_t need = L == 31u ? 0xffffffffu : ((2u << L) - 1u);
+    if ((vm & need) != need) return 0;
+    if (lane > L) v = make_uint4(0u, 0u, 0u, 0u);
+    // ordered tree: lane l ends up with lanes [l, 31] combined, higher lanes
+    // being earlier tiles
 #pragma unroll
-    for (int k = 0; k < DKMAX; ++k) {
-        const uint32_t i = ch.c0 + k * 32 + lane;
-        ch.v[k] = i < ch.c1 ? __ldg(w + i) : 0u;
+    for (int d = 1; d < 32; d <<= 1) {
+        uint4 o;
+        o.x = __shfl_down_sync(0xffffffffu, v.x, d);
+        o.y = __shfl_down_sync(0xffffffffu, v.y, d);
+        o.z = __shfl_down_sync(0xffffffffu, v.z, d);
+        o.w = 0;
+        if (lane + d < 32u) v = dagg_comb(o, v);
+    }
+    uint4 win;
+    win.x = __shfl_sync(0xffffffffu, v.x, 0);
+    win.y = __shfl_sync(0xffffffffu, v.y, 0);
+    win.z = __shfl_sync(0xffffffffu, v.z, 0);
+    win.w = 0;
+    acc = dagg_comb(win, acc);
+    if (im) { hi = 0; return 2; }
+    hi = hi > 32u ? hi - 32u : 0u;
+    return hi == 0 ? 2 : 1;
+}
+
+__device__ __forceinline__ void dense_fail(const DenseArgs& A, volatile uint32_t* abort) {
+    atomicExch(&A.meta->status, DEV_ERR_TIMEOUT);
+    *abort = 1u;
+}
+
+// Bounded wait that also gives up when another warp has aborted.
+__device__ __forceinline__ bool dwait(uint64_t* b, uint32_t par, volatile uint32_t* abort) {
+    if (mbar_test(b, par)) return true;
+    const uint64_t t0 = gtimer();
+    uint32_t ns = 32;
+    while (!mbar_test(b, par)) {
+        if (*abort) return false;
+        __nanosleep(ns);
+        if (ns < 256) ns <<= 1;
+        if (gtimer() - t0 > WAIT_LIMIT_NS) return false;
+    }
+    return true;
+}
+
+// ------------------------------------------------------------- control warp
+template <int TG, int NCW>
+__device__ __forceinline__ void dense_control(DShared<TG, NCW>& S, const DenseArgs& A, uint32_t epoch) {
+    using C = DCfg<TG, NCW>;
+    const uint32_t lane = threadIdx.x & 31u;
+    volatile uint32_t* abort = &S.abort;
+    const uint4* recs4 = A.drecs;
+    const uint32_t G = A.groups;
+    const uint32_t nt = (G + DT - 1) / DT;
+    uint32_t seq_claim = 0, n_real = 0, seq_lb = 0;
+    bool ended = false, lb_active = false;
+    uint32_t lb_hi = 0;
+    uint4 lb_acc = make_uint4(0u, 0u, 0u, 0u);
+    uint64_t last = gtimer();
+    uint32_t ns = 32;
+    // every branch below is taken by the whole warp: lane 0 decides
+    while (true) {
+        if (__shfl_sync(0xffffffffu, *abort, 0)) break;
+        bool progress = false;
+        // 1) claim the next tile and prefetch its words into a free slot
+        if (!ended && seq_claim < seq_lb + (uint32_t)C::NP) {
+            const uint32_t s = seq_claim % C::NI, u = seq_claim / C::NI;
+            const bool free_slot = __shfl_sync(0xffffffffu, (u == 0 || mbar_test(&S.empty[s], (u - 1u) & 1u)) ? 1u : 0u, 0);
+            if (free_slot) {
+                uint32_t t = 0;
+                if (lane == 0) t = atomicAdd(&A.sync->ticket, 1u);
+                t = __shfl_sync(0xffffffffu, t, 0);
+                if (t >= A.ntiles) {
+                    if (lane == 0) { S.slot[s].t = DEND; mbar_arrive(&S.full[s]); }
+                    ended = true;
+                } else {
+                    const uint32_t k0 = t * (uint32_t)(TG / DT), k1 = min(k0 + (uint32_t)(TG / DT), nt);
+                    uint2 e = make_uint2(0u, 0u);
+                    if (lane < 4) {
+                        const uint32_t* gt = (lane < 2) ? A.xgt : A.ygt;
+                        e = __ldg(reinterpret_cast<const uint2*>(gt) + ((lane & 1u) ? k1 : k0));
+                    }
+                    const uint32_t xi0 = __shfl_sync(0xffffffffu, e.x, 0), xs0 = __shfl_sync(0xffffffffu, e.y, 0);
+                    const uint32_t xn1 = __shfl_sync(0xffffffffu, e.x, 1), xg1 = __shfl_sync(0xffffffffu, e.y, 1);
+                    const uint32_t yi0 = __shfl_sync(0xffffffffu, e.x, 2), ys0 = __shfl_sync(0xffffffffu, e.y, 2);
+                    const uint32_t yn1 = __shfl_sync(0xffffffffu, e.x, 3), yg1 = __shfl_sync(0xffffffffu, e.y, 3);
+                    if (lane == 0) {
+                        const uint32_t g0 = t * (uint32_t)TG, g1 = min(g0 + (uint32_t)TG, G), ng = g1 - g0;
+                        const uint32_t xi1 = min(xg1 == g1 ? xn1 : xn1 + 1u, A.nx);
+                        const uint32_t yi1 = min(yg1 == g1 ? yn1 : yn1 + 1u, A.ny);
+                        // copies start at the word covering g0-1 when that is not
+                        // the tile's first word, rounded down to 16 bytes
+                        const uint32_t xcs = ((g0 > 0 && xs0 == g0) ? xi0 - 1u : xi0) & ~3u;
+                        const uint32_t ycs = ((g0 > 0 && ys0 == g0) ? yi0 - 1u : yi0) & ~3u;
+                        const uint32_t xb = ((xi1 - xcs + 3u) & ~3u) * 4u, yb = ((yi1 - ycs + 3u) & ~3u) * 4u;
+                        DSlot& m = S.slot[s];
+                        m.t = t; m.g0 = g0; m.ng = ng;
+                        m.flags = ((xs0 == g0 && xg1 == g1 && xn1 - xi0 == ng) ? 1u : 0u) |
+                                  ((ys0 == g0 && yg1 == g1 && yn1 - yi0 == ng) ? 2u : 0u);
+                        m.xlo = xi0 - xcs; m.xhi = xi1 - xcs; m.xs0 = xs0;
+                        m.xprev = g0 == 0 ? 0u : (xs0 < g0 ? m.xlo : m.xlo - 1u);
+                        m.ylo = yi0 - ycs; m.yhi = yi1 - ycs; m.ys0 = ys0;
+                        m.yprev = g0 == 0 ? 0u : (ys0 < g0 ? m.ylo : m.ylo - 1u);
+                        S.lbt[seq_claim % C::NP] = t;
+                        mbar_arrive_tx(&S.full[s], xb + yb);
+                        bulk_g2s(S.in[s][0], A.xw + xcs, xb, &S.full[s]);
+                        bulk_g2s(S.in[s][1], A.yw + ycs, yb, &S.full[s]);
+                    }
+                    ++n_real;
+                }
+                ++seq_claim;
+                progress = true;
+            }
+        }
+        // 2) look-back of the oldest claimed tile still without a prefix
+        if (seq_lb < n_real) {
+            __syncwarp();
+            if (!lb_active) {
+                lb_active = true;
+                lb_hi = S.lbt[seq_lb % C::NP];
+                lb_acc = make_uint4(0u, 0u, 0u, 0u);
+            }
+            int r;
+            while ((r = dlook_step(recs4, epoch, lb_hi, lb_acc)) == 1) {}
+            if (r == 2) {
+                if (lane == 0) {
+                    S.prefix[seq_lb % C::NP] = lb_acc;
+                    mbar_arrive(&S.pre[seq_lb % C::NP]);
+                }
+                ++seq_lb;
+                lb_active = false;
+                progress = true;
+            }
+        }
+        if (ended && seq_lb == n_real) break;
+        if (progress) {
+            last = gtimer();
+            ns = 32;
+        } else {
+            __nanosleep(ns);
+            if (ns < 256) ns <<= 1;
+            if (__shfl_sync(0xffffffffu, (gtimer() - last > WAIT_LIMIT_NS) ? 1u : 0u, 0)) {
+                if (lane == 0) dense_fail(A, abort);
+                break;
+            }
+        }
+    }
+    __syncwarp();
+    if (lane == 0 && *abort) {
+        // leave no bulk copy in flight: wait (bounded) for the last claims
+        const uint32_t first = seq_claim > (uint32_t)C::NI ? seq_claim - C::NI : 0u;
+        for (uint32_t q = first; q < seq_claim; ++q) {
+            if (S.slot[q % C::NI].t == DEND) continue;
+            const uint64_t t0 = gtimer();
+            while (!mbar_test(&S.full[q % C::NI], (q / C::NI) & 1u) && gtimer() - t0 < WAIT_LIMIT_NS) __nanosleep(256);
+        }
     }
 }
-__device__ __forceinline__ void dense_sum(DenseShared& S, int side, const Chunk& ch) {
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    // groups = words + (count - 1) summed over fill words
+
+// ------------------------------------------------------------ compute warps
+__device__ __forceinline__ uint4 realign4(const uint4* b4, uint32_t base) {
+    // words base .. base+3 of a 16-byte aligned word buffer
+    const uint32_t q = base >> 2, a = base & 3u;
+    const uint4 A = b4[q];
+    if (a == 0) return A;
+    const uint4 B = b4[q + 1];
+    if (a == 1) return make_uint4(A.y, A.z, A.w, B.x);
+    if (a == 2) return make_uint4(A.z, A.w, B.x, B.y);
+    return make_uint4(A.w, B.x, B.y, B.z);
+}
+__device__ __forceinline__ uint4 pattern4(uint4 v) {
+    return make_uint4(wpattern(v.x), wpattern(v.y), wpattern(v.z), wpattern(v.w));
+}
+template <int OP>
+__device__ __forceinline__ uint32_t op2(uint32_t a, uint32_t b) {
+    if (OP == OP_AND) return a & b;
+    if (OP == OP_OR) return a | b;
+    if (OP == OP_XOR) return a ^ b;
+    return a & ~b;  // patterns have bit 31 clear
+}
+// 1..ALLONES-1: a group that is neither all-0 nor all-1
+__device__ __forceinline__ bool is_mixed(uint32_t v) { return v - 1u < ALLONES - 1u; }
+__device__ __forceinline__ uint32_t cls_in(uint32_t v, bool in) { return in ? cls_of(v) : (uint32_t)C_NONE; }
+
+// Expansion of an impure operand: markers at word starts and the word
+// covering every step start.  Two calls: phase 0 sums the thread's words
+// (returns its exclusive position inside the warp), phase 1 places them.
+template <int TG, int NCW>
+__device__ __forceinline__ void exp_sum(DShared<TG, NCW>& S, int side, const uint32_t* buf, uint32_t lo, uint32_t hi,
+                                        uint32_t (&v)[DCfg<TG, NCW>::WPT], uint32_t& ex) {
+    using C = DCfg<TG, NCW>;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u;
+    const uint32_t j0 = lo + tid * C::WPT;
     uint32_t sum = 0;
 #pragma unroll
-    for (int k = 0; k < DKMAX; ++k) {
-        const bool in = ch.c0 + k * 32 + lane < ch.c1;
-        sum += in ? 1u : 0u;
-        if (in && is_fill(ch.v[k])) sum += wgroups(ch.v[k]) - 1u;
+    for (int j = 0; j < C::WPT; ++j) {
+        const bool in = j0 + j < hi;
+        v[j] = in ? buf[j0 + j] : 0u;
+        if (in) sum += wgroups(v[j]);
     }
-    sum = __reduce_add_sync(0xffffffffu, sum);
-    if (lane == 0) S.wsum[side][warp] = sum;
+    uint32_t x = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= (uint32_t)d) x += t;
+    }
+    if (lane == 31) S.xsum[side][tid >> 5] = x;
+    ex = x - sum;
 }
-__device__ __forceinline__ void dense_place(DenseShared& S, int side, const Chunk& ch, uint32_t s0,
-                                            uint32_t g0, uint32_t g1) {
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    uint32_t carry = s0;
-    for (uint32_t k = 0; k < warp; ++k) carry += S.wsum[side][k];
+template <int TG, int NCW>
+__device__ __forceinline__ void exp_place(DShared<TG, NCW>& S, int side, uint32_t lo, uint32_t hi, uint32_t s0,
+                                          const uint32_t (&v)[DCfg<TG, NCW>::WPT], uint32_t ex,
+                                          uint32_t g0, uint32_t g1) {
+    using C = DCfg<TG, NCW>;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t j0 = lo + tid * C::WPT;
+    uint32_t p = s0 + ex;
+    for (uint32_t k = 0; k < warp; ++k) p += S.xsum[side][k];
 #pragma unroll
-    for (int k = 0; k < DKMAX; ++k) {
-        const uint32_t i = ch.c0 + k * 32 + lane;
-        if (ch.c0 + k * 32 >= ch.c1) break;  // warp-uniform
-        const uint32_t wd = ch.v[k];
-        const bool in = i < ch.c1;
-        const uint32_t fm = __ballot_sync(0xffffffffu, in && is_fill(wd));
-        if (fm == 0 && ch.c0 + k * 32 + 32 <= ch.c1 && carry >= g0 && carry + 32 <= g1) {
-            // 32 literals inside the tile: word `lane` is group carry + lane
-            S.d[side][carry - g0 + lane] = wd;
-            carry += 32;
-            continue;
-        }
-        const uint32_t c = in ? wgroups(wd) : 0u;
-        uint32_t p;
-        if (fm == 0) {  // literals only: word `lane` starts at carry + lane
-            p = carry + lane;
-            carry += __popc(__ballot_sync(0xffffffffu, in));
-        } else {
-            uint32_t x = c;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) { uint32_t t = __shfl_up_sync(0xffffffffu, x, d); if (lane >= (uint32_t)d) x += t; }
-            p = carry + x - c;
-            carry += __shfl_sync(0xffffffffu, x, 31);
-        }
-        if (in) {
+    for (int j = 0; j < C::WPT; ++j) {
+        if (j0 + j < hi) {
+            const uint32_t c = wgroups(v[j]);
+            if (p >= g0 && p < g1) S.mk[side][p - g0] = (uint16_t)(j0 + j + 1u);
             const uint32_t a = max(p, g0), e = min(p + c, g1);
             if (a < e) {
-                const uint32_t pat = wpattern(wd);
-                if (e - a <= 32u) {
-                    for (uint32_t g = a; g < e; ++g) S.d[side][g - g0] = pat;
-                } else {
-                    const uint32_t slot = atomicAdd(&S.fl_n[side], 1u);
-                    S.fl_pos[side][slot] = a - g0; S.fl_len[side][slot] = e - a; S.fl_val[side][slot] = pat;
-                }
+                // step starts q*128 inside [a, e)
+                for (uint32_t q = (a - g0 + 127u) >> 7; (q << 7) < e - g0; ++q) S.cov[side][q] = j0 + j;
             }
+            p += c;
         }
     }
 }
-
-// 31-bit pattern of group g of one operand: straight from the words when the
-// operand is pure over the tile, else from the expansion.
-__device__ __forceinline__ uint32_t dense_pat(const DenseShared& S, int side, bool pure,
-                                              const uint32_t* __restrict__ w, uint32_t wbase, uint32_t l) {
-    return pure ? wpattern(__ldg(w + wbase + l)) : S.d[side][l];
+// buffer index of the word covering group 128q-1 of the tile (q >= 1)
+template <int TG, int NCW>
+__device__ __forceinline__ uint32_t exp_word_before(const DShared<TG, NCW>& S, int side, uint32_t q) {
+    return S.mk[side][q << 7] ? S.cov[side][q] - 1u : S.cov[side][q];
+}
+// the 4 patterns of groups l..l+3 of an impure operand (whole warp)
+template <int TG, int NCW>
+__device__ __forceinline__ uint4 exp_read4(const DShared<TG, NCW>& S, int side, const uint32_t* buf, uint32_t l,
+                                           uint32_t q) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint2 mm = *reinterpret_cast<const uint2*>(&S.mk[side][l]);
+    // lane 0 starts from the word covering the step's first group, so every
+    // lane's running maximum is at least 1
+    uint32_t a0 = max(mm.x & 0xFFFFu, lane == 0 ? S.cov[side][q] + 1u : 0u);
+    uint32_t a1 = max(a0, mm.x >> 16);
+    uint32_t a2 = max(a1, mm.y & 0xFFFFu);
+    uint32_t a3 = max(a2, mm.y >> 16);
+    uint32_t inc = a3;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xffffffffu, inc, d);
+        if (lane >= (uint32_t)d) inc = max(inc, o);
+    }
+    uint32_t ex = __shfl_up_sync(0xffffffffu, inc, 1);
+    if (lane == 0) ex = 0u;
+    a0 = max(a0, ex); a1 = max(a1, ex); a2 = max(a2, ex); a3 = max(a3, ex);
+    return make_uint4(wpattern(buf[a0 - 1u]), wpattern(buf[a1 - 1u]), wpattern(buf[a2 - 1u]), wpattern(buf[a3 - 1u]));
 }
 
-template <int OP>
-__global__ void __launch_bounds__(DTHREADS) k_dense(DenseArgs A) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    DenseShared& S = *reinterpret_cast<DenseShared*>(smem_raw);
+// Pass 1 of one tile: results and codes into buffer b, tile aggregate
+// published; the slot's words are released.
+template <int OP, int TG, int NCW>
+__device__ __forceinline__ void dense_pass1(DShared<TG, NCW>& S, const DenseArgs& A, const DSlot& m, uint32_t s,
+                                            uint32_t b, uint32_t epoch) {
+    using C = DCfg<TG, NCW>;
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-    if (tid == 0) {
-        S.hdr[0] = claim_tile(A.sync);
-        S.hdr[1] = ld_cg(&A.sync->epoch);
-        S.fl_n[0] = 0; S.fl_n[1] = 0;
-    }
-    __syncthreads();
-    const uint32_t t = S.hdr[0], epoch = S.hdr[1];
-    const uint32_t G = A.groups;
-    const uint32_t g0 = t * (uint32_t)DT, g1 = min(g0 + (uint32_t)DT, G);
-    const uint32_t ng = g1 - g0;
-
-    // word ranges; an operand is pure over the tile when its words there are
-    // exactly one per group
-    const uint32_t xi0 = __ldg(A.xgt + 2 * t), xs0 = __ldg(A.xgt + 2 * t + 1);
-    const uint32_t xn0 = __ldg(A.xgt + 2 * t + 2), xns = __ldg(A.xgt + 2 * t + 3);
-    const uint32_t yi0 = __ldg(A.ygt + 2 * t), ys0 = __ldg(A.ygt + 2 * t + 1);
-    const uint32_t yn0 = __ldg(A.ygt + 2 * t + 2), yns = __ldg(A.ygt + 2 * t + 3);
-    const bool xpure = xs0 == g0 && xns == g1 && xn0 - xi0 == ng;
-    const bool ypure = ys0 == g0 && yns == g1 && yn0 - yi0 == ng;
-    // words covering [g0, g1): [i0, i_end) with i_end past the word covering g1-1
-    const uint32_t xi1 = min(xns == g1 ? xn0 : xn0 + 1u, A.nx);
-    const uint32_t yi1 = min(yns == g1 ? yn0 : yn0 + 1u, A.ny);
-    // one batch of requests: both operands' words and the words before g0
-    uint32_t xprev = 0, yprev = 0;
-    if (tid == 0 && g0 > 0) {
-        xprev = (xs0 < g0) ? __ldg(A.xw + xi0) : __ldg(A.xw + xi0 - 1);
-        yprev = (ys0 < g0) ? __ldg(A.yw + yi0) : __ldg(A.yw + yi0 - 1);
-    }
-    {
-        Chunk cx, cy;
-        if (!xpure) dense_load(S, 0, A.xw, xi0, xi1, cx);
-        if (!ypure) dense_load(S, 1, A.yw, yi0, yi1, cy);
-        if (!xpure) dense_sum(S, 0, cx);
-        if (!ypure) dense_sum(S, 1, cy);
-        if (!xpure || !ypure) __syncthreads();
-        if (!xpure) dense_place(S, 0, cx, xs0, g0, g1);
-        if (!ypure) dense_place(S, 1, cy, ys0, g0, g1);
-    }
-    if (tid == 0) S.hdr[2] = (g0 > 0) ? cls_of(apply_op(OP, wpattern(xprev), wpattern(yprev))) : C_NONE;
+    const uint32_t* bx = reinterpret_cast<const uint32_t*>(S.in[s][0]);
+    const uint32_t* by = reinterpret_cast<const uint32_t*>(S.in[s][1]);
+    const uint4* bx4 = S.in[s][0];
+    const uint4* by4 = S.in[s][1];
+    const bool xpure = m.flags & 1u, ypure = m.flags & 2u;
+    const uint32_t g0 = m.g0, ng = m.ng, g1 = g0 + ng;
     if (!xpure || !ypure) {
-        __syncthreads();
-        for (int side = 0; side < 2; ++side) {
-            const uint32_t nf = S.fl_n[side];
-            for (uint32_t k = 0; k < nf; ++k) {
-                const uint32_t p = S.fl_pos[side][k], len = S.fl_len[side][k], val = S.fl_val[side][k];
-                for (uint32_t r = tid; r < len; r += DTHREADS) S.d[side][p + r] = val;
-            }
-        }
-        __syncthreads();
+        uint32_t vx[C::WPT], vy[C::WPT];
+        uint32_t ex = 0, ey = 0;
+        if (!xpure) for (uint32_t i = tid; i < (uint32_t)TG / 8u; i += C::CT) reinterpret_cast<uint4*>(S.mk[0])[i] = make_uint4(0u, 0u, 0u, 0u);
+        if (!ypure) for (uint32_t i = tid; i < (uint32_t)TG / 8u; i += C::CT) reinterpret_cast<uint4*>(S.mk[1])[i] = make_uint4(0u, 0u, 0u, 0u);
+        if (!xpure) exp_sum<TG, NCW>(S, 0, bx, m.xlo, m.xhi, vx, ex);
+        if (!ypure) exp_sum<TG, NCW>(S, 1, by, m.ylo, m.yhi, vy, ey);
+        bar_sync1(C::CT);
+        if (!xpure) exp_place<TG, NCW>(S, 0, m.xlo, m.xhi, m.xs0, vx, ex, g0, g1);
+        if (!ypure) exp_place<TG, NCW>(S, 1, m.ylo, m.yhi, m.ys0, vy, ey, g0, g1);
+        bar_sync1(C::CT);
     }
-
-    // ---- pass 1: warp w walks groups [w*DGPW, (w+1)*DGPW) of the tile
-    const uint32_t wl0 = warp * DGPW;
-    uint32_t r[DSTEPS];
-    uint32_t hm[DSTEPS];
-    uint32_t popc = 0;
-    uint32_t prevc;  // class of the group before this warp's first one
-    __syncthreads();  // S.hdr[2] (class before the tile) and the expansion are ready
-    {
-        uint32_t pc = C_NONE;
-        if (lane == 0 && wl0 < ng) {
-            if (wl0 > 0) {
-                pc = cls_of(apply_op(OP, dense_pat(S, 0, xpure, A.xw, xi0, wl0 - 1),
-                                     dense_pat(S, 1, ypure, A.yw, yi0, wl0 - 1)));
-            } else {
-                pc = S.hdr[2];
-            }
-        }
-        prevc = __shfl_sync(0xffffffffu, pc, 0);
-    }
-    uint32_t nheads = 0, lastpos = 0, lastcls = 0;
-    bool has = false;
-    // issue every load of the warp before using any: 2*DSTEPS independent
-    // coalesced 128-byte requests in flight per warp
-    uint32_t yv[DSTEPS];
-#pragma unroll
-    for (int s = 0; s < DSTEPS; ++s) {
-        const uint32_t l = wl0 + s * 32 + lane;
-        r[s] = 0; yv[s] = 0;
-        if (l < ng) {
-            r[s] = xpure ? __ldg(A.xw + xi0 + l) : S.d[0][l];
-            yv[s] = ypure ? __ldg(A.yw + yi0 + l) : S.d[1][l];
-        }
-    }
-#pragma unroll
-    for (int s = 0; s < DSTEPS; ++s) {
-        const uint32_t l = wl0 + s * 32 + lane;
-        const bool in = l < ng;
-        uint32_t v = 0, c = C_NONE;
-        if (in) {
-            v = apply_op(OP, xpure ? wpattern(r[s]) : r[s], ypure ? wpattern(yv[s]) : yv[s]);
-            c = cls_of(v);
-        }
-        uint32_t pcl = __shfl_up_sync(0xffffffffu, c, 1);
-        if (lane == 0) pcl = prevc;
-        const bool h = in && (c == C_MIXED || c != pcl);
-        const uint32_t m = __ballot_sync(0xffffffffu, h);
-        prevc = __shfl_sync(0xffffffffu, c, 31);
-        r[s] = v;
-        hm[s] = m;
-        popc += __popc(v);
-        if (m) {
-            const uint32_t hl = 31u - __clz(m);
-            nheads += __popc(m);
-            lastpos = g0 + wl0 + s * 32 + hl;
-            lastcls = __shfl_sync(0xffffffffu, c, hl);
-            has = true;
-        }
-    }
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) popc += __shfl_xor_sync(0xffffffffu, popc, d);
-    if (lane == 0) {
-        Agg a;
-        a.nheads = nheads; a.popc = popc; a.pos = lastpos;
-        a.info = mk_info(lastcls, has, 0, FSM_IDENTITY);
-        const uint4 v = agg_pack(a);
-        S.warp_agg[warp][0] = v.x; S.warp_agg[warp][1] = v.y; S.warp_agg[warp][2] = v.z; S.warp_agg[warp][3] = v.w;
-    }
-    __syncthreads();
-    // ---- block scan of the warp aggregates and look-back (warp 0)
-    if (warp == 0) {
-        Agg w = agg_identity();
-        if (lane < (uint32_t)DWARPS)
-            w = agg_unpack(make_uint4(S.warp_agg[lane][0], S.warp_agg[lane][1], S.warp_agg[lane][2], S.warp_agg[lane][3]));
-        Agg wi = w;
-#pragma unroll
-        for (int d = 1; d < DWARPS; d <<= 1) {
-            Agg o = agg_shfl_up<false>(wi, d);
-            if (lane >= (uint32_t)d) wi = agg_combine<false>(o, wi);
-        }
-        Agg wx = agg_shfl_up<false>(wi, 1);
-        if (lane == 0) wx = agg_identity();
-        const Agg tot = agg_unpack(make_uint4(__shfl_sync(0xffffffffu, wi.nheads, DWARPS - 1),
-                                              __shfl_sync(0xffffffffu, wi.pos, DWARPS - 1),
-                                              __shfl_sync(0xffffffffu, wi.info, DWARPS - 1),
-                                              __shfl_sync(0xffffffffu, wi.popc, DWARPS - 1)));
-        if (lane < (uint32_t)DWARPS) {
-            const uint4 pv = agg_pack(wx);
-            S.warp_agg[lane][0] = pv.x; S.warp_agg[lane][1] = pv.y; S.warp_agg[lane][2] = pv.z; S.warp_agg[lane][3] = pv.w;
-        }
-        Agg prefix = agg_identity();
-        if (t == 0) {
-            if (lane == 0) publish(&A.recs[0], epoch, REC_INCL, agg_pack(tot));
+    // class of the group before the warp's first one
+    const uint32_t wl0 = warp * C::GPW;
+    uint32_t prevc = C_NONE;
+    if (lane == 0 && wl0 < ng) {
+        if (wl0 == 0) {
+            if (g0 > 0) prevc = cls_of(op2<OP>(wpattern(bx[m.xprev]), wpattern(by[m.yprev])));
         } else {
-            if (lane == 0) publish(&A.recs[t], epoch, REC_AGG, agg_pack(tot));
-            bool ok;
-            prefix = agg_unpack(warp_lookback(A.recs, t, epoch, agg_pack(agg_identity()), AggComb<false>(), &ok));
-            if (lane == 0) {
-                if (!ok) atomicExch(&A.meta->status, DEV_ERR_TIMEOUT);
-                publish(&A.recs[t], epoch, REC_INCL, agg_pack(agg_combine<false>(prefix, tot)));
-            }
-        }
-        if (lane == 0) {
-            const uint4 pv = agg_pack(prefix);
-            S.tile_prefix[0] = pv.x; S.tile_prefix[1] = pv.y; S.tile_prefix[2] = pv.z; S.tile_prefix[3] = pv.w;
-            if (t == A.ntiles - 1) {
-                const Agg all = agg_combine<false>(prefix, tot);
-                const uint32_t n = all.nheads;
-                if (agg_has(all.info) && agg_cls(all.info) != C_MIXED) {
-                    const uint32_t wd = run_word(agg_cls(all.info), G - all.pos, 0, false);
-                    A.out[n - 1] = wd;
-                    if (n - 1 == 0) A.meta->w0 = wd;
-                    if (is_fill(wd)) atomicOr(&A.meta->nfill, 1u);
-                }
-                A.obp[(n + 31u) / 32u] = G;
-                A.meta->n = n;
-                A.meta->groups = G;
-                A.meta->nset = all.popc;
-                A.meta->anb = A.anb;
-                A.meta->aval = A.aval;
-                if (n == 0) A.meta->w0 = 0;
-            }
+            const uint32_t q = wl0 >> 7;
+            const uint32_t px = xpure ? wpattern(bx[m.xlo + wl0 - 1u]) : wpattern(bx[exp_word_before(S, 0, q)]);
+            const uint32_t py = ypure ? wpattern(by[m.ylo + wl0 - 1u]) : wpattern(by[exp_word_before(S, 1, q)]);
+            prevc = cls_of(op2<OP>(px, py));
         }
     }
-    __syncthreads();
-    // ---- pass 2: run words.  The lane of each head writes the word of the
-    // run before it (a uniform run's length is known only there) and, for a
-    // mixed group, its own literal.
-    const Agg tp = agg_unpack(make_uint4(S.tile_prefix[0], S.tile_prefix[1], S.tile_prefix[2], S.tile_prefix[3]));
-    const Agg wp = agg_unpack(make_uint4(S.warp_agg[warp][0], S.warp_agg[warp][1], S.warp_agg[warp][2], S.warp_agg[warp][3]));
-    const Agg pre = agg_combine<false>(tp, wp);
-    uint32_t idx = pre.nheads;                 // global index of the warp's next head
-    bool lhas = agg_has(pre.info);
-    uint32_t lcls = agg_cls(pre.info), lpos = pre.pos;
+    prevc = __shfl_sync(0xffffffffu, prevc, 0);
+
+    uint32_t nheads = 0, lastpos = 0, lastcls = 0, popc = 0;
+    bool has = false;
+#pragma unroll
+    for (int st = 0; st < C::STEPS; ++st) {
+        const uint32_t sb = wl0 + st * 128u;            // step's first group (tile-relative)
+        uint32_t* codep = &S.code[b][((warp * C::STEPS + st) << 5) + lane];
+        if (sb >= ng) {                                  // past the tile's end
+            *codep = 0u;
+            S.res[b][(sb >> 2) + lane] = make_uint4(0u, 0u, 0u, 0u);
+            continue;
+        }
+        const uint32_t l = sb + 4u * lane;
+        const uint32_t q = sb >> 7;
+        uint4 X = xpure ? realign4(bx4, m.xlo + l) : exp_read4(S, 0, bx, l, q);
+        uint4 Y = ypure ? realign4(by4, m.ylo + l) : exp_read4(S, 1, by, l, q);
+        // pure operands may hold count-1 fill words
+        if (__any_sync(0xffffffffu, ((X.x | X.y | X.z | X.w | Y.x | Y.y | Y.z | Y.w) >> 31) != 0u)) {
+            X = pattern4(X);
+            Y = pattern4(Y);
+        }
+        uint4 v = make_uint4(op2<OP>(X.x, Y.x), op2<OP>(X.y, Y.y), op2<OP>(X.z, Y.z), op2<OP>(X.w, Y.w));
+        const bool full = sb + 128u <= ng;
+        const bool allmixed = is_mixed(v.x) & is_mixed(v.y) & is_mixed(v.z) & is_mixed(v.w);
+        if (full && __all_sync(0xffffffffu, allmixed)) {
+            *codep = DFAST;
+            nheads += 128u;
+            lastpos = g0 + sb + 127u;
+            lastcls = C_MIXED;
+            has = true;
+            prevc = C_MIXED;
+        } else {
+            const bool i0 = l < ng, i1 = l + 1u < ng, i2 = l + 2u < ng, i3 = l + 3u < ng;
+            if (!i0) v.x = 0u;
+            if (!i1) v.y = 0u;
+            if (!i2) v.z = 0u;
+            if (!i3) v.w = 0u;
+            const uint32_t c0 = cls_in(v.x, i0), c1 = cls_in(v.y, i1), c2 = cls_in(v.z, i2), c3 = cls_in(v.w, i3);
+            uint32_t pc = __shfl_up_sync(0xffffffffu, c3, 1);
+            if (lane == 0) pc = prevc;
+            const uint32_t hf = ((i0 && (c0 == C_MIXED || c0 != pc)) ? 1u : 0u) |
+                                ((i1 && (c1 == C_MIXED || c1 != c0)) ? 2u : 0u) |
+                                ((i2 && (c2 == C_MIXED || c2 != c1)) ? 4u : 0u) |
+                                ((i3 && (c3 == C_MIXED || c3 != c2)) ? 8u : 0u);
+            const uint32_t cd = hf | (c0 << 4) | (c1 << 6) | (c2 << 8) | (c3 << 10);
+            *codep = cd;
+            nheads += __reduce_add_sync(0xffffffffu, __popc(hf));
+            const uint32_t hm = __ballot_sync(0xffffffffu, hf != 0u);
+            if (hm) {
+                const uint32_t hl = 31u - __clz(hm);
+                const uint32_t hc = __shfl_sync(0xffffffffu, cd, hl);
+                const uint32_t j = 31u - __clz(hc & 0xFu);
+                lastpos = g0 + sb + 4u * hl + j;
+                lastcls = (hc >> (4u + 2u * j)) & 3u;
+                has = true;
+            }
+            prevc = __shfl_sync(0xffffffffu, c3, 31);
+        }
+        S.res[b][l >> 2] = v;
+        popc += __popc(v.x) + __popc(v.y) + __popc(v.z) + __popc(v.w);
+    }
+    popc = __reduce_add_sync(0xffffffffu, popc);
+    if (lane == 0) S.wagg[b][warp] = dagg_make(nheads, popc, lastpos, lastcls, has);
+    bar_sync1(C::CT);  // every compute warp is done with the slot's words
+    if (tid == 0) mbar_arrive(&S.empty[s]);
+    if (warp == 0) {
+        uint4 w = make_uint4(0u, 0u, 0u, 0u);
+        if (lane < (uint32_t)NCW) w = S.wagg[b][lane];
+        uint4 wi = w;
+#pragma unroll
+        for (int d = 1; d < NCW; d <<= 1) {
+            uint4 o;
+            o.x = __shfl_up_sync(0xffffffffu, wi.x, d);
+            o.y = __shfl_up_sync(0xffffffffu, wi.y, d);
+            o.z = __shfl_up_sync(0xffffffffu, wi.z, d);
+            o.w = 0;
+            if (lane >= (uint32_t)d) wi = dagg_comb(o, wi);
+        }
+        uint4 wx;
+        wx.x = __shfl_up_sync(0xffffffffu, wi.x, 1);
+        wx.y = __shfl_up_sync(0xffffffffu, wi.y, 1);
+        wx.z = __shfl_up_sync(0xffffffffu, wi.z, 1);
+        wx.w = 0;
+        if (lane == 0) wx = make_uint4(0u, 0u, 0u, 0u);
+        uint4 tot;
+        tot.x = __shfl_sync(0xffffffffu, wi.x, NCW - 1);
+        tot.y = __shfl_sync(0xffffffffu, wi.y, NCW - 1);
+        tot.z = __shfl_sync(0xffffffffu, wi.z, NCW - 1);
+        tot.w = 0;
+        if (lane < (uint32_t)NCW) S.wagg[b][lane] = wx;
+        if (lane == 0) {
+            S.tagg[b] = tot;
+            S.tinfo[b][0] = m.t; S.tinfo[b][1] = g0; S.tinfo[b][2] = ng;
+            drec_publish(A.drecs, m.t, epoch, m.t == 0 ? REC_INCL : REC_AGG, tot);
+        }
+    }
+}
+
+// Pass 2 of the tile whose pass 1 left buffer b, with its prefix in slot p.
+template <int TG, int NCW>
+__device__ __forceinline__ void dense_pass2(DShared<TG, NCW>& S, const DenseArgs& A, uint32_t b, uint32_t p,
+                                            uint32_t epoch) {
+    using C = DCfg<TG, NCW>;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint4 prefix = S.prefix[p];
+    const uint32_t t = S.tinfo[b][0], g0 = S.tinfo[b][1];
+    const uint32_t G = A.groups;
+    if (tid == 0) {
+        const uint4 all = dagg_comb(prefix, S.tagg[b]);
+        if (t > 0) drec_publish(A.drecs, t, epoch, REC_INCL, all);
+        if (t == A.ntiles - 1) {
+            const uint32_t n = dagg_n(all);
+            if (dagg_has(all) && dagg_cls(all) != C_MIXED) {
+                const uint32_t wd = run_word(dagg_cls(all), G - all.z, 0, false);
+                A.out[n - 1] = wd;
+                if (n - 1 == 0) A.meta->w0 = wd;
+                if (is_fill(wd)) atomicOr(&A.meta->nfill, 1u);
+            }
+            A.obp[(n + 31u) / 32u] = G;
+            A.meta->n = n;
+            A.meta->groups = G;
+            A.meta->nset = all.x;
+            A.meta->anb = A.anb;
+            A.meta->aval = A.aval;
+            if (n == 0) A.meta->w0 = 0;
+        }
+    }
+    const uint4 pre = dagg_comb(prefix, S.wagg[b][warp]);
+    uint32_t idx = dagg_n(pre);                 // output index of the warp's next head
+    bool lhas = dagg_has(pre);                  // the last head before the step
+    uint32_t lcls = dagg_cls(pre), lpos = pre.z;
     uint32_t fill_seen = 0;
     const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t wl0 = warp * C::GPW;
 #pragma unroll
-    for (int s = 0; s < DSTEPS; ++s) {
-        const uint32_t m = hm[s];
-        if (!m) continue;
-        const uint32_t v = r[s];
-        const uint32_t c = cls_of(v);
-        const uint32_t pos = g0 + wl0 + s * 32 + lane;
-        if (m == 0xffffffffu && __all_sync(0xffffffffu, c == C_MIXED)) {
-            // 32 mixed literals: 32 consecutive words, one coalesced store
+    for (int st = 0; st < C::STEPS; ++st) {
+        const uint32_t sb = wl0 + st * 128u;
+        const uint32_t pos0 = g0 + sb;
+        const uint32_t gl = pos0 + 4u * lane;
+        const uint32_t cd = S.code[b][((warp * C::STEPS + st) << 5) + lane];
+        const uint4 v = S.res[b][(sb >> 2) + lane];
+        if (cd == DFAST) {                      // warp-uniform: 128 mixed literals
             if (lane == 0 && lhas && lcls != C_MIXED) {
-                const uint32_t wd = run_word(lcls, pos - lpos, 0, false);
+                const uint32_t wd = run_word(lcls, pos0 - lpos, 0, false);
                 A.out[idx - 1] = wd;
                 if (idx - 1 == 0) A.meta->w0 = wd;
                 fill_seen |= is_fill(wd) ? 1u : 0u;
             }
-            A.out[idx + lane] = v;
-            if (idx + lane == 0) A.meta->w0 = v;
-            if (((idx + lane) & 31u) == 0) A.obp[(idx + lane) >> 5] = pos;
-            idx += 32;
-            lhas = true; lcls = C_MIXED; lpos = pos - lane + 31u;
+            const uint32_t o = idx + 4u * lane;
+            A.out[o] = v.x; A.out[o + 1] = v.y; A.out[o + 2] = v.z; A.out[o + 3] = v.w;
+            if (o == 0) A.meta->w0 = v.x;
+            const uint32_t rr = (32u - (o & 31u)) & 31u;
+            if (rr < 4u) A.obp[(o + rr) >> 5] = gl + rr;
+            idx += 128u;
+            lhas = true; lcls = C_MIXED; lpos = pos0 + 127u;
             continue;
         }
-        const bool h = (m >> lane) & 1u;
-        const uint32_t before = m & lt;
-        const uint32_t my = idx + __popc(before);
-        // previous head: the highest head lane below me, else the running one
-        const uint32_t pl = before ? 31u - __clz(before) : 0u;
-        const uint32_t pcls = __shfl_sync(0xffffffffu, c, pl);
-        if (h) {
-            const bool phas = before ? true : lhas;
-            const uint32_t pc = before ? pcls : lcls;
-            const uint32_t pp = before ? (g0 + wl0 + s * 32 + pl) : lpos;
-            if (phas && pc != C_MIXED) {
-                const uint32_t wd = run_word(pc, pos - pp, 0, false);
-                A.out[my - 1] = wd;
-                if (my - 1 == 0) A.meta->w0 = wd;
-                fill_seen |= is_fill(wd) ? 1u : 0u;
-            }
-            if (c == C_MIXED) {
-                A.out[my] = v;
-                if (my == 0) A.meta->w0 = v;
-            }
-            if ((my & 31u) == 0) A.obp[my >> 5] = pos;
+        const uint32_t hf = cd & 0xFu;
+        const uint32_t cnt = __popc(hf);
+        const uint32_t b0 = __ballot_sync(0xffffffffu, cnt & 1u);
+        const uint32_t b1 = __ballot_sync(0xffffffffu, cnt & 2u);
+        const uint32_t b2 = __ballot_sync(0xffffffffu, cnt & 4u);
+        const uint32_t ex = __popc(b0 & lt) + 2u * __popc(b1 & lt) + 4u * __popc(b2 & lt);
+        const uint32_t tot = __popc(b0) + 2u * __popc(b1) + 4u * __popc(b2);
+        const uint32_t hm = __ballot_sync(0xffffffffu, hf != 0u);
+        uint32_t mylast = 0;                    // this lane's last head: pos << 2 | class
+        if (hf) {
+            const uint32_t j = 31u - __clz(hf);
+            mylast = ((gl + j) << 2) | ((cd >> (4u + 2u * j)) & 3u);
         }
-        const uint32_t hl = 31u - __clz(m);
-        idx += __popc(m);
-        lhas = true;
-        lcls = __shfl_sync(0xffffffffu, c, hl);
-        lpos = g0 + wl0 + s * 32 + hl;
+        const uint32_t before = hm & lt;
+        const uint32_t src = before ? 31u - __clz(before) : lane;
+        const uint32_t pk = __shfl_sync(0xffffffffu, mylast, src);
+        bool phas = before ? true : lhas;
+        uint32_t ppos = before ? (pk >> 2) : lpos;
+        uint32_t pcls = before ? (pk & 3u) : lcls;
+        uint32_t my = idx + ex;
+        const uint32_t vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if ((hf >> j) & 1u) {
+                const uint32_t pos = gl + j;
+                const uint32_t c = (cd >> (4 + 2 * j)) & 3u;
+                if (phas && pcls != C_MIXED) {
+                    const uint32_t wd = run_word(pcls, pos - ppos, 0, false);
+                    A.out[my - 1] = wd;
+                    if (my - 1 == 0) A.meta->w0 = wd;
+                    fill_seen |= is_fill(wd) ? 1u : 0u;
+                }
+                if (c == C_MIXED) {
+                    A.out[my] = vv[j];
+                    if (my == 0) A.meta->w0 = vv[j];
+                }
+                if ((my & 31u) == 0) A.obp[my >> 5] = pos;
+                ++my;
+                phas = true; ppos = pos; pcls = c;
+            }
+        }
+        idx += tot;
+        if (hm) {
+            const uint32_t qk = __shfl_sync(0xffffffffu, mylast, 31u - __clz(hm));
+            lhas = true; lpos = qk >> 2; lcls = qk & 3u;
+        }
     }
     if (__any_sync(0xffffffffu, fill_seen) && lane == 0) atomicOr(&A.meta->nfill, 1u);
+}
+
+template <int OP, int TG, int NCW>
+__device__ __forceinline__ void dense_compute(DShared<TG, NCW>& S, const DenseArgs& A, uint32_t epoch) {
+    using C = DCfg<TG, NCW>;
+    const uint32_t tid = threadIdx.x;
+    volatile uint32_t* abort = &S.abort;
+    volatile uint32_t* okp = &S.ok;
+    uint32_t k = 0;
+    bool ok = true;
+    while (true) {
+        const uint32_t s = k % C::NI;
+        // one thread waits for the slot; the barrier hands the outcome to all
+        if (tid == 0) {
+            const bool w = dwait(&S.full[s], (k / C::NI) & 1u, abort);
+            if (!w && !*abort) dense_fail(A, abort);
+            *okp = w ? 1u : 0u;
+        }
+        bar_sync1(C::CT);
+        if (!*okp) { ok = false; break; }
+        const DSlot m = S.slot[s];
+        if (m.t == DEND) break;
+        dense_pass1<OP, TG, NCW>(S, A, m, s, k & 1u, epoch);
+        if (k > 0) {
+            const uint32_t j = k - 1;
+            if (tid == 0) {
+                const bool w = dwait(&S.pre[j % C::NP], (j / C::NP) & 1u, abort);
+                if (!w && !*abort) dense_fail(A, abort);
+                *okp = w ? 1u : 0u;
+            }
+            bar_sync1(C::CT);
+            if (!*okp) { ok = false; break; }
+            dense_pass2<TG, NCW>(S, A, j & 1u, j % C::NP, epoch);
+        }
+        ++k;
+        bar_sync1(C::CT);  // pass 2 of k-1 done before its buffer is reused
+    }
+    if (ok && k > 0) {
+        const uint32_t j = k - 1;
+        if (tid == 0) {
+            const bool w = dwait(&S.pre[j % C::NP], (j / C::NP) & 1u, abort);
+            if (!w && !*abort) dense_fail(A, abort);
+            *okp = w ? 1u : 0u;
+        }
+        bar_sync1(C::CT);
+        if (*okp) dense_pass2<TG, NCW>(S, A, j & 1u, j % C::NP, epoch);
+    }
+}
+
+template <int OP, int TG, int NCW>
+__global__ void __launch_bounds__((NCW + 1) * 32) k_dense(DenseArgs A) {
+    using C = DCfg<TG, NCW>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    DShared<TG, NCW>& S = *reinterpret_cast<DShared<TG, NCW>*>(smem_raw);
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < C::NI; ++i) { mbar_init(&S.full[i], 1); mbar_init(&S.empty[i], 1); }
+        for (int i = 0; i < C::NP; ++i) mbar_init(&S.pre[i], 1);
+        mbar_init_fence();
+        S.epoch = ld_cg(&A.sync->epoch);
+        S.abort = 0;
+        S.ok = 1;
+    }
     __syncthreads();
-    if (tid == 0) finish_tile(A.sync, A.ntiles);
+    const uint32_t epoch = S.epoch;
+    if (threadIdx.x >= (uint32_t)C::CT) dense_control<TG, NCW>(S, A, epoch);
+    else dense_compute<OP, TG, NCW>(S, A, epoch);
+    __syncthreads();
+    if (threadIdx.x == 0) finish_tile(A.sync, gridDim.x);
 }
 
 }  // namespace wah

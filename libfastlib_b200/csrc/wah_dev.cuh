@@ -222,5 +222,61 @@ __device__ __forceinline__ bool lookback64(TileRec* recs, uint32_t t, uint32_t e
     return ok;
 }
 
+// ---- mbarriers and bulk copies (sm_90+ PTX), shared memory addressed by
+// its 32-bit shared-window offset
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(b)), "r"(count) : "memory");
+}
+// makes barrier initialisation visible to the bulk-copy (async) proxy
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+// non-blocking: has the phase of parity `par` completed?
+__device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t par) {
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok) : "r"(smem_u32(b)), "r"(par) : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t gtimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;  // 2 s without progress: give up
+// Bounded wait for phase `par` of barrier b; false after WAIT_LIMIT_NS.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t par) {
+    if (mbar_test(b, par)) return true;
+    const uint64_t t0 = gtimer();
+    uint32_t ns = 32;
+    while (!mbar_test(b, par)) {
+        __nanosleep(ns);
+        if (ns < 512) ns <<= 1;
+        if (gtimer() - t0 > WAIT_LIMIT_NS) return false;
+    }
+    return true;
+}
+// Bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned)
+// from global memory into this CTA's shared memory, completing on barrier b.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* b) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(b)) : "memory");
+}
+// Named barrier over the first `nthreads` threads of the CTA (id 1).
+__device__ __forceinline__ void bar_sync1(uint32_t nthreads) {
+    asm volatile("bar.sync 1, %0;" :: "r"(nthreads) : "memory");
+}
+
 }  // namespace wah
 #endif

@@ -51,6 +51,32 @@ def test_geometric_golden(gpu_ctx):
 @pytest.mark.parametrize("density", [1e-4, 1e-3, 1e-2, 0.1, 0.5])
 def test_full_size_against_oracle(gpu_ctx, density):
     """2^28-bit operands (the raw-WAH workload) — every op, both forms."""
+    _full_size(gpu_ctx, density)
+
+
+@pytest.mark.parametrize("tile", [1024, 4096])
+@pytest.mark.parametrize("density", [0.1, 0.5])
+def test_full_size_dense_tiles(gpu_ctx, density, tile):
+    """The dense-path kernel with other tile sizes gives the same words."""
+    with _tile(gpu_ctx, tile):
+        _full_size(gpu_ctx, density)
+
+
+class _tile:
+    def __init__(self, ctx, tile):
+        self.ctx, self.tile = ctx, tile
+
+    def __enter__(self):
+        import libfastlib_b200 as L
+        self.old = self.ctx.get_tuning(L.TUNE_DENSE_TILE)
+        self.ctx.set_tuning(L.TUNE_DENSE_TILE, self.tile)
+
+    def __exit__(self, *exc):
+        import libfastlib_b200 as L
+        self.ctx.set_tuning(L.TUNE_DENSE_TILE, self.old)
+
+
+def _full_size(gpu_ctx, density):
     nbits = 1 << 28
     a = oracle.build_runs(G.geometric_runs(11, nbits, density))
     b = oracle.build_runs(G.geometric_runs(12, nbits, density))
@@ -65,9 +91,15 @@ def test_full_size_against_oracle(gpu_ctx, density):
             assert np.array_equal(w, ref), (op, ip)
 
 
-def test_many_tiles_fuzz(gpu_ctx):
+@pytest.mark.parametrize("tile", [1024, 2048, 4096])
+def test_many_tiles_fuzz(gpu_ctx, tile):
     """Operands of ~10^5 words of mixed forms so results span many tiles and
     the look-back carries runs, heads and step states across tile edges."""
+    with _tile(gpu_ctx, tile):
+        _fuzz(gpu_ctx)
+
+
+def _fuzz(gpu_ctx):
     rng = np.random.default_rng(5)
     for trial in range(12):
         ng = int(rng.integers(20000, 200000))
@@ -125,3 +157,65 @@ def test_many_one_fills_per_tile(gpu_ctx):
     B = gpu_ctx.bitvector(a)
     B.decompress()
     assert np.array_equal(B.write(), oracle.decompress(a))
+
+
+def _dense_words(rng, ngroups):
+    """Literal stretches (mostly mixed, some 0/ALLONES literals and count-1
+    fills) between fills of up to a few thousand groups, so tiles are pure,
+    impure, all-mixed, or covered by fills that cross tile edges."""
+    words, g = [], 0
+    while g < ngroups:
+        left = ngroups - g
+        if rng.random() < 0.3:
+            c = int(min(left, rng.integers(1, 6000)))
+            words.append(G.fill(int(rng.integers(0, 2)), c))
+            g += c
+            continue
+        k = int(min(left, rng.integers(1, 5000)))
+        lit = rng.integers(1, G.ALLONES, size=k, dtype=np.int64)
+        r = rng.random(k)
+        lit[r < 0.02] = 0
+        lit[(r >= 0.02) & (r < 0.04)] = G.ALLONES
+        out = [int(x) for x in lit]
+        for i in np.nonzero(r > 0.995)[0]:
+            out[i] = G.fill(int(rng.integers(0, 2)), 1)
+        words.extend(out)
+        g += k
+    return words
+
+
+@pytest.mark.parametrize("tile", [1024, 2048, 4096])
+def test_dense_path_fuzz(gpu_ctx, tile):
+    """Operands dense enough for the _d2 path, sizes that leave partial last
+    tiles, fills longer than a tile, count-1 fill words among literals."""
+    rng = np.random.default_rng(77)
+    with _tile(gpu_ctx, tile):
+        for trial in range(10):
+            ng = int(rng.integers(1, 12)) * tile + int(rng.integers(0, tile))
+            wa, wb = _dense_words(rng, ng), _dense_words(rng, ng)
+            anb = int(rng.integers(0, 31))
+            a = G.serialize(wa, anb, int(rng.integers(0, 1 << 31)))
+            b = G.serialize(wb, anb, int(rng.integers(0, 1 << 31)))
+            if oracle.is_degenerate(a) or oracle.is_degenerate(b):
+                continue
+            for op in range(4):
+                for ip in (0, 1):
+                    ref, rc = oracle.binop(op, a, b, inplace=bool(ip))
+                    w, c = _bin(gpu_ctx, op, a, b, ip)
+                    assert c == rc and np.array_equal(w, ref), (trial, op, ip)
+
+
+def test_dense_small_sizes(gpu_ctx):
+    """1 to 3 tiles and tiny vectors: grids smaller than the SM count, a
+    control warp that meets the end at once."""
+    rng = np.random.default_rng(9)
+    for ng in (2, 3, 31, 127, 128, 129, 1023, 1024, 1025, 2047, 2049, 3000):
+        wa, wb = _dense_words(rng, ng), _dense_words(rng, ng)
+        a = G.serialize(wa, 7, 0x55)
+        b = G.serialize(wb, 7, 0x2A)
+        if oracle.is_degenerate(a) or oracle.is_degenerate(b):
+            continue
+        for op in range(4):
+            ref, rc = oracle.binop(op, a, b, inplace=False)
+            w, c = _bin(gpu_ctx, op, a, b, 0)
+            assert c == rc and np.array_equal(w, ref), (ng, op)

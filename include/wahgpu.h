@@ -172,6 +172,24 @@ int wahgpu_index_from_triple(wahgpu_ctx* ctx, int kind, uint64_t nrows, const do
  * the reference checks value by value (bin::checkBin / part::doScan,
  * src/ibin.cpp:2057-2304, src/part.cpp:4273). */
 int wahgpu_index_set_values(wahgpu_index* idx, int vtype, const void* values, uint64_t n);
+/* Builds an index of a column held in device memory, on the device
+ * (replaces relic::construct, src/irelic.cpp:879-925, with mapValues,
+ * src/index.cpp:2552-2611; and bin construction with
+ * <binning nbins=N equal_weight/>, src/ibin.cpp:2390-2582, 3350-3449).
+ * kind WAHGPU_RELIC: one bitmap per distinct value, keys ascending.
+ * kind WAHGPU_BIN: nbins bins of about equal row counts; a distinct value is
+ * never split between bins, and each bin's keys are the smallest and
+ * largest value it holds; the raw values are kept for edge-bin row checks.
+ * Every bitmap holds exactly the rows the reference's would; its words are
+ * in compress() form. */
+int wahgpu_index_build(wahgpu_ctx* ctx, int kind, int vtype, const void* dev_values, uint64_t nrows,
+                       uint32_t nbins, wahgpu_index** out);
+/* A copy of bitmap j as a bitvector (index::getBitvector, src/index.h). */
+int wahgpu_index_bitmap(wahgpu_index* idx, uint32_t j, wahgpu_bv** out);
+/* The index's keys in the triple's layout (relic: values; bin: minval then
+ * maxval); returns their count, WAHGPU_ESIZE if cap is too small. */
+int64_t wahgpu_index_keys(wahgpu_index* idx, double* out, uint64_t cap);
+
 int wahgpu_index_free(wahgpu_index* idx);
 int64_t wahgpu_index_nbitmaps(wahgpu_index* idx);
 int64_t wahgpu_index_nrows(wahgpu_index* idx);

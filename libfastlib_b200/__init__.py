@@ -101,6 +101,10 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
                                                     U32P, ctypes.c_uint64, ctypes.POINTER(P)]),
         "wahgpu_index_set_values": (ctypes.c_int, [P, ctypes.c_int, P, ctypes.c_uint64]),
         "wahgpu_index_free": (ctypes.c_int, [P]),
+        "wahgpu_index_build": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, P, ctypes.c_uint64, ctypes.c_uint32,
+                                              ctypes.POINTER(P)]),
+        "wahgpu_index_bitmap": (ctypes.c_int, [P, ctypes.c_uint32, ctypes.POINTER(P)]),
+        "wahgpu_index_keys": (ctypes.c_int64, [P, ctypes.POINTER(ctypes.c_double), ctypes.c_uint64]),
         "wahgpu_index_nbitmaps": (ctypes.c_int64, [P]),
         "wahgpu_index_nrows": (ctypes.c_int64, [P]),
         "wahgpu_index_total_ones": (ctypes.c_int64, [P]),
@@ -132,6 +136,7 @@ class Context:
         if rc != 0:
             raise WahError(rc, self.lib.wahgpu_last_error(None).decode())
         self.h = h
+        self.device = device
         self._live = weakref.WeakSet()
 
     def check(self, rc: int) -> int:
@@ -302,8 +307,46 @@ class Index:
             b.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), len(b), ctypes.byref(h)))
         self.h = h
         self.nrows = nrows
+        ctx._live.add(self)
         if values is not None:
             self.set_values(values)
+
+    @classmethod
+    def build(cls, ctx: Context, kind: int, values, nbins: int = 0) -> "Index":
+        """Builds the index on the device from a column (a CUDA tensor or a
+        numpy array of uint32 / int32 / float32): RELIC, one bitmap per
+        distinct value; BIN, `nbins` equal-weight bins."""
+        import torch
+        t = values if isinstance(values, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(values))
+        vt = {torch.int32: I32, torch.float32: F32, torch.uint32: U32}[t.dtype]
+        if not t.is_cuda:
+            t = t.to(f"cuda:{ctx.device}")
+        t = t.contiguous()
+        h = ctypes.c_void_p()
+        ctx.check(ctx.lib.wahgpu_index_build(ctx.h, kind, vt, ctypes.c_void_p(t.data_ptr()), t.numel(), nbins,
+                                             ctypes.byref(h)))
+        self = cls.__new__(cls)
+        self.ctx, self.h, self.nrows = ctx, h, t.numel()
+        ctx._live.add(self)
+        return self
+
+    def nbitmaps(self) -> int:
+        return self.ctx.check(int(self.ctx.lib.wahgpu_index_nbitmaps(self.h)))
+
+    def keys(self) -> np.ndarray:
+        cap = 2 * self.nbitmaps() + 2
+        out = np.empty(cap, dtype=np.float64)
+        n = self.ctx.check(int(self.ctx.lib.wahgpu_index_keys(
+            self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cap)))
+        return out[:n]
+
+    def bitmap(self, j: int) -> "Bitvector":
+        h = ctypes.c_void_p()
+        self.ctx.check(self.ctx.lib.wahgpu_index_bitmap(self.h, j, ctypes.byref(h)))
+        return Bitvector(self.ctx, h)
+
+    def _release(self):
+        self.close()
 
     def set_values(self, values):
         v = np.ascontiguousarray(values)

@@ -36,7 +36,8 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
     cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-O3",
            "-shared", "-I" + os.path.join(ROOT, "include"),
            "-o", out, os.path.join(HERE, "csrc", "wah_api.cu"),
-           os.path.join(HERE, "csrc", "wah_index.cu"), os.path.join(HERE, "csrc", "wah_noalloc.cu")]
+           os.path.join(HERE, "csrc", "wah_index.cu"), os.path.join(HERE, "csrc", "wah_build.cu"),
+           os.path.join(HERE, "csrc", "wah_noalloc.cu")]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

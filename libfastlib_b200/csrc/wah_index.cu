@@ -5,6 +5,7 @@
 #include "../../include/wahgpu.h"
 #include "wah_range.cuh"
 #include "wah_api_internal.h"
+#include "wah_index_internal.h"
 
 #include <cuda_runtime.h>
 #include <cmath>
@@ -13,38 +14,6 @@
 #include <algorithm>
 
 using namespace wah;
-
-struct wahgpu_index {
-    wahgpu_ctx* ctx = nullptr;
-    int kind = 0;                 // WAHGPU_RELIC / WAHGPU_BIN
-    uint32_t nrows = 0, groups = 0, anb = 0, nobs = 0, ntiles = 0;
-    std::vector<double> keys;     // relic: distinct values; bin: minval then maxval
-    std::vector<uint64_t> bwords; // m_vec words per bitmap (for the complement choice)
-    std::vector<uint32_t> bones;  // 1 bits per bitmap
-    uint32_t* d_words = nullptr;
-    BitmapMeta* d_bm = nullptr;
-    uint32_t* d_tiles = nullptr;
-    void* d_values = nullptr;
-    uint32_t vtype = 0;
-    DevIndex dev{};
-};
-
-struct wahgpu_batch {
-    wahgpu_ctx* ctx = nullptr;
-    uint32_t nq = 0, nterms = 0, nidx = 0;
-    uint32_t groups = 0, anb = 0, ntiles = 0;
-    DevIndex* d_idx = nullptr;
-    DevTerm* d_terms = nullptr;
-    DevQuery* d_queries = nullptr;
-    unsigned long long* d_counts = nullptr;
-    unsigned long long* d_start = nullptr;
-    uint32_t* d_rids = nullptr;
-    uint64_t rid_cap = 0;
-    uint32_t* d_dense = nullptr;
-    DevMeta* d_status = nullptr;
-    std::vector<unsigned long long> h_counts, h_start;
-    bool h_valid = false;
-};
 
 #define CUDA_TRY(ctx, call)                                                            \
     do {                                                                               \
@@ -88,19 +57,37 @@ extern "C" int wahgpu_index_from_triple(wahgpu_ctx* ctx, int kind, uint64_t nrow
         }
         x->bwords[j] = m.n;
     }
-    int rc = WAHGPU_OK;
-    const size_t tiles_bytes = (size_t)nobs * (x->ntiles + 1) * 8;
     x->d_words = static_cast<uint32_t*>(wg_alloc(ctx, std::max<uint64_t>(nbitmaps, 1) * 4));
     x->d_bm = static_cast<BitmapMeta*>(wg_alloc(ctx, std::max<size_t>(nobs, 1) * sizeof(BitmapMeta)));
-    x->d_tiles = static_cast<uint32_t*>(wg_alloc(ctx, std::max<size_t>(tiles_bytes, 8)));
-    uint32_t* d_ones = static_cast<uint32_t*>(wg_alloc(ctx, std::max<size_t>(nobs, 1) * 4));
-    DevMeta* d_st = static_cast<DevMeta*>(wg_alloc(ctx, sizeof(DevMeta)));
-    if (!x->d_words || !x->d_bm || !x->d_tiles || !d_ones || !d_st) {
+    if (!x->d_words || !x->d_bm) {
         wahgpu_index_free(x);
         return wg_fail(ctx, WAHGPU_ENOMEM, "index allocation failed");
     }
     CUDA_TRY(ctx, cudaMemcpyAsync(x->d_words, bitmaps, nbitmaps * 4, cudaMemcpyHostToDevice, ctx->stream));
     CUDA_TRY(ctx, cudaMemcpyAsync(x->d_bm, bm.data(), nobs * sizeof(BitmapMeta), cudaMemcpyHostToDevice, ctx->stream));
+    int rc = wg_index_attach(x);
+    if (rc) { wahgpu_index_free(x); return rc; }
+    *out = x;
+    return WAHGPU_OK;
+}
+
+// Second half of building an index, shared by the triple upload and the
+// device build: x->d_words / d_bm / bwords / keys are set; computes the
+// per-bitmap tile index and 1-bit counts and validates the words.
+int wg_index_attach(wahgpu_index* x) {
+    wahgpu_ctx* ctx = x->ctx;
+    const uint32_t nobs = x->nobs;
+    x->ntiles = (x->groups + (x->anb ? 1 : 0) + RT - 1) / RT;
+    const size_t tiles_bytes = (size_t)nobs * (x->ntiles + 1) * 8;
+    x->d_tiles = static_cast<uint32_t*>(wg_alloc(ctx, std::max<size_t>(tiles_bytes, 8)));
+    uint32_t* d_ones = static_cast<uint32_t*>(wg_alloc(ctx, std::max<size_t>(nobs, 1) * 4));
+    DevMeta* d_st = static_cast<DevMeta*>(wg_alloc(ctx, sizeof(DevMeta)));
+    if (!x->d_tiles || !d_ones || !d_st) {
+        wg_free(ctx, d_ones);
+        wg_free(ctx, d_st);
+        return wg_fail(ctx, WAHGPU_ENOMEM, "index allocation failed");
+    }
+    int rc = WAHGPU_OK;
     CUDA_TRY(ctx, cudaMemsetAsync(d_st, 0, sizeof(DevMeta), ctx->stream));
     if (nobs) {
         const uint32_t threads = 256, blocks = (nobs * 32 + threads - 1) / threads;
@@ -118,10 +105,10 @@ extern "C" int wahgpu_index_from_triple(wahgpu_ctx* ctx, int kind, uint64_t nrow
     wg_free(ctx, d_st);
     if (st.status == DEV_ERR_FORMAT) rc = wg_fail(ctx, WAHGPU_EFORMAT, "a bitmap holds a fill word of length 0");
     else if (st.status) rc = wg_fail(ctx, WAHGPU_ERANGE, "a bitmap holds more bits than the index has rows");
-    if (rc) { wahgpu_index_free(x); return rc; }
+    if (rc) return rc;
     x->dev.words = x->d_words; x->dev.bm = x->d_bm; x->dev.tiles = x->d_tiles;
     x->dev.values = nullptr; x->dev.nobs = nobs; x->dev.vtype = 0; x->dev.ntiles = x->ntiles;
-    *out = x;
+    if (x->d_values) { x->dev.values = x->d_values; x->dev.vtype = x->vtype; }
     return WAHGPU_OK;
 }
 

@@ -1,0 +1,43 @@
+// Internal state behind the opaque index and batch handles of
+// include/wahgpu.h, shared by the index store (wah_index.cu) and the device
+// index builder (wah_build.cu).
+#ifndef WAH_INDEX_INTERNAL_H
+#define WAH_INDEX_INTERNAL_H
+#include <vector>
+#include "wah_range.cuh"
+#include "wah_api_internal.h"
+
+struct wahgpu_index {
+    wahgpu_ctx* ctx = nullptr;
+    int kind = 0;                 // WAHGPU_RELIC / WAHGPU_BIN
+    uint32_t nrows = 0, groups = 0, anb = 0, nobs = 0, ntiles = 0;
+    std::vector<double> keys;     // relic: distinct values; bin: minval then maxval
+    std::vector<uint64_t> bwords; // m_vec words per bitmap (for the complement choice)
+    std::vector<uint32_t> bones;  // 1 bits per bitmap
+    uint32_t* d_words = nullptr;
+    wah::BitmapMeta* d_bm = nullptr;
+    uint32_t* d_tiles = nullptr;
+    void* d_values = nullptr;
+    uint32_t vtype = 0;
+    wah::DevIndex dev{};
+};
+
+struct wahgpu_batch {
+    wahgpu_ctx* ctx = nullptr;
+    uint32_t nq = 0, nterms = 0, nidx = 0;
+    uint32_t groups = 0, anb = 0, ntiles = 0;
+    wah::DevIndex* d_idx = nullptr;
+    wah::DevTerm* d_terms = nullptr;
+    wah::DevQuery* d_queries = nullptr;
+    unsigned long long* d_counts = nullptr;
+    unsigned long long* d_start = nullptr;
+    uint32_t* d_rids = nullptr;
+    uint64_t rid_cap = 0;
+    uint32_t* d_dense = nullptr;
+    wah::DevMeta* d_status = nullptr;
+    std::vector<unsigned long long> h_counts, h_start;
+    bool h_valid = false;
+};
+
+int wg_index_attach(wahgpu_index* x);
+#endif

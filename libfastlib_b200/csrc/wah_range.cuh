@@ -94,6 +94,7 @@ struct RangeShared {
     unsigned long long base;
 };
 
+#ifndef WAH_RANGE_TYPES_ONLY
 __device__ __forceinline__ bool pass_cmp(double v, uint32_t lop, double lo, uint32_t rop, double hi) {
     const bool a = lop == 0 ? true : (lop == 1 ? lo < v : lo <= v);
     const bool b = rop == 0 ? true : (rop == 1 ? v < hi : v <= hi);
@@ -319,6 +320,8 @@ __global__ void k_index_tiles(const uint32_t* __restrict__ words, BitmapMeta* __
         else if ((uint64_t)carry * 31u + m.anb > nrows) atomicExch(&status->status, DEV_ERR_RANGE);
     }
 }
+
+#endif  // WAH_RANGE_TYPES_ONLY
 
 }  // namespace wah
 #endif

@@ -50,6 +50,8 @@ class _Term(ctypes.Structure):
 
 RELIC, BIN = 1, 2
 TUNE_DENSE_TILE = 1
+TUNE_RANGE_ORDER = 2
+TUNE_RANGE_CTAS = 3
 DENSE_TILES = (1024, 2048, 4096)
 CMP_NONE, CMP_LT, CMP_LE = 0, 1, 2
 U32, F32, I32 = 0, 1, 2

@@ -165,6 +165,14 @@ extern "C" int wahgpu_ctx_set_tuning(wahgpu_ctx* ctx, int key, int64_t value) {
             return wg_fail(ctx, WAHGPU_EINVAL, "dense tile must be 1024, 2048 or 4096 groups, not %lld", (long long)value);
         ctx->dense_tile = (uint32_t)value;
         return WAHGPU_OK;
+    case WAHGPU_TUNE_RANGE_ORDER:
+        if (value != 0 && value != 1) return wg_fail(ctx, WAHGPU_EINVAL, "range order must be 0 or 1");
+        ctx->range_order = (uint32_t)value;
+        return WAHGPU_OK;
+    case WAHGPU_TUNE_RANGE_CTAS:
+        if (value < 0 || value > 32) return wg_fail(ctx, WAHGPU_EINVAL, "range CTAs per SM must be 0..32");
+        ctx->range_ctas = (uint32_t)value;
+        return WAHGPU_OK;
     default:
         return wg_fail(ctx, WAHGPU_EINVAL, "unknown tuning key %d", key);
     }
@@ -173,6 +181,8 @@ extern "C" int64_t wahgpu_ctx_get_tuning(wahgpu_ctx* ctx, int key) {
     if (!ctx) return WAHGPU_EINVAL;
     switch (key) {
     case WAHGPU_TUNE_DENSE_TILE: return ctx->dense_tile;
+    case WAHGPU_TUNE_RANGE_ORDER: return ctx->range_order;
+    case WAHGPU_TUNE_RANGE_CTAS: return ctx->range_ctas;
     default: return wg_fail(ctx, WAHGPU_EINVAL, "unknown tuning key %d", key);
     }
 }

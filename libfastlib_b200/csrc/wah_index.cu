@@ -8,6 +8,8 @@
 #include "wah_index_internal.h"
 
 #include <cuda_runtime.h>
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -71,6 +73,55 @@ extern "C" int wahgpu_index_from_triple(wahgpu_ctx* ctx, int kind, uint64_t nrow
     return WAHGPU_OK;
 }
 
+// Per tile, the bitmaps holding a 1 bit in it (ascending), so a range term
+// visits only bitmaps with data in the tile: pairs (tile, bitmap) emitted in
+// bitmap order, stably sorted by tile, cut into CSR offsets.
+static int build_tile_lists(wahgpu_index* x) {
+    wahgpu_ctx* ctx = x->ctx;
+    const uint32_t nobs = x->nobs, nt = x->ntiles;
+    x->d_tl_off = static_cast<uint32_t*>(wg_alloc(ctx, ((size_t)nt + 1) * 4));
+    if (!x->d_tl_off) return wg_fail(ctx, WAHGPU_ENOMEM, "index allocation failed");
+    if (nobs == 0) {
+        CUDA_TRY(ctx, cudaMemsetAsync(x->d_tl_off, 0, ((size_t)nt + 1) * 4, ctx->stream));
+        x->d_tl_bm = static_cast<uint32_t*>(wg_alloc(ctx, 4));
+        return x->d_tl_bm ? WAHGPU_OK : wg_fail(ctx, WAHGPU_ENOMEM, "index allocation failed");
+    }
+    std::vector<void*> tmp;
+    auto get = [&](size_t bytes) { void* p = wg_alloc(ctx, std::max<size_t>(bytes, 16)); if (p) tmp.push_back(p); return p; };
+    auto release = [&]() { cudaStreamSynchronize(ctx->stream); for (void* p : tmp) wg_free(ctx, p); };
+    uint32_t* cnt = static_cast<uint32_t*>(get(((size_t)nobs + 1) * 4));
+    if (!cnt) { release(); return wg_fail(ctx, WAHGPU_ENOMEM, "index allocation failed"); }
+    const uint32_t threads = 256, blocks = (nobs * 32 + threads - 1) / threads;
+    CUDA_TRY(ctx, cudaMemsetAsync(cnt + nobs, 0, 4, ctx->stream));
+    k_tile_touch<<<blocks, threads, 0, ctx->stream>>>(x->d_words, x->d_bm, nobs, 0, cnt, nullptr, nullptr, nullptr);
+    size_t tb = 0;
+    CUDA_TRY(ctx, cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, cnt, nobs + 1, ctx->stream));
+    void* t1 = get(tb);
+    if (!t1) { release(); return wg_fail(ctx, WAHGPU_ENOMEM, "index allocation failed"); }
+    CUDA_TRY(ctx, cub::DeviceScan::ExclusiveSum(t1, tb, cnt, cnt, nobs + 1, ctx->stream));
+    uint32_t npairs = 0;
+    CUDA_TRY(ctx, cudaMemcpyAsync(&npairs, cnt + nobs, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    uint32_t* pt = static_cast<uint32_t*>(get((size_t)npairs * 4));
+    uint32_t* pb = static_cast<uint32_t*>(get((size_t)npairs * 4));
+    uint32_t* st = static_cast<uint32_t*>(get((size_t)npairs * 4));
+    x->d_tl_bm = static_cast<uint32_t*>(wg_alloc(ctx, std::max<size_t>((size_t)npairs * 4, 16)));
+    if (!pt || !pb || !st || !x->d_tl_bm) { release(); return wg_fail(ctx, WAHGPU_ENOMEM, "index allocation failed"); }
+    k_tile_touch<<<blocks, threads, 0, ctx->stream>>>(x->d_words, x->d_bm, nobs, 1, nullptr, cnt, pt, pb);
+    int bits = 1;
+    while (bits < 32 && (1ull << bits) <= nt) ++bits;
+    tb = 0;
+    CUDA_TRY(ctx, cub::DeviceRadixSort::SortPairs(nullptr, tb, pt, st, pb, x->d_tl_bm, npairs, 0, bits, ctx->stream));
+    void* t2 = get(tb);
+    if (!t2) { release(); return wg_fail(ctx, WAHGPU_ENOMEM, "index allocation failed"); }
+    CUDA_TRY(ctx, cub::DeviceRadixSort::SortPairs(t2, tb, pt, st, pb, x->d_tl_bm, npairs, 0, bits, ctx->stream));
+    k_tile_offsets<<<(npairs + 1 + threads - 1) / threads, threads, 0, ctx->stream>>>(st, npairs, nt, x->d_tl_off);
+    ctx->launches += 5;
+    CUDA_TRY(ctx, cudaGetLastError());
+    release();
+    return WAHGPU_OK;
+}
+
 // Second half of building an index, shared by the triple upload and the
 // device build: x->d_words / d_bm / bwords / keys are set; computes the
 // per-bitmap tile index and 1-bit counts and validates the words.
@@ -106,7 +157,16 @@ int wg_index_attach(wahgpu_index* x) {
     if (st.status == DEV_ERR_FORMAT) rc = wg_fail(ctx, WAHGPU_EFORMAT, "a bitmap holds a fill word of length 0");
     else if (st.status) rc = wg_fail(ctx, WAHGPU_ERANGE, "a bitmap holds more bits than the index has rows");
     if (rc) return rc;
+    rc = build_tile_lists(x);
+    if (rc) return rc;
+    x->cum_words.assign(nobs + 1, 0);
+    x->cum_ones.assign(nobs + 1, 0);
+    for (uint32_t j = 0; j < nobs; ++j) {
+        x->cum_words[j + 1] = x->cum_words[j] + x->bwords[j];
+        x->cum_ones[j + 1] = x->cum_ones[j] + x->bones[j];
+    }
     x->dev.words = x->d_words; x->dev.bm = x->d_bm; x->dev.tiles = x->d_tiles;
+    x->dev.tl_off = x->d_tl_off; x->dev.tl_bm = x->d_tl_bm;
     x->dev.values = nullptr; x->dev.nobs = nobs; x->dev.vtype = 0; x->dev.ntiles = x->ntiles;
     if (x->d_values) { x->dev.values = x->d_values; x->dev.vtype = x->vtype; }
     return WAHGPU_OK;
@@ -133,6 +193,8 @@ extern "C" int wahgpu_index_free(wahgpu_index* x) {
     wg_free(ctx, x->d_words);
     wg_free(ctx, x->d_bm);
     wg_free(ctx, x->d_tiles);
+    wg_free(ctx, x->d_tl_off);
+    wg_free(ctx, x->d_tl_bm);
     wg_free(ctx, x->d_values);
     delete x;
     return WAHGPU_OK;
@@ -165,11 +227,20 @@ static bool pass_h(double v, int lop, double lo, int rop, double hi) {
 static int locate(wahgpu_ctx* ctx, const wahgpu_index* x, const wahgpu_term* t, DevTerm& out) {
     out = DevTerm{};
     out.lop = (uint32_t)t->lop; out.rop = (uint32_t)t->rop; out.lo = t->lo; out.hi = t->hi;
-    std::vector<uint8_t> cls(x->nobs);  // 0 none, 1 all, 2 some
-    for (uint32_t j = 0; j < x->nobs; ++j) {
-        if (x->kind == WAHGPU_RELIC) {
-            cls[j] = pass_h(x->keys[j], t->lop, t->lo, t->rop, t->hi) ? 1 : 0;
-        } else {
+    uint32_t h0 = 0, h1 = 0, nc = 0;
+    if (x->kind == WAHGPU_RELIC) {
+        // keys ascending: the passing keys are one interval, found by the
+        // same double comparisons (qContinuousRange::inRange) as the scan
+        const auto& k = x->keys;
+        uint32_t a = 0, b = x->nobs;
+        if (t->lop == 1) a = (uint32_t)(std::upper_bound(k.begin(), k.end(), t->lo) - k.begin());
+        else if (t->lop == 2) a = (uint32_t)(std::lower_bound(k.begin(), k.end(), t->lo) - k.begin());
+        if (t->rop == 1) b = (uint32_t)(std::lower_bound(k.begin(), k.end(), t->hi) - k.begin());
+        else if (t->rop == 2) b = (uint32_t)(std::upper_bound(k.begin(), k.end(), t->hi) - k.begin());
+        if (b > a) { h0 = a; h1 = b; }
+    } else {
+        std::vector<uint8_t> cls(x->nobs);  // 0 none, 1 all, 2 some
+        for (uint32_t j = 0; j < x->nobs; ++j) {
             const double mn = x->keys[j], mx = x->keys[x->nobs + j];
             if (x->bones[j] == 0 || !(mn <= mx)) { cls[j] = 0; continue; }
             const bool pmn = pass_h(mn, t->lop, t->lo, t->rop, t->hi), pmx = pass_h(mx, t->lop, t->lo, t->rop, t->hi);
@@ -181,27 +252,38 @@ static int locate(wahgpu_ctx* ctx, const wahgpu_index* x, const wahgpu_term* t, 
                 cls[j] = (below || above) ? 0 : 2;
             }
         }
-    }
-    uint32_t h0 = x->nobs, h1 = x->nobs, nc = 0;
-    for (uint32_t j = 0; j < x->nobs; ++j) {
-        if (cls[j] == 1) { if (h0 == x->nobs) h0 = j; h1 = j + 1; }
-        else if (cls[j] == 2) {
-            if (nc >= 2) return wg_fail(ctx, WAHGPU_EINVAL, "more than two bins straddle the range");
-            out.cand[nc++] = j;
+        h0 = x->nobs; h1 = x->nobs;
+        for (uint32_t j = 0; j < x->nobs; ++j) {
+            if (cls[j] == 1) { if (h0 == x->nobs) h0 = j; h1 = j + 1; }
+            else if (cls[j] == 2) {
+                if (nc >= 2) return wg_fail(ctx, WAHGPU_EINVAL, "more than two bins straddle the range");
+                out.cand[nc++] = j;
+            }
         }
+        if (h0 == x->nobs) { h0 = 0; h1 = 0; }
+        for (uint32_t j = h0; j < h1; ++j)
+            if (cls[j] == 0 && x->bones[j] != 0)
+                return wg_fail(ctx, WAHGPU_EINVAL, "bitmaps wholly inside the range are not contiguous");
+            else if (cls[j] == 2)
+                return wg_fail(ctx, WAHGPU_EINVAL, "bitmaps wholly inside the range are not contiguous");
     }
-    if (h0 == x->nobs) { h0 = 0; h1 = 0; }
-    for (uint32_t j = h0; j < h1; ++j)
-        if (cls[j] != 1) return wg_fail(ctx, WAHGPU_EINVAL, "bitmaps wholly inside the range are not contiguous");
     if (nc > 0 && !x->d_values)
         return wg_fail(ctx, WAHGPU_EINVAL, "range needs row checks but the index has no raw values attached");
     out.h0 = h0; out.h1 = h1; out.ncand = nc;
     // sumBins reads the complement when the range holds more than half the
     // index's words (src/index.cpp:6490); the bits are the same either way
-    uint64_t in = 0, all = 0;
-    for (uint32_t j = 0; j < x->nobs; ++j) { all += x->bwords[j]; if (j >= h0 && j < h1) in += x->bwords[j]; }
+    const uint64_t in = x->cum_words[h1] - x->cum_words[h0], all = x->cum_words[x->nobs];
     out.flip = (2 * in > all) ? 1u : 0u;
     return WAHGPU_OK;
+}
+
+// Estimated hits of a located term (its bitmaps' 1 bits), for ordering the
+// terms of a query: the most selective first, so a tile whose AND is
+// already empty skips the rest.
+static uint64_t term_estimate(const wahgpu_index* x, const DevTerm& d) {
+    uint64_t e = x->cum_ones[d.h1] - x->cum_ones[d.h0];
+    for (uint32_t c = 0; c < d.ncand; ++c) e += x->bones[d.cand[c]];
+    return e;
 }
 
 // ------------------------------------------------------------------ batches
@@ -226,8 +308,12 @@ extern "C" int wahgpu_batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, co
     }
     std::vector<DevQuery> dq(nq);
     for (uint32_t q = 0; q < nq; ++q) {
-        if (query_offsets[q + 1] <= query_offsets[q]) return wg_fail(ctx, WAHGPU_EINVAL, "query %u has no term", q);
+        if (query_offsets[q + 1] <= query_offsets[q] || query_offsets[q + 1] > nt)
+            return wg_fail(ctx, WAHGPU_EINVAL, "query %u has no term", q);
         dq[q].t0 = query_offsets[q]; dq[q].t1 = query_offsets[q + 1];
+        std::stable_sort(dt.begin() + dq[q].t0, dt.begin() + dq[q].t1, [&](const DevTerm& a, const DevTerm& b) {
+            return term_estimate(idx[a.index], a) < term_estimate(idx[b.index], b);
+        });
     }
     std::vector<DevIndex> di;
     for (auto* x : idx) di.push_back(x->dev);
@@ -272,10 +358,18 @@ extern "C" int wahgpu_batch_run(wahgpu_batch* B) {
     a.counts = B->d_counts; a.rids = B->d_rids; a.rid_cap = B->rid_cap; a.rid_start = B->d_start;
     a.dense = B->d_dense;
     a.recs = recs; a.sync = sync; a.nitems = nitems; a.status = B->d_status;
-    static bool attr = false;
+    // tile by tile when only counts are wanted and the tuning asks for it
+    a.tile_major = (ctx->range_order == 1 && !B->d_rids && !B->d_dense) ? 1u : 0u;
+    static int per_sm = 0;
     const size_t sm = sizeof(RangeShared);
-    if (!attr) { cudaFuncSetAttribute(k_range, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); attr = true; }
-    k_range<<<nitems, RTHREADS, sm, ctx->stream>>>(a);
+    if (!per_sm) {
+        cudaFuncSetAttribute(k_range, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_range, RTHREADS, sm);
+        if (per_sm < 1) per_sm = 1;
+    }
+    const uint32_t ctas = ctx->range_ctas ? std::min<uint32_t>(ctx->range_ctas, (uint32_t)per_sm) : (uint32_t)per_sm;
+    const uint32_t grid = std::min<uint32_t>(nitems, ctas * (uint32_t)ctx->sm_count);
+    k_range<<<grid, RTHREADS, sm, ctx->stream>>>(a);
     ctx->launches++;
     CUDA_TRY(ctx, cudaGetLastError());
     B->h_valid = false;

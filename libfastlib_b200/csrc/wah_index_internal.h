@@ -14,9 +14,12 @@ struct wahgpu_index {
     std::vector<double> keys;     // relic: distinct values; bin: minval then maxval
     std::vector<uint64_t> bwords; // m_vec words per bitmap (for the complement choice)
     std::vector<uint32_t> bones;  // 1 bits per bitmap
+    std::vector<uint64_t> cum_words, cum_ones;  // prefix sums of bwords / bones
     uint32_t* d_words = nullptr;
     wah::BitmapMeta* d_bm = nullptr;
     uint32_t* d_tiles = nullptr;
+    uint32_t* d_tl_off = nullptr;     // per tile: bitmaps with a 1 bit there (CSR)
+    uint32_t* d_tl_bm = nullptr;
     void* d_values = nullptr;
     uint32_t vtype = 0;
     wah::DevIndex dev{};

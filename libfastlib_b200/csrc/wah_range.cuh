@@ -47,6 +47,8 @@ struct DevIndex {
     const uint32_t* words;     // word pool (the bitmaps' serialized arrays)
     const BitmapMeta* bm;      // nobs entries
     const uint32_t* tiles;     // nobs x (ntiles+1) x {word index, first group}
+    const uint32_t* tl_off;    // ntiles+1: tile k's bitmaps are tl_bm[tl_off[k], tl_off[k+1])
+    const uint32_t* tl_bm;     // bitmaps holding a 1 bit in each tile, ascending
     const void* values;        // raw column (nrows), or null
     uint32_t nobs;
     uint32_t vtype;            // 0 uint32, 1 float32, 2 int32
@@ -84,6 +86,7 @@ struct RangeArgs {
     uint32_t* dense;          // dense hit words of query 0 (or null)
     TileRec* recs; LaunchSync* sync; uint32_t nitems;
     DevMeta* status;
+    uint32_t tile_major;      // 1: items ordered tile by tile (counts only)
 };
 
 struct RangeShared {
@@ -179,98 +182,134 @@ __device__ __forceinline__ void warp_or_bitmap(RangeShared& S, const DevIndex& I
     }
 }
 
+// Lower bound of v in the ascending list a[0, n).
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* __restrict__ a, uint32_t n, uint32_t v) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t m = (lo + hi) >> 1;
+        if (__ldg(a + m) < v) lo = m + 1; else hi = m;
+    }
+    return lo;
+}
+
+// Persistent: every CTA claims items until none is left.
 __global__ void __launch_bounds__(RTHREADS) k_range(RangeArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     RangeShared& S = *reinterpret_cast<RangeShared*>(smem_raw);
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-    if (tid == 0) { S.hdr[0] = claim_tile(A.sync); S.hdr[1] = ld_cg(&A.sync->epoch); }
-    __syncthreads();
-    const uint32_t item = S.hdr[0], epoch = S.hdr[1];
-    const uint32_t q = item / A.ntiles, k = item % A.ntiles;
+    if (tid == 0) S.hdr[1] = ld_cg(&A.sync->epoch);
     const uint32_t G = A.groups, anb = A.anb;
     const uint32_t GX = G + (anb > 0 ? 1u : 0u);  // groups incl. the active one
-    const uint32_t g0 = k * (uint32_t)RT, g1 = min(g0 + (uint32_t)RT, GX);
-    const uint32_t ng = g1 > g0 ? g1 - g0 : 0u;
     const uint32_t lastmask = anb > 0 ? (((1u << anb) - 1u) << (31u - anb)) : ALLONES;
-    const DevQuery Q = A.queries[q];
+    while (true) {
+        if (tid == 0) S.hdr[0] = claim_tile(A.sync);
+        __syncthreads();
+        const uint32_t item = S.hdr[0], epoch = S.hdr[1];
+        if (item >= A.nitems) break;
+        // query-major items keep a query's row ids contiguous (look-back in
+        // claim order); tile-major items let the queries of one batch share
+        // each tile's bitmap words in L2 (counts only)
+        const uint32_t q = A.tile_major ? item % A.nq : item / A.ntiles;
+        const uint32_t k = A.tile_major ? item / A.nq : item % A.ntiles;
+        const uint32_t g0 = k * (uint32_t)RT, g1 = min(g0 + (uint32_t)RT, GX);
+        const uint32_t ng = g1 > g0 ? g1 - g0 : 0u;
+        const DevQuery Q = A.queries[q];
 
-    for (uint32_t l = tid; l < RT; l += RTHREADS) S.acc[l] = ALLONES;
-    for (uint32_t t = Q.t0; t < Q.t1; ++t) {
-        const DevTerm T = A.terms[t];
-        const DevIndex I = A.idx[T.index];
-        for (uint32_t l = tid; l < RT; l += RTHREADS) S.tmp[l] = 0u;
-        __syncthreads();
-        // wholly-inside bitmaps (or their complement)
-        const uint32_t nsel = T.flip ? (T.h0 + (I.nobs - T.h1)) : (T.h1 - T.h0);
-        for (uint32_t j = warp; j < nsel; j += RWARPS) {
-            uint32_t b;
-            if (T.flip) b = j < T.h0 ? j : T.h1 + (j - T.h0);
-            else b = T.h0 + j;
-            warp_or_bitmap(S, I, b, k, g0, g1, G, anb, nullptr);
-        }
-        __syncthreads();
-        if (T.flip) {
-            for (uint32_t l = tid; l < ng; l += RTHREADS) {
-                const uint32_t msk = (g0 + l == G && anb > 0) ? lastmask : ALLONES;
-                S.tmp[l] ^= msk;
+        for (uint32_t l = tid; l < RT; l += RTHREADS) S.acc[l] = ALLONES;
+        for (uint32_t t = Q.t0; t < Q.t1; ++t) {
+            const DevTerm T = A.terms[t];
+            const DevIndex I = A.idx[T.index];
+            for (uint32_t l = tid; l < RT; l += RTHREADS) S.tmp[l] = 0u;
+            if (tid == 0) {
+                // the term's bitmaps holding a 1 bit in this tile
+                const uint32_t o0 = __ldg(I.tl_off + k), o1 = __ldg(I.tl_off + k + 1);
+                const uint32_t a = lower_bound_u32(I.tl_bm + o0, o1 - o0, T.h0);
+                const uint32_t b = lower_bound_u32(I.tl_bm + o0, o1 - o0, T.h1);
+                S.hdr[2] = o0; S.hdr[3] = o0 + a; S.hdr[4] = o0 + b; S.hdr[5] = o1;
             }
             __syncthreads();
+            // wholly-inside bitmaps, or their complement: entries [e0, e1) of
+            // the tile list, or [o0, e0) and [e1, o1)
+            const uint32_t o0 = S.hdr[2], e0 = S.hdr[3], e1 = S.hdr[4], o1 = S.hdr[5];
+            const uint32_t nsel = T.flip ? (e0 - o0) + (o1 - e1) : (e1 - e0);
+            for (uint32_t j = warp; j < nsel; j += RWARPS) {
+                uint32_t e;
+                if (T.flip) e = j < e0 - o0 ? o0 + j : e1 + (j - (e0 - o0));
+                else e = e0 + j;
+                warp_or_bitmap(S, I, __ldg(I.tl_bm + e), k, g0, g1, G, anb, nullptr);
+            }
+            __syncthreads();
+            if (T.flip) {
+                for (uint32_t l = tid; l < ng; l += RTHREADS) {
+                    const uint32_t msk = (g0 + l == G && anb > 0) ? lastmask : ALLONES;
+                    S.tmp[l] ^= msk;
+                }
+                __syncthreads();
+            }
+            // edge bitmaps: rows checked against the raw values
+            for (uint32_t c = warp; c < T.ncand; c += RWARPS)
+                warp_or_bitmap(S, I, T.cand[c], k, g0, g1, G, anb, &T);
+            __syncthreads();
+            uint32_t any = 0;
+            for (uint32_t l = tid; l < RT; l += RTHREADS) { const uint32_t v = S.acc[l] & S.tmp[l]; S.acc[l] = v; any |= v; }
+            // an empty AND ends the query's work on this tile
+            if (!__syncthreads_or(any != 0u)) break;
         }
-        // edge bitmaps: rows checked against the raw values
-        for (uint32_t c = warp; c < T.ncand; c += RWARPS)
-            warp_or_bitmap(S, I, T.cand[c], k, g0, g1, G, anb, &T);
-        __syncthreads();
-        for (uint32_t l = tid; l < RT; l += RTHREADS) S.acc[l] &= S.tmp[l];
-        __syncthreads();
-    }
-    // ---- counts and row ids
-    const uint32_t l0 = tid * RGPT;
-    uint32_t cnt = 0;
+        // ---- counts and row ids
+        const uint32_t l0 = tid * RGPT;
+        uint32_t cnt = 0;
 #pragma unroll
-    for (int j = 0; j < RGPT; ++j) {
-        const uint32_t l = l0 + j;
-        if (l < ng) {
-            uint32_t v = S.acc[l];
-            if (g0 + l == G && anb > 0) v &= lastmask;
-            S.acc[l] = v;
-            cnt += __popc(v);
-        } else if (l < RT) {
-            S.acc[l] = 0u;
-        }
-    }
-    uint64_t total;
-    const uint64_t ex = block_exscan64(cnt, S.scan, total);
-    if (warp == 0) {
-        uint64_t prefix; uint32_t pa, pb;
-        const bool ok = lookback64(A.recs, item, epoch, total, 0, 0, prefix, pa, pb);
-        if (lane == 0) {
-            if (!ok) atomicExch(&A.status->status, DEV_ERR_TIMEOUT);
-            S.base = prefix;
-            if (total) atomicAdd(&A.counts[q], (unsigned long long)total);
-            if (k == 0) A.rid_start[q] = prefix;
-        }
-    }
-    __syncthreads();
-    if (A.rids) {
-        uint64_t off = S.base + ex;
         for (int j = 0; j < RGPT; ++j) {
             const uint32_t l = l0 + j;
-            if (l >= ng) break;
-            uint32_t bits = S.acc[l];
-            const uint32_t rbase = (g0 + l) * 31u;
-            while (bits) {
-                const uint32_t hb = 31u - __clz(bits);
-                if (off < A.rid_cap) A.rids[off] = rbase + (30u - hb);
-                ++off;
-                bits &= ~(1u << hb);
+            if (l < ng) {
+                uint32_t v = S.acc[l];
+                if (g0 + l == G && anb > 0) v &= lastmask;
+                S.acc[l] = v;
+                cnt += __popc(v);
+            } else if (l < RT) {
+                S.acc[l] = 0u;
             }
         }
+        if (A.tile_major) {
+            cnt = __reduce_add_sync(0xffffffffu, cnt);
+            if (lane == 0 && cnt) atomicAdd(&A.counts[q], (unsigned long long)cnt);
+            __syncthreads();
+            continue;
+        }
+        uint64_t total;
+        const uint64_t ex = block_exscan64(cnt, S.scan, total);
+        if (warp == 0) {
+            uint64_t prefix; uint32_t pa, pb;
+            const bool ok = lookback64(A.recs, item, epoch, total, 0, 0, prefix, pa, pb);
+            if (lane == 0) {
+                if (!ok) atomicExch(&A.status->status, DEV_ERR_TIMEOUT);
+                S.base = prefix;
+                if (total) atomicAdd(&A.counts[q], (unsigned long long)total);
+                if (k == 0) A.rid_start[q] = prefix;
+            }
+        }
+        __syncthreads();
+        if (A.rids) {
+            uint64_t off = S.base + ex;
+            for (int j = 0; j < RGPT; ++j) {
+                const uint32_t l = l0 + j;
+                if (l >= ng) break;
+                uint32_t bits = S.acc[l];
+                const uint32_t rbase = (g0 + l) * 31u;
+                while (bits) {
+                    const uint32_t hb = 31u - __clz(bits);
+                    if (off < A.rid_cap) A.rids[off] = rbase + (30u - hb);
+                    ++off;
+                    bits &= ~(1u << hb);
+                }
+            }
+        }
+        if (A.dense && q == 0) {
+            for (uint32_t l = tid; l < ng; l += RTHREADS) A.dense[g0 + l] = S.acc[l];
+        }
+        __syncthreads();
     }
-    if (A.dense && q == 0) {
-        for (uint32_t l = tid; l < ng; l += RTHREADS) A.dense[g0 + l] = S.acc[l];
-    }
-    __syncthreads();
-    if (tid == 0) finish_tile(A.sync, A.nitems);
+    if (tid == 0) finish_tile(A.sync, gridDim.x);
 }
 
 // Per-bitmap group-tile index of an attached index: one warp per bitmap
@@ -319,6 +358,80 @@ __global__ void k_index_tiles(const uint32_t* __restrict__ words, BitmapMeta* __
         if (bad) atomicExch(&status->status, DEV_ERR_FORMAT);
         else if ((uint64_t)carry * 31u + m.anb > nrows) atomicExch(&status->status, DEV_ERR_RANGE);
     }
+}
+
+// Tiles of RT groups in which bitmap b holds a 1 bit, each once and in
+// order (one warp per bitmap).  Pass 0 counts them into cnt[b]; pass 1
+// writes (tile, bitmap) pairs from pos[b].
+__global__ void k_tile_touch(const uint32_t* __restrict__ words, const BitmapMeta* __restrict__ bm,
+                             uint32_t nobs, int pass, uint32_t* __restrict__ cnt,
+                             const uint32_t* __restrict__ pos, uint32_t* __restrict__ out_tile,
+                             uint32_t* __restrict__ out_bm) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (b >= nobs) return;
+    const BitmapMeta m = bm[b];
+    const uint32_t* w = words + m.wstart;
+    uint32_t carry = 0;        // first group of the next word
+    int64_t last = -1;         // last tile emitted
+    uint32_t n = 0;            // tiles emitted so far
+    const uint32_t o = pass ? pos[b] : 0u;
+    for (uint32_t base = 0; base < m.n; base += 32) {
+        const uint32_t i = base + lane;
+        const bool in = i < m.n;
+        const uint32_t wd = in ? __ldg(w + i) : 0u;
+        const uint32_t c = in ? wgroups(wd) : 0u;
+        uint32_t x = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) { uint32_t t = __shfl_up_sync(0xffffffffu, x, d); if (lane >= (uint32_t)d) x += t; }
+        const uint32_t p = carry + x - c;
+        const bool bits = in && c > 0 && (wd >= HEADER1 || (wd <= ALLONES && wd != 0u));
+        // tiles [k0, k1] of this word, minus those an earlier word emitted
+        int64_t k0 = bits ? (int64_t)(p / RT) : 0, k1 = bits ? (int64_t)((p + c - 1u) / RT) : -1;
+        int64_t prev = bits ? k1 : -1;  // highest tile of lanes up to this one
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int64_t t = __shfl_up_sync(0xffffffffu, prev, d);
+            if (lane >= (uint32_t)d) prev = max(prev, t);
+        }
+        int64_t before = __shfl_up_sync(0xffffffffu, prev, 1);
+        if (lane == 0) before = -1;
+        before = max(before, last);
+        if (bits) k0 = max(k0, before + 1);
+        const uint32_t mine = (bits && k1 >= k0) ? (uint32_t)(k1 - k0 + 1) : 0u;
+        uint32_t ex = mine;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) { uint32_t t = __shfl_up_sync(0xffffffffu, ex, d); if (lane >= (uint32_t)d) ex += t; }
+        if (pass && mine) {
+            uint32_t q = o + n + ex - mine;
+            for (int64_t k = k0; k <= k1; ++k, ++q) { out_tile[q] = (uint32_t)k; out_bm[q] = b; }
+        }
+        n += __shfl_sync(0xffffffffu, ex, 31);
+        last = max(last, __shfl_sync(0xffffffffu, prev, 31));
+        carry += __shfl_sync(0xffffffffu, x, 31);
+    }
+    // the active bits form the group after the whole words
+    if (lane == 0) {
+        if (m.anb > 0 && (m.aval & ((1u << m.anb) - 1u)) != 0u) {
+            const int64_t k = carry / RT;
+            if (k > last) {
+                if (pass) { out_tile[o + n] = (uint32_t)k; out_bm[o + n] = b; }
+                ++n;
+            }
+        }
+        if (!pass) cnt[b] = n;
+    }
+}
+
+// CSR offsets of the tile-sorted pairs: off[k] = first pair of tile k.
+__global__ void k_tile_offsets(const uint32_t* __restrict__ tile, uint32_t npairs, uint32_t ntiles,
+                               uint32_t* __restrict__ off) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e > npairs) return;
+    const uint32_t k = e < npairs ? tile[e] : ntiles;
+    const uint32_t kp = e > 0 ? tile[e - 1] : 0u;
+    const uint32_t from = e > 0 ? kp + 1u : 0u;
+    for (uint32_t t = from; t <= k && t <= ntiles; ++t) off[t] = e;  // tiles kp+1 .. k start here
 }
 
 #endif  // WAH_RANGE_TYPES_ONLY

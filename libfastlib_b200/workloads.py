@@ -88,3 +88,94 @@ def canonical_wah(groups: np.ndarray, anb: int = 0, aval: int = 0) -> np.ndarray
 def raw_wah_operand(seed: int, nbits: int, density: float, device: str = "cpu") -> np.ndarray:
     groups, anb, aval = groups_from_runs(geometric_runs(seed, nbits, density), device)
     return canonical_wah(groups, anb, aval)
+
+
+# ---------------------------------------------------------------- range workloads
+# Columns are generated on the device with a seeded torch generator, so a
+# workload is the same on every run of the same GPU model.
+
+def _gen(seed: int, device: str):
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    return g
+
+
+def zipf_column(seed: int, n: int, s: float, ranks: int, device: str = "cuda"):
+    """Ranks 1..`ranks` drawn with P(k) ~ k^-s (inverse CDF), as float64."""
+    import torch
+    g = _gen(seed, device)
+    k = torch.arange(1, ranks + 1, device=device, dtype=torch.float64)
+    cdf = torch.cumsum(k.pow(-s), 0)
+    cdf /= cdf[-1].clone()
+    u = torch.rand(n, generator=g, device=device, dtype=torch.float64)
+    return (torch.searchsorted(cdf, u).clamp_(max=ranks - 1) + 1).to(torch.float64)
+
+
+def mixture_column(seed: int, n: int, device: str = "cuda"):
+    """float32: with probability 0.7 Normal(0, 1), else a Zipf(1.2) rank over
+    10^5 values (the binned range workload's column)."""
+    import torch
+    g = _gen(seed, device)
+    norm = torch.randn(n, generator=g, device=device, dtype=torch.float32)
+    pick = torch.rand(n, generator=g, device=device) < 0.7
+    z = zipf_column(seed + 1, n, 1.2, 100_000, device).to(torch.float32)
+    return torch.where(pick, norm, z)
+
+
+def uniform_int_column(seed: int, n: int, card: int, device: str = "cuda", dtype=None):
+    import torch
+    g = _gen(seed, device)
+    t = torch.randint(0, card, (n,), generator=g, device=device, dtype=torch.int64)
+    return t.to(dtype or torch.int32)
+
+
+def normal_column(seed: int, n: int, device: str = "cuda"):
+    import torch
+    return torch.randn(n, generator=_gen(seed, device), device=device, dtype=torch.float32)
+
+
+def bin_edge_term(rng, keys: np.ndarray, nobs: int, span: int):
+    """A range over `span` consecutive bins whose two ends fall inside the
+    first and last bin (so both edge bins need row checks): (lo, hi) for
+    lo <= x < hi."""
+    span = max(1, min(span, nobs - 2))
+    b = int(rng.integers(1, max(2, nobs - span)))
+    e = min(b + span - 1, nobs - 1)
+    mn, mx = keys[:nobs], keys[nobs:]
+    lo = mn[b] + rng.random() * (mx[b] - mn[b])
+    hi = mn[e] + rng.random() * (mx[e] - mn[e])
+    if hi <= lo:
+        hi = np.nextafter(lo, np.inf)
+    return float(lo), float(hi)
+
+
+def binned_range_queries(seed: int, keys: np.ndarray, nobs: int, nq: int = 1000, max_span: int = 500):
+    """The binned range workload's queries: bin span uniform in [1, max_span],
+    start bin uniform, both ends jittered inside their edge bins."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return [bin_edge_term(rng, keys, nobs, int(rng.integers(1, max_span + 1))) for _ in range(nq)]
+
+
+def conjunctive_queries(seed: int, columns, nq: int, max_terms: int = 4):
+    """WHERE clauses of 1..max_terms distinct columns, each a range of uneven
+    span.  columns: list of dicts {kind: 'relic'|'bin', card | (keys, nobs)};
+    returns [[(column, lo, hi), ...], ...] for lo <= x < hi."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for _ in range(nq):
+        k = int(rng.integers(1, max_terms + 1))
+        cols = rng.choice(len(columns), size=min(k, len(columns)), replace=False)
+        q = []
+        for c in cols:
+            col = columns[int(c)]
+            if col["kind"] == "relic":
+                card = col["card"]
+                span = int(rng.integers(1, max(2, card // 2 + 1)))
+                lo = int(rng.integers(0, max(1, card - span + 1)))
+                q.append((int(c), float(lo), float(lo + span)))
+            else:
+                span = int(rng.integers(1, col.get("max_span", 256) + 1))
+                q.append((int(c),) + bin_edge_term(rng, col["keys"], col["nobs"], span))
+        out.append(q)
+    return out

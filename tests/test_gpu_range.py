@@ -179,3 +179,45 @@ def test_hit_bitvector_is_compressed_result(gpu_ctx):
     assert np.array_equal(hits.rids(), rids)
     dense = oracle.decompress(hits.write())
     assert np.array_equal(oracle.compress(dense)[0], hits.write())
+
+
+def test_relic_all_comparisons_and_orders(gpu_ctx):
+    """Every operator pair on a relic index (binary-search locate) and both
+    batch work orders give the scan's counts."""
+    import libfastlib_b200 as L
+    rng = np.random.default_rng(21)
+    n = 200_003
+    vals = rng.integers(0, 5000, n).astype(np.uint32)
+    idx = L.Index.build(gpu_ctx, L.RELIC, vals)
+    bidx = L.Index.build(gpu_ctx, L.BIN, rng.normal(0, 1, n).astype(np.float32), nbins=64)
+    f = vals.astype(np.float64)
+    ops = [(L.CMP_NONE, L.CMP_LT), (L.CMP_LT, L.CMP_LE), (L.CMP_LE, L.CMP_NONE), (L.CMP_LE, L.CMP_LE), (L.CMP_LT, L.CMP_LT)]
+    queries, want = [], []
+    for i in range(60):
+        lo, hi = sorted(rng.integers(-5, 5005, 2).astype(float) + rng.choice([0.0, 0.5]))
+        lop, rop = ops[i % len(ops)]
+        m = np.ones(n, bool)
+        if lop == L.CMP_LT: m &= lo < f
+        if lop == L.CMP_LE: m &= lo <= f
+        if rop == L.CMP_LT: m &= f < hi
+        if rop == L.CMP_LE: m &= f <= hi
+        t = idx.term(lo if lop else None, hi if rop else None, lop=lop or L.CMP_LE, rop=rop or L.CMP_LT)
+        c, rids, _ = L.evaluate(gpu_ctx, [t])
+        assert c == m.sum() and np.array_equal(rids, np.flatnonzero(m)), (i, lo, hi, lop, rop)
+        queries.append([t, bidx.term(-0.5, 0.7)] if i % 2 else [t])
+        want.append(c if i % 2 == 0 else None)
+    B = L.Batch(gpu_ctx, queries, 0)
+    try:
+        for order in (0, 1):
+            gpu_ctx.set_tuning(L.TUNE_RANGE_ORDER, order)
+            for ctas in (0, 1):
+                gpu_ctx.set_tuning(L.TUNE_RANGE_CTAS, ctas)
+                B.run()
+                got = B.counts()
+                if order == 0 and ctas == 0:
+                    ref = got.copy()
+                assert np.array_equal(got, ref), (order, ctas)
+        assert all(int(ref[i]) == w for i, w in enumerate(want) if w is not None)
+    finally:
+        gpu_ctx.set_tuning(L.TUNE_RANGE_ORDER, 0)
+        gpu_ctx.set_tuning(L.TUNE_RANGE_CTAS, 0)

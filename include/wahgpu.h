@@ -220,6 +220,36 @@ int64_t wahgpu_batch_rids(wahgpu_batch* batch, uint32_t q, uint32_t* out, uint64
 const uint32_t* wahgpu_batch_device_rids(wahgpu_batch* batch);
 int wahgpu_batch_free(wahgpu_batch* batch);
 
+
+/* ---- serving ----------------------------------------------------------- */
+/* Continuous batching of conjunctive range queries over resident indexes
+ * (no counterpart in the reference, which evaluates one query per caller
+ * under a global lock, src/iapi.cpp:33).  A worker thread keeps `nslots`
+ * execution slots (each its own stream and scratch); an idle slot takes the
+ * waiting queries in arrival order, as many as fit `max_batch` and the
+ * scratch budget (device bytes for their evaluation), and runs them as one
+ * batch while later arrivals queue for the next idle slot.  Results are
+ * those of wahgpu_evaluate for each query alone. */
+typedef struct wahgpu_server wahgpu_server;
+int wahgpu_server_create(wahgpu_ctx* ctx, uint32_t nslots, uint32_t max_batch, uint64_t scratch_budget,
+                         wahgpu_server** out);
+/* Queues one query (its terms are copied); returns a request id > 0, or
+ * WAHGPU_EBUSY when the query's scratch alone exceeds the budget.  rid_cap
+ * > 0 asks for up to rid_cap row ids. */
+int64_t wahgpu_server_submit(wahgpu_server* s, const wahgpu_term* terms, uint32_t nterms, uint64_t rid_cap);
+/* Waits for a request: hit count, row ids (if asked for), latency in
+ * seconds from submit to answer; returns the number of row ids written. */
+int64_t wahgpu_server_wait(wahgpu_server* s, int64_t id, uint64_t* count, uint32_t* rids, uint64_t cap,
+                           double* latency_s);
+/* Open-loop replay: query q = terms[qoff[q], qoff[q+1]) arrives arrival_s[q]
+ * seconds after the call starts; waits for all; counts and latencies
+ * (scheduled arrival to answer) per query; returns the wall time in
+ * microseconds. */
+int64_t wahgpu_server_replay(wahgpu_server* s, const wahgpu_term* terms, const uint32_t* qoff, uint32_t nq,
+                             const double* arrival_s, uint64_t* counts, double* latency_s);
+int wahgpu_server_stats(wahgpu_server* s, uint64_t* batches, uint64_t* served);
+int wahgpu_server_free(wahgpu_server* s);
+
 /* ---- allocation-free row ids -------------------------------------------
  * No counterpart in the reference: an addition for callers that cannot
  * allocate device memory while they run — code issuing work during CUDA

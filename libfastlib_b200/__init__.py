@@ -119,6 +119,15 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "wahgpu_batch_rids": (ctypes.c_int64, [P, ctypes.c_uint32, U32P, ctypes.c_uint64]),
         "wahgpu_batch_device_rids": (P, [P]),
         "wahgpu_batch_free": (ctypes.c_int, [P]),
+        "wahgpu_server_create": (ctypes.c_int, [P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(P)]),
+        "wahgpu_server_submit": (ctypes.c_int64, [P, ctypes.POINTER(_Term), ctypes.c_uint32, ctypes.c_uint64]),
+        "wahgpu_server_wait": (ctypes.c_int64, [P, ctypes.c_int64, ctypes.POINTER(ctypes.c_uint64), U32P,
+                                                 ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)]),
+        "wahgpu_server_replay": (ctypes.c_int64, [P, ctypes.POINTER(_Term), U32P, ctypes.c_uint32,
+                                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64),
+                                                   ctypes.POINTER(ctypes.c_double)]),
+        "wahgpu_server_stats": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
+        "wahgpu_server_free": (ctypes.c_int, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -425,6 +434,63 @@ class Batch:
     def close(self):
         if getattr(self, "h", None) and self.ctx.h:
             self.ctx.lib.wahgpu_batch_free(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous batching of conjunctive queries over resident indexes
+    (wahgpu_server_*): `nslots` batches in flight, batches of up to
+    `max_batch` queries admitted by a device scratch budget."""
+
+    def __init__(self, ctx: Context, nslots: int = 2, max_batch: int = 1024, scratch_budget: int = 256 << 20):
+        self.ctx = ctx
+        h = ctypes.c_void_p()
+        ctx.check(ctx.lib.wahgpu_server_create(ctx.h, nslots, max_batch, scratch_budget, ctypes.byref(h)))
+        self.h = h
+
+    def submit(self, terms, rid_cap: int = 0) -> int:
+        arr = (_Term * len(terms))(*terms)
+        return self.ctx.check(int(self.ctx.lib.wahgpu_server_submit(self.h, arr, len(terms), rid_cap)))
+
+    def wait(self, rid: int, rid_cap: int = 0):
+        """(count, row ids or None, latency seconds)."""
+        c = ctypes.c_uint64()
+        lat = ctypes.c_double()
+        out = np.empty(max(rid_cap, 1), dtype=np.uint32)
+        n = self.ctx.check(int(self.ctx.lib.wahgpu_server_wait(
+            self.h, rid, ctypes.byref(c), out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)) if rid_cap else None,
+            rid_cap, ctypes.byref(lat))))
+        return int(c.value), (out[:n].copy() if rid_cap else None), float(lat.value)
+
+    def replay(self, queries, arrival_s):
+        """Open-loop replay; returns (counts, latencies seconds, wall seconds)."""
+        flat = [t for q in queries for t in q]
+        offs = np.zeros(len(queries) + 1, dtype=np.uint32)
+        offs[1:] = np.cumsum([len(q) for q in queries])
+        arr = (_Term * len(flat))(*flat)
+        arrival = np.ascontiguousarray(arrival_s, dtype=np.float64)
+        counts = np.zeros(len(queries), dtype=np.uint64)
+        lat = np.zeros(len(queries), dtype=np.float64)
+        us = self.ctx.check(int(self.ctx.lib.wahgpu_server_replay(
+            self.h, arr, offs.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), len(queries),
+            arrival.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+            counts.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), lat.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))))
+        return counts, lat, us / 1e6
+
+    def stats(self):
+        b, s = ctypes.c_uint64(), ctypes.c_uint64()
+        self.ctx.check(self.ctx.lib.wahgpu_server_stats(self.h, ctypes.byref(b), ctypes.byref(s)))
+        return int(b.value), int(s.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.wahgpu_server_free(self.h)
         self.h = None
 
     def __del__(self):

@@ -37,6 +37,7 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
            "-shared", "-I" + os.path.join(ROOT, "include"),
            "-o", out, os.path.join(HERE, "csrc", "wah_api.cu"),
            os.path.join(HERE, "csrc", "wah_index.cu"), os.path.join(HERE, "csrc", "wah_build.cu"),
+           os.path.join(HERE, "csrc", "wah_server.cu"),
            os.path.join(HERE, "csrc", "wah_noalloc.cu")]
     if verbose:
         print(" ".join(cmd))

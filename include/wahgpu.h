@@ -218,6 +218,10 @@ int wahgpu_batch_run(wahgpu_batch* batch);
 int wahgpu_batch_counts(wahgpu_batch* batch, uint64_t* counts);
 int64_t wahgpu_batch_rids(wahgpu_batch* batch, uint32_t q, uint32_t* out, uint64_t cap);
 const uint32_t* wahgpu_batch_device_rids(wahgpu_batch* batch);
+/* Algorithmic bytes one run reads: per term the words of the bitmaps it
+ * ORs (or their complement), of its edge bitmaps and the raw values of the
+ * edge bitmaps' rows; 8 per query for the count. */
+int64_t wahgpu_batch_bytes(wahgpu_batch* batch);
 int wahgpu_batch_free(wahgpu_batch* batch);
 
 

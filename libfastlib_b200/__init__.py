@@ -119,6 +119,7 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "wahgpu_batch_rids": (ctypes.c_int64, [P, ctypes.c_uint32, U32P, ctypes.c_uint64]),
         "wahgpu_batch_device_rids": (P, [P]),
         "wahgpu_batch_free": (ctypes.c_int, [P]),
+        "wahgpu_batch_bytes": (ctypes.c_int64, [P]),
         "wahgpu_server_create": (ctypes.c_int, [P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(P)]),
         "wahgpu_server_submit": (ctypes.c_int64, [P, ctypes.POINTER(_Term), ctypes.c_uint32, ctypes.c_uint64]),
         "wahgpu_server_wait": (ctypes.c_int64, [P, ctypes.c_int64, ctypes.POINTER(ctypes.c_uint64), U32P,
@@ -420,6 +421,10 @@ class Batch:
 
     def run(self):
         self.ctx.check(self.ctx.lib.wahgpu_batch_run(self.h))
+
+    def nbytes(self) -> int:
+        """Algorithmic bytes of one run (bitmap words read, edge-row values)."""
+        return self.ctx.check(int(self.ctx.lib.wahgpu_batch_bytes(self.h)))
 
     def counts(self) -> np.ndarray:
         out = np.zeros(self.nq, dtype=np.uint64)

@@ -297,6 +297,7 @@ extern "C" int wahgpu_batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, co
     if (!x0) return wg_fail(ctx, WAHGPU_EINVAL, "term without an index");
     std::vector<const wahgpu_index*> idx;
     std::vector<DevTerm> dt(nt);
+    uint64_t bytes = 0;
     for (uint32_t i = 0; i < nt; ++i) {
         const wahgpu_index* x = terms[i].idx;
         if (!x || x->nrows != x0->nrows) return wg_fail(ctx, WAHGPU_EINVAL, "term %u: indexes of one batch must share their row count", i);
@@ -305,6 +306,12 @@ extern "C" int wahgpu_batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, co
         auto it = std::find(idx.begin(), idx.end(), x);
         dt[i].index = (uint32_t)(it - idx.begin());
         if (it == idx.end()) idx.push_back(x);
+        // bytes the term reads: the OR'ed bitmaps' words, the edge bitmaps'
+        // words and the raw value of each of their rows
+        const uint64_t in = x->cum_words[dt[i].h1] - x->cum_words[dt[i].h0];
+        bytes += 4 * (dt[i].flip ? x->cum_words[x->nobs] - in : in);
+        for (uint32_t c = 0; c < dt[i].ncand; ++c)
+            bytes += 4 * (x->bwords[dt[i].cand[c]] + x->bones[dt[i].cand[c]]);
     }
     std::vector<DevQuery> dq(nq);
     for (uint32_t q = 0; q < nq; ++q) {
@@ -319,6 +326,7 @@ extern "C" int wahgpu_batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, co
     for (auto* x : idx) di.push_back(x->dev);
     wahgpu_batch* B = new wahgpu_batch();
     B->ctx = ctx; B->nq = nq; B->nterms = nt; B->nidx = (uint32_t)idx.size();
+    B->bytes = bytes + 8ull * nq;
     B->groups = x0->groups; B->anb = x0->anb; B->ntiles = x0->ntiles;
     B->d_idx = static_cast<DevIndex*>(wg_alloc(ctx, di.size() * sizeof(DevIndex)));
     B->d_terms = static_cast<DevTerm*>(wg_alloc(ctx, nt * sizeof(DevTerm)));
@@ -415,6 +423,11 @@ extern "C" int64_t wahgpu_batch_rids(wahgpu_batch* B, uint32_t q, uint32_t* out,
 }
 
 extern "C" const uint32_t* wahgpu_batch_device_rids(wahgpu_batch* B) { return B ? B->d_rids : nullptr; }
+
+// Algorithmic bytes of one run: per term the words of the bitmaps it ORs
+// (or of their complement), of its edge bitmaps and the raw values of the
+// edge bitmaps' rows; 8 per query for its count.
+extern "C" int64_t wahgpu_batch_bytes(wahgpu_batch* B) { return B ? (int64_t)B->bytes : WAHGPU_EINVAL; }
 
 extern "C" int wahgpu_batch_free(wahgpu_batch* B) {
     if (!B) return WAHGPU_EINVAL;

@@ -39,6 +39,7 @@ struct wahgpu_batch {
     uint32_t* d_dense = nullptr;
     wah::DevMeta* d_status = nullptr;
     std::vector<unsigned long long> h_counts, h_start;
+    uint64_t bytes = 0;               // algorithmic bytes one run reads
     bool h_valid = false;
 };
 

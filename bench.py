@@ -228,6 +228,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--dense-tile", type=int, default=2048, choices=[1024, 2048, 4096],
                     help="groups per tile of the dense-path kernel")
+    ap.add_argument("--dense-engine", type=int, default=0, choices=[0, 1, 2],
+                    help="canonical-result operators: 0 auto, 1 group-space kernel, 2 word-space merge")
     ap.add_argument("--workloads", default=None,
                     help="comma list of range workloads to add to the line: range,batched,served "
                          "(default: all three on one GPU, none under torchrun)")
@@ -260,6 +262,7 @@ def main():
         OPS[:] = [OPNAMES.index(op_s)]
     ctx = L.Context(local)
     ctx.set_tuning(L.TUNE_DENSE_TILE, args.dense_tile)
+    ctx.set_tuning(L.TUNE_DENSE_ENGINE, args.dense_engine)
     # a dedicated stream: the legacy default stream (handle 0) cannot be
     # handed to the library, which treats NULL as "its own stream"
     stream = torch.cuda.Stream()

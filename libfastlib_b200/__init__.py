@@ -52,6 +52,7 @@ RELIC, BIN = 1, 2
 TUNE_DENSE_TILE = 1
 TUNE_RANGE_ORDER = 2
 TUNE_RANGE_CTAS = 3
+TUNE_DENSE_ENGINE = 4
 DENSE_TILES = (1024, 2048, 4096)
 CMP_NONE, CMP_LT, CMP_LE = 0, 1, 2
 U32, F32, I32 = 0, 1, 2
@@ -190,7 +191,14 @@ class Context:
 
     # constructors
     def bitvector(self, serial) -> "Bitvector":
-        """ibis::bitvector(const array_t<word_t>&) from a serialized array."""
+        """ibis::bitvector(const array_t<word_t>&) from a serialized array
+        (host array, or a CUDA tensor of 32-bit words read on the device)."""
+        if getattr(serial, "is_cuda", False):
+            t = serial.contiguous()
+            h = ctypes.c_void_p()
+            self.check(self.lib.wahgpu_bv_from_device_serial(self.h, ctypes.c_void_p(t.data_ptr()), t.numel(),
+                                                            ctypes.byref(h)))
+            return Bitvector(self, h)
         a = np.ascontiguousarray(serial, dtype=np.uint32)
         h = ctypes.c_void_p()
         self.check(self.lib.wahgpu_bv_from_serial(

@@ -165,6 +165,10 @@ extern "C" int wahgpu_ctx_set_tuning(wahgpu_ctx* ctx, int key, int64_t value) {
             return wg_fail(ctx, WAHGPU_EINVAL, "dense tile must be 1024, 2048 or 4096 groups, not %lld", (long long)value);
         ctx->dense_tile = (uint32_t)value;
         return WAHGPU_OK;
+    case WAHGPU_TUNE_DENSE_ENGINE:
+        if (value < 0 || value > 2) return wg_fail(ctx, WAHGPU_EINVAL, "dense engine must be 0, 1 or 2");
+        ctx->dense_engine = (uint32_t)value;
+        return WAHGPU_OK;
     case WAHGPU_TUNE_RANGE_ORDER:
         if (value != 0 && value != 1) return wg_fail(ctx, WAHGPU_EINVAL, "range order must be 0 or 1");
         ctx->range_order = (uint32_t)value;
@@ -181,6 +185,7 @@ extern "C" int64_t wahgpu_ctx_get_tuning(wahgpu_ctx* ctx, int key) {
     if (!ctx) return WAHGPU_EINVAL;
     switch (key) {
     case WAHGPU_TUNE_DENSE_TILE: return ctx->dense_tile;
+    case WAHGPU_TUNE_DENSE_ENGINE: return ctx->dense_engine;
     case WAHGPU_TUNE_RANGE_ORDER: return ctx->range_order;
     case WAHGPU_TUNE_RANGE_CTAS: return ctx->range_ctas;
     default: return wg_fail(ctx, WAHGPU_EINVAL, "unknown tuning key %d", key);
@@ -562,6 +567,13 @@ static OperandMeta opmeta(const wahgpu_bv* b) {
     return m;
 }
 
+// Engine for a canonical-result operator (WAHGPU_TUNE_DENSE_ENGINE): 1 group
+// space, 2 word space, 0 (default) group space — measured faster at every
+// density of the raw-WAH workload.
+static bool dense_in_word_space(const wahgpu_ctx* ctx, const wahgpu_bv*, const wahgpu_bv*, uint32_t) {
+    return ctx->dense_engine == 2;
+}
+
 extern "C" int wahgpu_bv_binop_into(wahgpu_ctx* ctx, int op, int inplace, wahgpu_bv* a, wahgpu_bv* b,
                                     wahgpu_bv* res) {
     if (!ctx || !a || !b || !res || op < 0 || op > 3) return wg_fail(ctx, WAHGPU_EINVAL, "bad argument");
@@ -593,7 +605,12 @@ extern "C" int wahgpu_bv_binop_into(wahgpu_ctx* ctx, int op, int inplace, wahgpu
         rc = wg_launch_merge(ctx, op, true, false, false, ca, cb, G, anb, aval, res);
         break;
     case PK_MERGE_CANON:
-        rc = wg_launch_dense(ctx, op, ca, cb, G, anb, aval, res);
+        // canonical result: the group-space kernel, or the word-space merge
+        // (no step states) when the tuning asks for it
+        if (dense_in_word_space(ctx, ca, cb, G))
+            rc = wg_launch_merge(ctx, op, false, false, false, ca, cb, G, anb, aval, res);
+        else
+            rc = wg_launch_dense(ctx, op, ca, cb, G, anb, aval, res);
         break;
     case PK_COPY:
     case PK_COPY_FLIP:

@@ -219,3 +219,15 @@ def test_dense_small_sizes(gpu_ctx):
             ref, rc = oracle.binop(op, a, b, inplace=False)
             w, c = _bin(gpu_ctx, op, a, b, 0)
             assert c == rc and np.array_equal(w, ref), (ng, op)
+
+
+@pytest.mark.parametrize("density", [0.1, 0.5])
+def test_word_space_engine_same_words(gpu_ctx, density):
+    """Canonical-result operators through the word-space merge
+    (WAHGPU_TUNE_DENSE_ENGINE = 2) give the same words."""
+    import libfastlib_b200 as L
+    gpu_ctx.set_tuning(L.TUNE_DENSE_ENGINE, 2)
+    try:
+        _full_size(gpu_ctx, density)
+    finally:
+        gpu_ctx.set_tuning(L.TUNE_DENSE_ENGINE, 0)

@@ -1,0 +1,103 @@
+// Drives include/wahgpu.hpp the way FastBit code would use ibis::bitvector,
+// relic/bin and countQuery.  Reads cases from argv[1], writes results to
+// argv[2] (binary, little endian); tests/test_gpu_cpp_shim.py checks them.
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <fstream>
+#include <string>
+#include <vector>
+#include "wahgpu.hpp"
+
+using namespace wahgpu_ibis;
+
+static uint32_t rd(std::ifstream& f) { uint32_t v; f.read(reinterpret_cast<char*>(&v), 4); return v; }
+static std::vector<uint32_t> rdv(std::ifstream& f) {
+    std::vector<uint32_t> v(rd(f));
+    if (!v.empty()) f.read(reinterpret_cast<char*>(v.data()), v.size() * 4);
+    return v;
+}
+static void wr(std::ofstream& f, uint64_t v) { f.write(reinterpret_cast<const char*>(&v), 8); }
+static void wrv(std::ofstream& f, const std::vector<uint32_t>& v) {
+    wr(f, v.size());
+    f.write(reinterpret_cast<const char*>(v.data()), v.size() * 4);
+}
+
+int main(int argc, char** argv) {
+    if (argc < 3) return 2;
+    std::ifstream in(argv[1], std::ios::binary);
+    std::ofstream out(argv[2], std::ios::binary);
+    context& ctx = context::standard();
+    // 1. operators: a OP b and a OP= b, words and cnt()
+    const uint32_t nbin = rd(in);
+    for (uint32_t i = 0; i < nbin; ++i) {
+        const uint32_t op = rd(in), inplace = rd(in);
+        bitvector a(rdv(in)), b(rdv(in));
+        std::vector<uint32_t> w;
+        uint64_t c;
+        if (inplace) {
+            bitvector r(a);
+            if (op == 0) r &= b; else if (op == 1) r |= b; else if (op == 2) r ^= b; else r -= b;
+            r.write(w);
+            c = r.cnt();
+        } else {
+            bitvector* r = op == 0 ? (a & b) : op == 1 ? (a | b) : op == 2 ? (a ^ b) : (a - b);
+            r->write(w);
+            c = r->cnt();
+            delete r;
+        }
+        wrv(out, w);
+        wr(out, c);
+    }
+    // 2. construction: setBit in row order, then appendFill to the size
+    const uint32_t nset = rd(in);
+    for (uint32_t i = 0; i < nset; ++i) {
+        const uint32_t nbits = rd(in);
+        std::vector<uint32_t> rows = rdv(in);
+        bitvector b;
+        b.set(0, 0);
+        for (uint32_t r : rows) b.setBit(r, 1);
+        if (b.size() < nbits) b.appendFill(0, (uint32_t)(nbits - b.size()));
+        std::vector<uint32_t> w;
+        b.write(w);
+        wrv(out, w);
+        wrv(out, b.rows());
+    }
+    // 3. countQuery over two device-built indexes
+    const uint32_t n = rd(in);
+    std::vector<uint32_t> ca = rdv(in), cb = rdv(in);  // column b holds float32 bits
+    void *da = nullptr, *db = nullptr;
+    cudaMalloc(&da, (size_t)n * 4);
+    cudaMalloc(&db, (size_t)n * 4);
+    cudaMemcpy(da, ca.data(), (size_t)n * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(db, cb.data(), (size_t)n * 4, cudaMemcpyHostToDevice);
+    {
+        relic ra(WAHGPU_U32, da, n);
+        bin rb(WAHGPU_F32, db, n, 64);
+        countQuery q;
+        q.addColumn("a", ra);
+        q.addColumn("b", rb);
+        const uint32_t nq = rd(in);
+        for (uint32_t i = 0; i < nq; ++i) {
+            std::vector<uint32_t> txt = rdv(in);
+            std::string clause(txt.begin(), txt.end());
+            const int rc = q.setWhereClause(clause.c_str());
+            wr(out, (uint64_t)(int64_t)rc);
+            if (rc == 0) {
+                q.evaluate();
+                std::vector<uint32_t> rows;
+                q.getHitRows(rows);
+                wr(out, (uint64_t)q.getNumHits());
+                wrv(out, rows);
+            }
+        }
+        // relic::evaluate / estimate with a qContinuousRange
+        bitvector hits;
+        const long c = ra.evaluate(qContinuousRange(10, qContinuousRange::OP_LE, 20, qContinuousRange::OP_LT), hits);
+        wr(out, (uint64_t)c);
+        wr(out, ra.estimate(qContinuousRange(10, qContinuousRange::OP_LE, 20, qContinuousRange::OP_LT)));
+        wrv(out, hits.rows());
+    }
+    cudaFree(da);
+    cudaFree(db);
+    return 0;
+}

@@ -45,3 +45,15 @@ def test_no_device_fails_loudly():
     with pytest.raises(L.WahError) as e:
         L.Context(0)
     assert e.value.code == -2
+
+
+def test_cpp_header_compiles():
+    """include/wahgpu.hpp compiles on its own (warnings as errors)."""
+    import subprocess
+    import tempfile
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    with tempfile.TemporaryDirectory() as td:
+        src = os.path.join(td, "t.cpp")
+        open(src, "w").write('#define WAHGPU_AS_IBIS\n#include "wahgpu.hpp"\nint main() { return 0; }\n')
+        subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-fsyntax-only",
+                        "-I" + os.path.join(root, "include"), src], check=True)

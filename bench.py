@@ -230,6 +230,9 @@ def main():
                     help="groups per tile of the dense-path kernel")
     ap.add_argument("--dense-engine", type=int, default=0, choices=[0, 1, 2],
                     help="canonical-result operators: 0 auto, 1 group-space kernel, 2 word-space merge")
+    ap.add_argument("--only-range", default=None,
+                    help="ROWS:QUERIES — only the binned range case at that size, tile-major count batch run "
+                         "warmup+steps times (for ncu)")
     ap.add_argument("--workloads", default=None,
                     help="comma list of range workloads to add to the line: range,batched,served "
                          "(default: all three on one GPU, none under torchrun)")
@@ -245,6 +248,10 @@ def main():
     import torch
     import torch.distributed as dist
     import libfastlib_b200 as L
+
+    if args.only_range:
+        run_only_range(args)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -459,6 +466,30 @@ def main():
     ctx.set_stream(None)
     if world > 1:
         dist.destroy_process_group()
+
+
+def run_only_range(args):
+    """The binned range case at a chosen size (bin index of 1000 equal-weight
+    bins built on the GPU, QUERIES ranges of 1-500 bins), one count-only
+    tile-major batch run warmup + steps times; prints one JSON line."""
+    import torch
+    import libfastlib_b200 as L
+    from libfastlib_b200 import workloads as W
+    rows, nq = (int(x) for x in args.only_range.split(":"))
+    ctx = L.Context(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    idx = L.Index.build(ctx, L.BIN, W.mixture_column(3, rows), nbins=1000)
+    qs = W.binned_range_queries(5, idx.keys(), idx.nbitmaps(), nq, 500)
+    B = L.Batch(ctx, [[idx.term(lo, hi)] for lo, hi in qs], 0)
+    ctx.set_tuning(L.TUNE_RANGE_ORDER, 1)
+    for _ in range(args.warmup):
+        B.run()
+    ms = _ev_time(stream, B.run, args.steps)
+    print(json.dumps({"only_range": args.only_range, "ms_per_batch": ms, "queries_per_s": nq / ms * 1e3,
+                      "algorithmic_bytes": B.nbytes(), "GBps": B.nbytes() / ms / 1e6}))
+    ctx.set_stream(None)
 
 
 # ---------------------------------------------------------------- range workloads

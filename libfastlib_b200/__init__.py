@@ -53,6 +53,7 @@ TUNE_DENSE_TILE = 1
 TUNE_RANGE_ORDER = 2
 TUNE_RANGE_CTAS = 3
 TUNE_DENSE_ENGINE = 4
+TUNE_CUM_STRIDE = 5
 DENSE_TILES = (1024, 2048, 4096)
 CMP_NONE, CMP_LT, CMP_LE = 0, 1, 2
 U32, F32, I32 = 0, 1, 2

@@ -177,6 +177,10 @@ extern "C" int wahgpu_ctx_set_tuning(wahgpu_ctx* ctx, int key, int64_t value) {
         if (value < 0 || value > 32) return wg_fail(ctx, WAHGPU_EINVAL, "range CTAs per SM must be 0..32");
         ctx->range_ctas = (uint32_t)value;
         return WAHGPU_OK;
+    case WAHGPU_TUNE_CUM_STRIDE:
+        if (value < 0 || value > (1 << 30)) return wg_fail(ctx, WAHGPU_EINVAL, "cumulative stride must be 0 (auto), 1 (none) or a stride");
+        ctx->cum_stride = (uint32_t)value;
+        return WAHGPU_OK;
     default:
         return wg_fail(ctx, WAHGPU_EINVAL, "unknown tuning key %d", key);
     }
@@ -188,6 +192,7 @@ extern "C" int64_t wahgpu_ctx_get_tuning(wahgpu_ctx* ctx, int key) {
     case WAHGPU_TUNE_DENSE_ENGINE: return ctx->dense_engine;
     case WAHGPU_TUNE_RANGE_ORDER: return ctx->range_order;
     case WAHGPU_TUNE_RANGE_CTAS: return ctx->range_ctas;
+    case WAHGPU_TUNE_CUM_STRIDE: return ctx->cum_stride;
     default: return wg_fail(ctx, WAHGPU_EINVAL, "unknown tuning key %d", key);
     }
 }

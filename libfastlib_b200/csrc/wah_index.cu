@@ -122,6 +122,36 @@ static int build_tile_lists(wahgpu_index* x) {
     return WAHGPU_OK;
 }
 
+// Cumulative rows: for a stride S, dense row k-1 = OR of bitmaps [0, k*S)
+// (k = 1..K), so a range's wholly-inside span costs two dense reads per tile
+// plus at most 2S edge bitmaps.  S is the smallest stride >= 8 that keeps
+// the rows within CUM_BUDGET bytes (or the context's WAHGPU_TUNE_CUM_STRIDE);
+// indexes with fewer than two rows' worth of bitmaps keep none.
+static constexpr uint64_t CUM_BUDGET = 2ull << 30;
+static int build_cumulative(wahgpu_index* x) {
+    wahgpu_ctx* ctx = x->ctx;
+    const uint32_t nobs = x->nobs;
+    const uint64_t gx = (uint64_t)x->groups + (x->anb ? 1 : 0);
+    x->cum_k = 0; x->cum_stride = 0;
+    if (ctx->cum_stride == 1 || gx == 0) return WAHGPU_OK;
+    const uint64_t stride = ctx->cum_stride ? ctx->cum_stride
+                                            : std::max<uint64_t>(8, (nobs * gx * 4 + CUM_BUDGET - 1) / CUM_BUDGET);
+    const uint64_t K = nobs / stride;
+    if (K < 2) return WAHGPU_OK;
+    x->d_cum = static_cast<uint32_t*>(wg_alloc(ctx, K * gx * 4));
+    if (!x->d_cum) return WAHGPU_OK;  // no room: ranges use the bitmaps alone
+    CUDA_TRY(ctx, cudaMemsetAsync(x->d_cum, 0, K * gx * 4, ctx->stream));
+    const uint32_t nb = (uint32_t)(K * stride), threads = 256;
+    const uint32_t blocks = (uint32_t)(((uint64_t)nb * 32 + threads - 1) / threads);
+    k_cum_blocks<<<blocks, threads, 0, ctx->stream>>>(x->d_words, x->d_bm, nb, (uint32_t)stride, (uint32_t)gx, x->d_cum);
+    k_cum_prefix<<<(uint32_t)((gx + 255) / 256), 256, 0, ctx->stream>>>(x->d_cum, (uint32_t)K, (uint32_t)gx);
+    ctx->launches += 2;
+    CUDA_TRY(ctx, cudaGetLastError());
+    x->cum_k = (uint32_t)K;
+    x->cum_stride = (uint32_t)stride;
+    return WAHGPU_OK;
+}
+
 // Second half of building an index, shared by the triple upload and the
 // device build: x->d_words / d_bm / bwords / keys are set; computes the
 // per-bitmap tile index and 1-bit counts and validates the words.
@@ -159,6 +189,8 @@ int wg_index_attach(wahgpu_index* x) {
     if (rc) return rc;
     rc = build_tile_lists(x);
     if (rc) return rc;
+    rc = build_cumulative(x);
+    if (rc) return rc;
     x->cum_words.assign(nobs + 1, 0);
     x->cum_ones.assign(nobs + 1, 0);
     for (uint32_t j = 0; j < nobs; ++j) {
@@ -167,6 +199,8 @@ int wg_index_attach(wahgpu_index* x) {
     }
     x->dev.words = x->d_words; x->dev.bm = x->d_bm; x->dev.tiles = x->d_tiles;
     x->dev.tl_off = x->d_tl_off; x->dev.tl_bm = x->d_tl_bm;
+    x->dev.cum = x->d_cum; x->dev.cum_stride = x->cum_stride; x->dev.cum_k = x->cum_k;
+    x->dev.gx = x->groups + (x->anb ? 1u : 0u);
     x->dev.values = nullptr; x->dev.nobs = nobs; x->dev.vtype = 0; x->dev.ntiles = x->ntiles;
     if (x->d_values) { x->dev.values = x->d_values; x->dev.vtype = x->vtype; }
     return WAHGPU_OK;
@@ -194,6 +228,7 @@ extern "C" int wahgpu_index_free(wahgpu_index* x) {
     wg_free(ctx, x->d_bm);
     wg_free(ctx, x->d_tiles);
     wg_free(ctx, x->d_tl_off);
+    wg_free(ctx, x->d_cum);
     wg_free(ctx, x->d_tl_bm);
     wg_free(ctx, x->d_values);
     delete x;
@@ -270,6 +305,19 @@ static int locate(wahgpu_ctx* ctx, const wahgpu_index* x, const wahgpu_term* t, 
     if (nc > 0 && !x->d_values)
         return wg_fail(ctx, WAHGPU_EINVAL, "range needs row checks but the index has no raw values attached");
     out.h0 = h0; out.h1 = h1; out.ncand = nc;
+    if (x->cum_k && h1 > h0) {
+        // C(k1) & ~C(k0) covers [k0*S, k1*S); the rest are edge bitmaps
+        const uint32_t S = x->cum_stride;
+        const uint32_t k0 = (h0 + S - 1) / S, k1 = std::min(h1 / S, x->cum_k);
+        // worth it when the span's words outweigh the dense rows read instead
+        const uint64_t span = k1 > k0 ? x->cum_words[k1 * S] - x->cum_words[k0 * S] : 0;
+        const uint64_t gx = (uint64_t)x->groups + (x->anb ? 1 : 0);
+        if (k1 > k0 && 4 * span >= (k0 ? 2 : 1) * gx) {
+            out.c0 = k0; out.c1 = k1; out.e0 = k0 * S; out.e1 = k1 * S;
+            out.flip = 0;
+            return WAHGPU_OK;
+        }
+    }
     // sumBins reads the complement when the range holds more than half the
     // index's words (src/index.cpp:6490); the bits are the same either way
     const uint64_t in = x->cum_words[h1] - x->cum_words[h0], all = x->cum_words[x->nobs];
@@ -309,7 +357,12 @@ extern "C" int wahgpu_batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, co
         // bytes the term reads: the OR'ed bitmaps' words, the edge bitmaps'
         // words and the raw value of each of their rows
         const uint64_t in = x->cum_words[dt[i].h1] - x->cum_words[dt[i].h0];
-        bytes += 4 * (dt[i].flip ? x->cum_words[x->nobs] - in : in);
+        if (dt[i].c1)
+            bytes += 4 * ((dt[i].c0 ? 2 : 1) * ((uint64_t)x->groups + (x->anb ? 1 : 0)) +
+                          (x->cum_words[dt[i].e0] - x->cum_words[dt[i].h0]) +
+                          (x->cum_words[dt[i].h1] - x->cum_words[dt[i].e1]));
+        else
+            bytes += 4 * (dt[i].flip ? x->cum_words[x->nobs] - in : in);
         for (uint32_t c = 0; c < dt[i].ncand; ++c)
             bytes += 4 * (x->bwords[dt[i].cand[c]] + x->bones[dt[i].cand[c]]);
     }

@@ -20,6 +20,8 @@ struct wahgpu_index {
     uint32_t* d_tiles = nullptr;
     uint32_t* d_tl_off = nullptr;     // per tile: bitmaps with a 1 bit there (CSR)
     uint32_t* d_tl_bm = nullptr;
+    uint32_t* d_cum = nullptr;        // cumulative dense rows (range spans in two reads)
+    uint32_t cum_stride = 0, cum_k = 0;
     void* d_values = nullptr;
     uint32_t vtype = 0;
     wah::DevIndex dev{};

@@ -49,6 +49,8 @@ struct DevIndex {
     const uint32_t* tiles;     // nobs x (ntiles+1) x {word index, first group}
     const uint32_t* tl_off;    // ntiles+1: tile k's bitmaps are tl_bm[tl_off[k], tl_off[k+1])
     const uint32_t* tl_bm;     // bitmaps holding a 1 bit in each tile, ascending
+    const uint32_t* cum;       // cum_k dense rows of gx words: row k-1 = OR of bitmaps [0, k*cum_stride)
+    uint32_t cum_stride, cum_k, gx, pad2;
     const void* values;        // raw column (nrows), or null
     uint32_t nobs;
     uint32_t vtype;            // 0 uint32, 1 float32, 2 int32
@@ -61,6 +63,9 @@ struct DevTerm {
     uint32_t index;       // into the DevIndex table
     uint32_t h0, h1;      // bitmaps wholly inside: [h0, h1)
     uint32_t flip;        // OR the complement [0,h0) u [h1,nobs) and flip
+    // with cumulative rows: [h0, h1) = C(c1) & ~C(c0) | OR of [h0, e0) and
+    // [e1, h1), C(k) = row k-1 of DevIndex::cum (C(0) empty); c1 == 0: unused
+    uint32_t c0, c1, e0, e1;
     uint32_t ncand;       // edge bitmaps to check row by row (0..2)
     uint32_t cand[2];
     uint32_t lop, rop;    // lo lop x rop hi
@@ -220,21 +225,39 @@ __global__ void __launch_bounds__(RTHREADS) k_range(RangeArgs A) {
             const DevTerm T = A.terms[t];
             const DevIndex I = A.idx[T.index];
             for (uint32_t l = tid; l < RT; l += RTHREADS) S.tmp[l] = 0u;
+            if (T.c1) {
+                // the wholly-inside span from two cumulative rows
+                const uint32_t* hi = I.cum + (size_t)(T.c1 - 1u) * I.gx + g0;
+                const uint32_t* lo = T.c0 ? I.cum + (size_t)(T.c0 - 1u) * I.gx + g0 : nullptr;
+                for (uint32_t l = tid; l < ng; l += RTHREADS)
+                    S.tmp[l] = __ldg(hi + l) & (lo ? ~__ldg(lo + l) : 0xFFFFFFFFu);
+            }
             if (tid == 0) {
-                // the term's bitmaps holding a 1 bit in this tile
+                // the term's bitmaps holding a 1 bit in this tile: [h0, h1),
+                // or with cumulative rows the edge spans [h0, e0), [e1, h1)
                 const uint32_t o0 = __ldg(I.tl_off + k), o1 = __ldg(I.tl_off + k + 1);
-                const uint32_t a = lower_bound_u32(I.tl_bm + o0, o1 - o0, T.h0);
-                const uint32_t b = lower_bound_u32(I.tl_bm + o0, o1 - o0, T.h1);
-                S.hdr[2] = o0; S.hdr[3] = o0 + a; S.hdr[4] = o0 + b; S.hdr[5] = o1;
+                const uint32_t* L = I.tl_bm + o0;
+                const uint32_t n = o1 - o0;
+                if (T.c1) {
+                    S.hdr[2] = o0 + lower_bound_u32(L, n, T.h0);
+                    S.hdr[3] = o0 + lower_bound_u32(L, n, T.e0);
+                    S.hdr[4] = o0 + lower_bound_u32(L, n, T.e1);
+                    S.hdr[5] = o0 + lower_bound_u32(L, n, T.h1);
+                } else {
+                    const uint32_t a = lower_bound_u32(L, n, T.h0);
+                    const uint32_t b = lower_bound_u32(L, n, T.h1);
+                    S.hdr[2] = o0; S.hdr[3] = o0 + a; S.hdr[4] = o0 + b; S.hdr[5] = o1;
+                }
             }
             __syncthreads();
-            // wholly-inside bitmaps, or their complement: entries [e0, e1) of
-            // the tile list, or [o0, e0) and [e1, o1)
+            // entries of the tile list: [o0, e0) u [e1, o1) (complement or
+            // cumulative edges), or [e0, e1) (the plain span)
             const uint32_t o0 = S.hdr[2], e0 = S.hdr[3], e1 = S.hdr[4], o1 = S.hdr[5];
-            const uint32_t nsel = T.flip ? (e0 - o0) + (o1 - e1) : (e1 - e0);
+            const bool two = T.flip || T.c1;
+            const uint32_t nsel = two ? (e0 - o0) + (o1 - e1) : (e1 - e0);
             for (uint32_t j = warp; j < nsel; j += RWARPS) {
                 uint32_t e;
-                if (T.flip) e = j < e0 - o0 ? o0 + j : e1 + (j - (e0 - o0));
+                if (two) e = j < e0 - o0 ? o0 + j : e1 + (j - (e0 - o0));
                 else e = e0 + j;
                 warp_or_bitmap(S, I, __ldg(I.tl_bm + e), k, g0, g1, G, anb, nullptr);
             }
@@ -432,6 +455,57 @@ __global__ void k_tile_offsets(const uint32_t* __restrict__ tile, uint32_t npair
     const uint32_t kp = e > 0 ? tile[e - 1] : 0u;
     const uint32_t from = e > 0 ? kp + 1u : 0u;
     for (uint32_t t = from; t <= k && t <= ntiles; ++t) off[t] = e;  // tiles kp+1 .. k start here
+}
+
+// Block ORs for the cumulative rows: bitmap b (< k*stride) is OR'ed into
+// row b / stride (one warp per bitmap; fills of more than 32 groups are
+// written by the whole warp).
+__global__ void k_cum_blocks(const uint32_t* __restrict__ words, const BitmapMeta* __restrict__ bm,
+                             uint32_t nb, uint32_t stride, uint32_t gx, uint32_t* __restrict__ rows) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (b >= nb) return;
+    const BitmapMeta m = bm[b];
+    const uint32_t* w = words + m.wstart;
+    uint32_t* row = rows + (size_t)(b / stride) * gx;
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < m.n; base += 32) {
+        const uint32_t i = base + lane;
+        const bool in = i < m.n;
+        const uint32_t wd = in ? __ldg(w + i) : 0u;
+        const uint32_t c = in ? wgroups(wd) : 0u;
+        uint32_t x = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) { uint32_t t = __shfl_up_sync(0xffffffffu, x, d); if (lane >= (uint32_t)d) x += t; }
+        const uint32_t p = carry + x - c;
+        if (in && wd <= ALLONES && wd != 0u) atomicOr(row + p, wd);
+        else if (in && wd >= HEADER1 && c <= 32u) for (uint32_t g = 0; g < c; ++g) row[p + g] = ALLONES;
+        uint32_t f = __ballot_sync(0xffffffffu, in && wd >= HEADER1 && c > 32u);
+        while (f) {
+            const uint32_t src = __ffs(f) - 1u;
+            f &= f - 1u;
+            const uint32_t fp = __shfl_sync(0xffffffffu, p, src), fc = __shfl_sync(0xffffffffu, c, src);
+            for (uint32_t g = lane; g < fc; g += 32u) row[fp + g] = ALLONES;
+        }
+        carry += __shfl_sync(0xffffffffu, x, 31);
+    }
+    if (lane == 0 && m.anb > 0) {
+        const uint32_t pat = (m.aval & ((1u << m.anb) - 1u)) << (31u - m.anb);
+        if (pat) atomicOr(row + m.groups, pat);
+    }
+}
+
+// Prefix OR down the rows: row k |= row k-1 for k = 1..nrows-1 (a thread per
+// word column; neighbouring threads read neighbouring words of each row).
+__global__ void k_cum_prefix(uint32_t* __restrict__ rows, uint32_t nrows, uint32_t gx) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= gx) return;
+    uint32_t acc = 0;
+    for (uint32_t k = 0; k < nrows; ++k) {
+        uint32_t* p = rows + (size_t)k * gx + i;
+        acc |= *p;
+        *p = acc;
+    }
 }
 
 #endif  // WAH_RANGE_TYPES_ONLY

@@ -221,3 +221,44 @@ def test_relic_all_comparisons_and_orders(gpu_ctx):
     finally:
         gpu_ctx.set_tuning(L.TUNE_RANGE_ORDER, 0)
         gpu_ctx.set_tuning(L.TUNE_RANGE_CTAS, 0)
+
+
+def test_cumulative_rows_any_stride(gpu_ctx):
+    """Indexes built with cumulative rows of several strides (and none)
+    give the scan's row ids: relic over a random and over a sorted column,
+    bin over a mixture, with ragged last groups."""
+    import libfastlib_b200 as L
+    rng = np.random.default_rng(5)
+    n = 300_007
+    cols = [
+        (L.RELIC, rng.integers(0, 3000, n).astype(np.uint32), {}),
+        (L.RELIC, np.sort(rng.integers(0, 700, n)).astype(np.uint32), {}),
+        (L.BIN, np.where(rng.random(n) < 0.6, rng.normal(size=n), rng.zipf(1.3, size=n) % 5000).astype(np.float32),
+         {"nbins": 400}),
+    ]
+    try:
+        for kind, vals, kw in cols:
+            f = vals.astype(np.float64)
+            sv = np.sort(f)
+            spans = []
+            for i in range(24):
+                a, b = sorted(rng.integers(0, n, 2))
+                lo, hi = sv[a], sv[b]
+                if i % 3 == 0:
+                    lo, hi = sv[0] - 1, sv[b]  # from below the smallest key
+                if i % 5 == 0:
+                    hi = sv[-1] + 1           # to above the largest
+                spans.append((float(lo), float(hi) + (0.5 if i % 2 else 0.0)))
+            want = [np.flatnonzero((f >= lo) & (f < hi)) for lo, hi in spans]
+            for stride in (1, 2, 3, 8, 0):
+                gpu_ctx.set_tuning(L.TUNE_CUM_STRIDE, stride)
+                idx = L.Index.build(gpu_ctx, kind, vals, **kw)
+                B = L.Batch(gpu_ctx, [[idx.term(lo, hi)] for lo, hi in spans], rid_cap=sum(len(w) for w in want))
+                B.run()
+                counts = B.counts()
+                for q, w in enumerate(want):
+                    assert int(counts[q]) == len(w), (kind, stride, q)
+                    assert np.array_equal(B.rids(q, len(w)), w), (kind, stride, q)
+                del B, idx
+    finally:
+        gpu_ctx.set_tuning(L.TUNE_CUM_STRIDE, 0)

@@ -505,6 +505,34 @@ def _ev_time(stream, fn, reps=1):
     return e0.elapsed_time(e1) / reps
 
 
+_ORDER_NAMES = {0: "query-major", 1: "tile-major", 2: "two-pass tile-major"}
+
+
+def _with_row_ids(L, tune, ctx, stream, queries, counts):
+    """The same queries with their row ids written (a sample, so the ids fit
+    in HBM): query-major order with the look-back against two tile-major
+    passes around a scan, autotuned, then timed as a captured graph."""
+    import torch
+    total = int(sum(int(c) for c in counts))
+    B = L.Batch(ctx, queries, rid_cap=total)
+    best, table = tune.tune_batch(ctx, B, count_only=False, ctas=(0,), reps=1)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        B.run()
+    g.replay()
+    ms = _ev_time(stream, g.replay, 2)
+    got = B.counts()
+    assert [int(c) for c in got] == [int(c) for c in counts], "row-id batch counts differ"
+    del g
+    B.close()
+    ctx.set_tuning(L.TUNE_RANGE_ORDER, 2)
+    ctx.set_tuning(L.TUNE_RANGE_CTAS, 0)
+    return {"queries": len(queries), "row_ids": total, "queries_per_s": len(queries) / (ms / 1e3), "ms_per_batch": ms,
+            "row_ids_per_s": total / (ms / 1e3),
+            "tuned": {"order": _ORDER_NAMES[best[0]],
+                      "candidates_ms": {_ORDER_NAMES[k[0]]: round(v, 2) for k, v in table.items()}}}
+
+
 def _batched_vs_single(L, tune, ctx, stream, queries, nsingle, peak):
     """One fused launch for all queries (launch shape autotuned) against one
     query per launch (a sample of nsingle queries)."""
@@ -521,7 +549,7 @@ def _batched_vs_single(L, tune, ctx, stream, queries, nsingle, peak):
     counts = B.counts()
     del g
     nbytes = B.nbytes()
-    ctx.set_tuning(L.TUNE_RANGE_ORDER, 0)
+    ctx.set_tuning(L.TUNE_RANGE_ORDER, 2)
     ctx.set_tuning(L.TUNE_RANGE_CTAS, 0)
     singles = [L.Batch(ctx, [q], 0) for q in queries[:nsingle]]
     for b in singles[:4]:
@@ -537,11 +565,12 @@ def _batched_vs_single(L, tune, ctx, stream, queries, nsingle, peak):
         "queries": len(queries), "queries_per_s": len(queries) / (ms / 1e3), "ms_per_batch": ms,
         "one_query_per_launch_queries_per_s": nsingle / (ms1 / 1e3), "one_query_per_launch_sample": nsingle,
         "speedup_vs_one_per_launch": (len(queries) / ms) / (nsingle / ms1),
-        "tuned": {"order": "tile-major" if best[0] else "query-major", "ctas_per_sm": best[1] or "max",
-                  "candidates_ms": {f"{'tile' if k[0] else 'query'}-major/ctas={k[1] or 'max'}": round(v, 2)
+        "tuned": {"order": _ORDER_NAMES[best[0]], "ctas_per_sm": best[1] or "max",
+                  "candidates_ms": {f"{_ORDER_NAMES[k[0]]}/ctas={k[1] or 'max'}": round(v, 2)
                                     for k, v in table.items()}},
         "algorithmic_bytes_per_batch": nbytes, "achieved_GBps": gbs, "frac_of_hbm_peak": gbs / peak,
         "avg_hits": float(np.mean(counts)),
+        "_counts": counts,
         "cuda_graph": True,
         "timing": "CUDA events on the batch stream: 2 replays of the captured fused launch; singles launched "
                   "directly",
@@ -563,6 +592,7 @@ def range_workloads(args, ctx, stream, peak, which):
         keys, nobs = idx.keys(), idx.nbitmaps()
         qs = W.binned_range_queries(5, keys, nobs, 1000, 500)
         r = _batched_vs_single(L, tune, ctx, stream, [[idx.term(lo, hi)] for lo, hi in qs], 1000, peak)
+        r.pop("_counts")
         r.update({"workload": "binned range: bin index (1000 equal-weight bins, built on the GPU) over 100M "
                               "float32 rows (70% Normal(0,1), 30% Zipf(1.2) over 1e5 ranks); 1000 queries "
                               "lo <= x < hi spanning 1..500 bins, both ends inside edge bins (row checks); "
@@ -589,6 +619,8 @@ def range_workloads(args, ctx, stream, peak, which):
         qs = W.conjunctive_queries(4, metas, 4096, max_terms=4)
         queries = [[cols[c].term(lo, hi) for c, lo, hi in q] for q in qs]
         r = _batched_vs_single(L, tune, ctx, stream, queries, 512, peak)
+        counts = r.pop("_counts")
+        r["with_row_ids"] = _with_row_ids(L, tune, ctx, stream, queries[:256], counts[:256])
         r.update({"workload": "batched conjunctive: 8 columns x 50M rows (3 uint32 U{0..999} relic, 3 uint32 "
                               "Zipf(1.1) over 1e6 relic, 2 float32 Normal bin 512), 4096 WHERE clauses of 1-4 "
                               "column ranges of uneven span; one persistent fused launch vs one query per launch",

@@ -170,7 +170,7 @@ extern "C" int wahgpu_ctx_set_tuning(wahgpu_ctx* ctx, int key, int64_t value) {
         ctx->dense_engine = (uint32_t)value;
         return WAHGPU_OK;
     case WAHGPU_TUNE_RANGE_ORDER:
-        if (value != 0 && value != 1) return wg_fail(ctx, WAHGPU_EINVAL, "range order must be 0 or 1");
+        if (value < 0 || value > 2) return wg_fail(ctx, WAHGPU_EINVAL, "range order must be 0, 1 or 2");
         ctx->range_order = (uint32_t)value;
         return WAHGPU_OK;
     case WAHGPU_TUNE_RANGE_CTAS:

@@ -131,7 +131,8 @@ static constexpr uint64_t CUM_BUDGET = 2ull << 30;
 static int build_cumulative(wahgpu_index* x) {
     wahgpu_ctx* ctx = x->ctx;
     const uint32_t nobs = x->nobs;
-    const uint64_t gx = (uint64_t)x->groups + (x->anb ? 1 : 0);
+    // rows are gx words rounded up to 4, so a tile's slice starts 16-byte aligned
+    const uint64_t gx = ((uint64_t)x->groups + (x->anb ? 1 : 0) + 3) & ~3ull;
     x->cum_k = 0; x->cum_stride = 0;
     if (ctx->cum_stride == 1 || gx == 0) return WAHGPU_OK;
     const uint64_t stride = ctx->cum_stride ? ctx->cum_stride
@@ -200,7 +201,7 @@ int wg_index_attach(wahgpu_index* x) {
     x->dev.words = x->d_words; x->dev.bm = x->d_bm; x->dev.tiles = x->d_tiles;
     x->dev.tl_off = x->d_tl_off; x->dev.tl_bm = x->d_tl_bm;
     x->dev.cum = x->d_cum; x->dev.cum_stride = x->cum_stride; x->dev.cum_k = x->cum_k;
-    x->dev.gx = x->groups + (x->anb ? 1u : 0u);
+    x->dev.gx = (x->groups + (x->anb ? 1u : 0u) + 3u) & ~3u;
     x->dev.values = nullptr; x->dev.nobs = nobs; x->dev.vtype = 0; x->dev.ntiles = x->ntiles;
     if (x->d_values) { x->dev.values = x->d_values; x->dev.vtype = x->vtype; }
     return WAHGPU_OK;
@@ -311,7 +312,7 @@ static int locate(wahgpu_ctx* ctx, const wahgpu_index* x, const wahgpu_term* t, 
         const uint32_t k0 = (h0 + S - 1) / S, k1 = std::min(h1 / S, x->cum_k);
         // worth it when the span's words outweigh the dense rows read instead
         const uint64_t span = k1 > k0 ? x->cum_words[k1 * S] - x->cum_words[k0 * S] : 0;
-        const uint64_t gx = (uint64_t)x->groups + (x->anb ? 1 : 0);
+        const uint64_t gx = ((uint64_t)x->groups + (x->anb ? 1 : 0) + 3) & ~3ull;
         if (k1 > k0 && 4 * span >= (k0 ? 2 : 1) * gx) {
             out.c0 = k0; out.c1 = k1; out.e0 = k0 * S; out.e1 = k1 * S;
             out.flip = 0;
@@ -419,8 +420,27 @@ extern "C" int wahgpu_batch_run(wahgpu_batch* B) {
     a.counts = B->d_counts; a.rids = B->d_rids; a.rid_cap = B->rid_cap; a.rid_start = B->d_start;
     a.dense = B->d_dense;
     a.recs = recs; a.sync = sync; a.nitems = nitems; a.status = B->d_status;
-    // tile by tile when only counts are wanted and the tuning asks for it
-    a.tile_major = (ctx->range_order == 1 && !B->d_rids && !B->d_dense) ? 1u : 0u;
+    // tile by tile when only counts are wanted (orders 1 and 2); with row ids
+    // order 2 runs two tile-by-tile passes around a scan of the items' hits,
+    // order 1 (and a single query) goes query by query with the look-back
+    const bool ids = B->d_rids || B->d_dense;
+    const bool two_pass = ctx->range_order == 2 && ids && B->nq > 1;
+    a.tile_major = ((ctx->range_order != 0 && !ids) || two_pass) ? 1u : 0u;
+    a.pass = 0; a.item_cnt = nullptr; a.item_off = nullptr;
+    if (two_pass) {
+        if (!B->d_items) {
+            B->d_items = static_cast<unsigned long long*>(wg_alloc(ctx, (size_t)nitems * 16));
+            cub::DeviceScan::ExclusiveSum(nullptr, B->scan_tmp_bytes, B->d_items, B->d_items + nitems, (int)nitems,
+                                          ctx->stream);
+            B->d_scan_tmp = wg_alloc(ctx, std::max<size_t>(B->scan_tmp_bytes, 16));
+            if (!B->d_items || !B->d_scan_tmp) {
+                wg_free(ctx, B->d_items); wg_free(ctx, B->d_scan_tmp);
+                B->d_items = nullptr; B->d_scan_tmp = nullptr;
+                return wg_fail(ctx, WAHGPU_ENOMEM, "two-pass item arrays: allocation failed");
+            }
+        }
+        if (B->d_dense) CUDA_TRY(ctx, cudaMemsetAsync(B->d_dense, 0, ((size_t)B->groups + 1) * 4, ctx->stream));
+    }
     static int per_sm = 0;
     const size_t sm = sizeof(RangeShared);
     if (!per_sm) {
@@ -430,6 +450,15 @@ extern "C" int wahgpu_batch_run(wahgpu_batch* B) {
     }
     const uint32_t ctas = ctx->range_ctas ? std::min<uint32_t>(ctx->range_ctas, (uint32_t)per_sm) : (uint32_t)per_sm;
     const uint32_t grid = std::min<uint32_t>(nitems, ctas * (uint32_t)ctx->sm_count);
+    if (two_pass) {
+        a.pass = 1; a.item_cnt = B->d_items;
+        k_range<<<grid, RTHREADS, sm, ctx->stream>>>(a);
+        CUDA_TRY(ctx, cudaGetLastError());
+        CUDA_TRY(ctx, cub::DeviceScan::ExclusiveSum(B->d_scan_tmp, B->scan_tmp_bytes, B->d_items, B->d_items + nitems,
+                                                    (int)nitems, ctx->stream));
+        a.pass = 2; a.item_off = B->d_items + nitems;
+        ctx->launches += 2;  // the count pass and the scan
+    }
     k_range<<<grid, RTHREADS, sm, ctx->stream>>>(a);
     ctx->launches++;
     CUDA_TRY(ctx, cudaGetLastError());
@@ -489,6 +518,7 @@ extern "C" int wahgpu_batch_free(wahgpu_batch* B) {
     wg_free(ctx, B->d_idx); wg_free(ctx, B->d_terms); wg_free(ctx, B->d_queries);
     wg_free(ctx, B->d_counts); wg_free(ctx, B->d_start); wg_free(ctx, B->d_status);
     wg_free(ctx, B->d_rids); wg_free(ctx, B->d_dense);
+    wg_free(ctx, B->d_items); wg_free(ctx, B->d_scan_tmp);
     delete B;
     return WAHGPU_OK;
 }

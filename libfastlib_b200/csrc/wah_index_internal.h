@@ -40,6 +40,11 @@ struct wahgpu_batch {
     uint64_t rid_cap = 0;
     uint32_t* d_dense = nullptr;
     wah::DevMeta* d_status = nullptr;
+    // two-pass order: per-item hits and first row-id slots (2 x nq*ntiles)
+    // and the scan's temporary storage, allocated at the first such run
+    unsigned long long* d_items = nullptr;
+    void* d_scan_tmp = nullptr;
+    size_t scan_tmp_bytes = 0;
     std::vector<unsigned long long> h_counts, h_start;
     uint64_t bytes = 0;               // algorithmic bytes one run reads
     bool h_valid = false;

@@ -33,6 +33,7 @@ constexpr int RT = 4096;             // groups per tile
 constexpr int RTHREADS = 256;
 constexpr int RWARPS = RTHREADS / 32;
 constexpr int RGPT = RT / RTHREADS;  // groups per thread in the epilogue
+constexpr uint32_t RDIRECT = 32;     // spans of at most this many bitmaps skip the tile lists
 
 // per-bitmap metadata of an attached index
 struct BitmapMeta {
@@ -49,8 +50,8 @@ struct DevIndex {
     const uint32_t* tiles;     // nobs x (ntiles+1) x {word index, first group}
     const uint32_t* tl_off;    // ntiles+1: tile k's bitmaps are tl_bm[tl_off[k], tl_off[k+1])
     const uint32_t* tl_bm;     // bitmaps holding a 1 bit in each tile, ascending
-    const uint32_t* cum;       // cum_k dense rows of gx words: row k-1 = OR of bitmaps [0, k*cum_stride)
-    uint32_t cum_stride, cum_k, gx, pad2;
+    const uint32_t* cum;       // cum_k dense rows, gx words apart: row k-1 = OR of bitmaps [0, k*cum_stride)
+    uint32_t cum_stride, cum_k, gx, pad2;  // gx: groups incl. the active one, rounded up to 4
     const void* values;        // raw column (nrows), or null
     uint32_t nobs;
     uint32_t vtype;            // 0 uint32, 1 float32, 2 int32
@@ -91,7 +92,13 @@ struct RangeArgs {
     uint32_t* dense;          // dense hit words of query 0 (or null)
     TileRec* recs; LaunchSync* sync; uint32_t nitems;
     DevMeta* status;
-    uint32_t tile_major;      // 1: items ordered tile by tile (counts only)
+    uint32_t tile_major;      // 1: items ordered tile by tile (no look-back)
+    // two-pass order (tile by tile, row ids placed without a look-back):
+    // pass 1 writes each item's hits to item_cnt, the host scans them into
+    // item_off, pass 2 writes the row ids; items are indexed q*ntiles + k
+    uint32_t pass;            // 0 one pass, 1 counts, 2 row ids
+    unsigned long long* item_cnt;
+    const unsigned long long* item_off;
 };
 
 struct RangeShared {
@@ -100,7 +107,12 @@ struct RangeShared {
     uint64_t scan[RWARPS + 1];
     uint32_t hdr[8];
     unsigned long long base;
+    DevTerm term;    // the term being evaluated and its index
+    DevIndex index;
 };
+constexpr uint32_t TERM_WORDS = sizeof(DevTerm) / 4, INDEX_WORDS = sizeof(DevIndex) / 4;
+static_assert(sizeof(DevTerm) % 4 == 0 && TERM_WORDS <= 32, "a warp stages a term");
+static_assert(sizeof(DevIndex) % 4 == 0 && INDEX_WORDS <= 32, "a warp stages an index");
 
 #ifndef WAH_RANGE_TYPES_ONLY
 __device__ __forceinline__ bool pass_cmp(double v, uint32_t lop, double lo, uint32_t rop, double hi) {
@@ -129,40 +141,53 @@ __device__ __forceinline__ void warp_or_bitmap(RangeShared& S, const DevIndex& I
     const uint32_t i1 = min(sn1 < g1 ? in1 + 1u : in1, m.n);  // words covering [g0, min(g1, G))
     const uint32_t* w = I.words + m.wstart;
     uint32_t carry = s0;
-    for (uint32_t base = i0; base < i1; base += 32) {
-        const uint32_t i = base + lane;
-        const bool in = i < i1;
-        const uint32_t wd = in ? __ldg(w + i) : 0u;
-        const uint32_t c = in ? wgroups(wd) : 0u;
-        uint32_t p;
-        const uint32_t fm = __ballot_sync(0xffffffffu, in && is_fill(wd));
-        if (fm == 0) {
-            p = carry + lane;
-            carry += __popc(__ballot_sync(0xffffffffu, in));
-        } else {
-            uint32_t x = c;
+    // four 32-word chunks are loaded before any is placed, so one memory
+    // latency covers 128 words
+    for (uint32_t base0 = i0; base0 < i1; base0 += 128) {
+        uint32_t wv[4];
 #pragma unroll
-            for (int d = 1; d < 32; d <<= 1) { uint32_t t = __shfl_up_sync(0xffffffffu, x, d); if (lane >= (uint32_t)d) x += t; }
-            p = carry + x - c;
-            carry += __shfl_sync(0xffffffffu, x, 31);
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t i = base0 + 32u * j + lane;
+            wv[j] = i < i1 ? __ldg(w + i) : 0u;
         }
-        if (in && wd != 0u && !(is_fill(wd) && wd < HEADER1)) {
-            const uint32_t a = max(p, g0), e = min(p + c, g1);
-            const uint32_t pat = wpattern(wd);
-            for (uint32_t g = a; g < e; ++g) {
-                if (!check) {
-                    if (pat == ALLONES) S.tmp[g - g0] = ALLONES;
-                    else atomicOr(&S.tmp[g - g0], pat);
-                } else {
-                    uint32_t bits = pat, set = 0;
-                    while (bits) {
-                        const uint32_t hb = 31u - __clz(bits);
-                        const uint32_t row = g * 31u + (30u - hb);
-                        if (pass_cmp(col_value(I.values, I.vtype, row), check->lop, check->lo, check->rop, check->hi))
-                            set |= 1u << hb;
-                        bits &= ~(1u << hb);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t base = base0 + 32u * j;
+            if (base >= i1) break;
+            const uint32_t i = base + lane;
+            const bool in = i < i1;
+            const uint32_t wd = wv[j];
+            const uint32_t c = in ? wgroups(wd) : 0u;
+            uint32_t p;
+            const uint32_t fm = __ballot_sync(0xffffffffu, in && is_fill(wd));
+            if (fm == 0) {
+                p = carry + lane;
+                carry += __popc(__ballot_sync(0xffffffffu, in));
+            } else {
+                uint32_t x = c;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) { uint32_t t = __shfl_up_sync(0xffffffffu, x, d); if (lane >= (uint32_t)d) x += t; }
+                p = carry + x - c;
+                carry += __shfl_sync(0xffffffffu, x, 31);
+            }
+            if (in && wd != 0u && !(is_fill(wd) && wd < HEADER1)) {
+                const uint32_t a = max(p, g0), e = min(p + c, g1);
+                const uint32_t pat = wpattern(wd);
+                for (uint32_t g = a; g < e; ++g) {
+                    if (!check) {
+                        if (pat == ALLONES) S.tmp[g - g0] = ALLONES;
+                        else atomicOr(&S.tmp[g - g0], pat);
+                    } else {
+                        uint32_t bits = pat, set = 0;
+                        while (bits) {
+                            const uint32_t hb = 31u - __clz(bits);
+                            const uint32_t row = g * 31u + (30u - hb);
+                            if (pass_cmp(col_value(I.values, I.vtype, row), check->lop, check->lo, check->rop, check->hi))
+                                set |= 1u << hb;
+                            bits &= ~(1u << hb);
+                        }
+                        if (set) atomicOr(&S.tmp[g - g0], set);
                     }
-                    if (set) atomicOr(&S.tmp[g - g0], set);
                 }
             }
         }
@@ -187,18 +212,33 @@ __device__ __forceinline__ void warp_or_bitmap(RangeShared& S, const DevIndex& I
     }
 }
 
-// Lower bound of v in the ascending list a[0, n).
-__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* __restrict__ a, uint32_t n, uint32_t v) {
-    uint32_t lo = 0, hi = n;
-    while (lo < hi) {
-        const uint32_t m = (lo + hi) >> 1;
-        if (__ldg(a + m) < v) lo = m + 1; else hi = m;
+// Lower bound of v in the ascending list a[0, n) by a group of 16 lanes
+// (lanes [gbase, gbase+16) of a full warp; every lane of the warp calls it):
+// each round the 16 lanes probe evenly spaced entries of [lo, hi) and the
+// count of entries below v narrows the span 16-fold.
+__device__ __forceinline__ uint32_t group16_lower_bound(const uint32_t* __restrict__ a, uint32_t n, uint32_t v,
+                                                         uint32_t gbase, uint32_t gl) {
+    uint32_t lo = 0, hi = n;  // the answer lies in [lo, hi]
+    while (__any_sync(0xffffffffu, lo < hi)) {
+        uint32_t p = lo;
+        bool less = false;
+        if (lo < hi) {
+            p = lo + (uint32_t)(((uint64_t)(hi - lo) * gl) >> 4);  // < hi
+            less = __ldg(a + p) < v;
+        }
+        const uint32_t c = __popc((__ballot_sync(0xffffffffu, less) >> gbase) & 0xFFFFu);
+        const uint32_t plast = __shfl_sync(0xffffffffu, p, gbase + (c ? c - 1u : 0u));
+        const uint32_t pnext = __shfl_sync(0xffffffffu, p, gbase + (c < 16u ? c : 0u));
+        if (lo < hi) {
+            if (c == 0) hi = lo;  // a[lo] >= v
+            else { lo = plast + 1u; if (c < 16u) hi = pnext; }
+        }
     }
     return lo;
 }
 
 // Persistent: every CTA claims items until none is left.
-__global__ void __launch_bounds__(RTHREADS) k_range(RangeArgs A) {
+__global__ void __launch_bounds__(RTHREADS, 6) k_range(RangeArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     RangeShared& S = *reinterpret_cast<RangeShared*>(smem_raw);
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
@@ -206,72 +246,128 @@ __global__ void __launch_bounds__(RTHREADS) k_range(RangeArgs A) {
     const uint32_t G = A.groups, anb = A.anb;
     const uint32_t GX = G + (anb > 0 ? 1u : 0u);  // groups incl. the active one
     const uint32_t lastmask = anb > 0 ? (((1u << anb) - 1u) << (31u - anb)) : ALLONES;
+    // tile-major items are claimed one item ahead, so the ticket's round
+    // trip overlaps the current item (not with the look-back: an item held
+    // back behind a long one would stall every later item waiting on it)
+    const bool ahead = A.tile_major != 0u;
+    uint32_t next = 0;
+    if (tid == 0 && ahead) next = claim_tile(A.sync);
     while (true) {
-        if (tid == 0) S.hdr[0] = claim_tile(A.sync);
+        if (tid == 0) {
+            if (ahead) {
+                S.hdr[0] = next;
+                if (next < A.nitems) next = claim_tile(A.sync);
+            } else {
+                S.hdr[0] = claim_tile(A.sync);
+            }
+        }
         __syncthreads();
         const uint32_t item = S.hdr[0], epoch = S.hdr[1];
         if (item >= A.nitems) break;
         // query-major items keep a query's row ids contiguous (look-back in
         // claim order); tile-major items let the queries of one batch share
-        // each tile's bitmap words in L2 (counts only)
+        // each tile's bitmap words in L2
         const uint32_t q = A.tile_major ? item % A.nq : item / A.ntiles;
         const uint32_t k = A.tile_major ? item / A.nq : item % A.ntiles;
         const uint32_t g0 = k * (uint32_t)RT, g1 = min(g0 + (uint32_t)RT, GX);
         const uint32_t ng = g1 > g0 ? g1 - g0 : 0u;
+        const uint32_t qi = q * A.ntiles + k;  // the item's place in query-major order
+        if (A.pass == 2u) {
+            // row ids of the two-pass order: items without hits are done
+            if (tid == 0 && k == 0) A.rid_start[q] = A.item_off[qi];
+            if (A.item_cnt[qi] == 0ull) { __syncthreads(); continue; }
+        }
         const DevQuery Q = A.queries[q];
 
         for (uint32_t l = tid; l < RT; l += RTHREADS) S.acc[l] = ALLONES;
         for (uint32_t t = Q.t0; t < Q.t1; ++t) {
-            const DevTerm T = A.terms[t];
-            const DevIndex I = A.idx[T.index];
-            for (uint32_t l = tid; l < RT; l += RTHREADS) S.tmp[l] = 0u;
+            // the term and its index, staged in shared memory by warp 0
+            if (warp == 0) {
+                const uint32_t v = lane < TERM_WORDS ? __ldg(reinterpret_cast<const uint32_t*>(A.terms + t) + lane) : 0u;
+                const uint32_t ix = __shfl_sync(0xffffffffu, v, 0);  // DevTerm::index
+                if (lane < TERM_WORDS) reinterpret_cast<uint32_t*>(&S.term)[lane] = v;
+                if (lane < INDEX_WORDS)
+                    reinterpret_cast<uint32_t*>(&S.index)[lane] = __ldg(reinterpret_cast<const uint32_t*>(A.idx + ix) + lane);
+            }
+            __syncthreads();
+            const DevTerm& T = S.term;
+            const DevIndex& I = S.index;
+            uint4* t4 = reinterpret_cast<uint4*>(S.tmp);
             if (T.c1) {
                 // the wholly-inside span from two cumulative rows
-                const uint32_t* hi = I.cum + (size_t)(T.c1 - 1u) * I.gx + g0;
-                const uint32_t* lo = T.c0 ? I.cum + (size_t)(T.c0 - 1u) * I.gx + g0 : nullptr;
-                for (uint32_t l = tid; l < ng; l += RTHREADS)
-                    S.tmp[l] = __ldg(hi + l) & (lo ? ~__ldg(lo + l) : 0xFFFFFFFFu);
-            }
-            if (tid == 0) {
-                // the term's bitmaps holding a 1 bit in this tile: [h0, h1),
-                // or with cumulative rows the edge spans [h0, e0), [e1, h1)
-                const uint32_t o0 = __ldg(I.tl_off + k), o1 = __ldg(I.tl_off + k + 1);
-                const uint32_t* L = I.tl_bm + o0;
-                const uint32_t n = o1 - o0;
-                if (T.c1) {
-                    S.hdr[2] = o0 + lower_bound_u32(L, n, T.h0);
-                    S.hdr[3] = o0 + lower_bound_u32(L, n, T.e0);
-                    S.hdr[4] = o0 + lower_bound_u32(L, n, T.e1);
-                    S.hdr[5] = o0 + lower_bound_u32(L, n, T.h1);
-                } else {
-                    const uint32_t a = lower_bound_u32(L, n, T.h0);
-                    const uint32_t b = lower_bound_u32(L, n, T.h1);
-                    S.hdr[2] = o0; S.hdr[3] = o0 + a; S.hdr[4] = o0 + b; S.hdr[5] = o1;
+                // (16-byte slices: g0 is a multiple of RT and the rows'
+                // padding past the last group is zero)
+                const uint4* hi = reinterpret_cast<const uint4*>(I.cum + (size_t)(T.c1 - 1u) * I.gx + g0);
+                const uint4* lo = reinterpret_cast<const uint4*>(T.c0 ? I.cum + (size_t)(T.c0 - 1u) * I.gx + g0 : I.cum);
+                const uint32_t n4 = (ng + 3u) >> 2;
+                const bool two = T.c0 != 0u;
+#pragma unroll
+                for (uint32_t l = tid; l < RT / 4; l += RTHREADS) {
+                    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                    if (l < n4) {
+                        const uint4 a = __ldg(hi + l);
+                        const uint4 b = two ? __ldg(lo + l) : v;
+                        v = make_uint4(a.x & ~b.x, a.y & ~b.y, a.z & ~b.z, a.w & ~b.w);
+                    }
+                    t4[l] = v;
                 }
+            } else {
+#pragma unroll
+                for (uint32_t l = tid; l < RT / 4; l += RTHREADS) t4[l] = make_uint4(0u, 0u, 0u, 0u);
+            }
+            // the bitmaps to OR: with cumulative rows the edge spans
+            // [h0, e0) u [e1, h1) and a plain span of at most RDIRECT
+            // bitmaps are walked directly (one that misses the tile costs
+            // its tile-index lookup); wider spans and complements take the
+            // entries of the tile's list that hold a 1 bit in it
+            const bool flip = T.flip != 0u;
+            const bool direct = T.c1 || (!flip && T.h1 - T.h0 <= RDIRECT);
+            if (!direct && warp == 0) {
+                const uint32_t o0 = __ldg(I.tl_off + k), o1 = __ldg(I.tl_off + k + 1);
+                const uint32_t gbase = lane & 16u;
+                const uint32_t r = group16_lower_bound(I.tl_bm + o0, o1 - o0, gbase ? T.h1 : T.h0, gbase, lane & 15u);
+                if (lane == 0) { S.hdr[2] = o0; S.hdr[3] = o0 + r; }
+                if (lane == 16) { S.hdr[4] = o0 + r; S.hdr[5] = o1; }
             }
             __syncthreads();
-            // entries of the tile list: [o0, e0) u [e1, o1) (complement or
-            // cumulative edges), or [e0, e1) (the plain span)
-            const uint32_t o0 = S.hdr[2], e0 = S.hdr[3], e1 = S.hdr[4], o1 = S.hdr[5];
-            const bool two = T.flip || T.c1;
-            const uint32_t nsel = two ? (e0 - o0) + (o1 - e1) : (e1 - e0);
-            for (uint32_t j = warp; j < nsel; j += RWARPS) {
-                uint32_t e;
-                if (two) e = j < e0 - o0 ? o0 + j : e1 + (j - (e0 - o0));
-                else e = e0 + j;
-                warp_or_bitmap(S, I, __ldg(I.tl_bm + e), k, g0, g1, G, anb, nullptr);
+            // one job list per term: the edge bitmaps' row checks first
+            // (the longest jobs), then the bitmaps to OR; a complement is
+            // flipped before the checked rows join it
+            const uint32_t nc = flip ? 0u : T.ncand;
+            uint32_t nsel, ne0 = 0, o0 = 0, e0 = 0, e1 = 0;
+            if (direct) {
+                ne0 = T.c1 ? T.e0 - T.h0 : T.h1 - T.h0;
+                nsel = T.c1 ? ne0 + (T.h1 - T.e1) : ne0;
+            } else {
+                // entries of the tile list: [o0, e0) u [e1, o1) (complement),
+                // or [e0, e1) (the plain span)
+                o0 = S.hdr[2]; e0 = S.hdr[3]; e1 = S.hdr[4];
+                const uint32_t o1 = S.hdr[5];
+                nsel = flip ? (e0 - o0) + (o1 - e1) : (e1 - e0);
             }
-            __syncthreads();
-            if (T.flip) {
+            for (uint32_t j = warp; j < nc + nsel; j += RWARPS) {
+                if (j < nc) {
+                    warp_or_bitmap(S, I, T.cand[j], k, g0, g1, G, anb, &T);
+                    continue;
+                }
+                const uint32_t jj = j - nc;
+                uint32_t b;
+                if (direct) b = jj < ne0 ? T.h0 + jj : T.e1 + (jj - ne0);
+                else if (flip) b = __ldg(I.tl_bm + (jj < e0 - o0 ? o0 + jj : e1 + (jj - (e0 - o0))));
+                else b = __ldg(I.tl_bm + e0 + jj);
+                warp_or_bitmap(S, I, b, k, g0, g1, G, anb, nullptr);
+            }
+            if (flip) {
+                __syncthreads();
                 for (uint32_t l = tid; l < ng; l += RTHREADS) {
                     const uint32_t msk = (g0 + l == G && anb > 0) ? lastmask : ALLONES;
                     S.tmp[l] ^= msk;
                 }
                 __syncthreads();
+                // edge bitmaps: rows checked against the raw values
+                for (uint32_t c = warp; c < T.ncand; c += RWARPS)
+                    warp_or_bitmap(S, I, T.cand[c], k, g0, g1, G, anb, &T);
             }
-            // edge bitmaps: rows checked against the raw values
-            for (uint32_t c = warp; c < T.ncand; c += RWARPS)
-                warp_or_bitmap(S, I, T.cand[c], k, g0, g1, G, anb, &T);
             __syncthreads();
             uint32_t any = 0;
             for (uint32_t l = tid; l < RT; l += RTHREADS) { const uint32_t v = S.acc[l] & S.tmp[l]; S.acc[l] = v; any |= v; }
@@ -293,7 +389,17 @@ __global__ void __launch_bounds__(RTHREADS) k_range(RangeArgs A) {
                 S.acc[l] = 0u;
             }
         }
-        if (A.tile_major) {
+        if (A.tile_major && A.pass == 1u) {
+            uint64_t total;
+            block_exscan64(cnt, S.scan, total);
+            if (tid == 0) {
+                A.item_cnt[qi] = total;
+                if (total) atomicAdd(&A.counts[q], (unsigned long long)total);
+            }
+            __syncthreads();
+            continue;
+        }
+        if (A.tile_major && A.pass == 0u) {
             cnt = __reduce_add_sync(0xffffffffu, cnt);
             if (lane == 0 && cnt) atomicAdd(&A.counts[q], (unsigned long long)cnt);
             __syncthreads();
@@ -301,7 +407,9 @@ __global__ void __launch_bounds__(RTHREADS) k_range(RangeArgs A) {
         }
         uint64_t total;
         const uint64_t ex = block_exscan64(cnt, S.scan, total);
-        if (warp == 0) {
+        if (A.pass == 2u) {
+            if (tid == 0) S.base = A.item_off[qi];
+        } else if (warp == 0) {
             uint64_t prefix; uint32_t pa, pb;
             const bool ok = lookback64(A.recs, item, epoch, total, 0, 0, prefix, pa, pb);
             if (lane == 0) {

@@ -27,10 +27,11 @@ def _time(fn, reps: int) -> float:
 
 
 def tune_batch(ctx, batch, count_only: bool = True, ctas=(0, 1, 2, 4), reps: int = 2):
-    """Work order (query by query / tile by tile) x resident CTAs per SM for
-    the persistent range launch, timed on `batch`.  Tile-by-tile order is
-    tried only for count-only batches (it does not produce row ids)."""
-    orders = (0, 1) if count_only else (0,)
+    """Work order x resident CTAs per SM for the persistent range launch,
+    timed on `batch`.  Count-only batches try query by query (0) and tile by
+    tile (1); batches with row ids try query by query with the look-back (0)
+    and two tile-by-tile passes around a scan (2)."""
+    orders = (0, 1) if count_only else (0, 2)
     table = {}
     for order, c in itertools.product(orders, ctas):
         ctx.set_tuning(TUNE_RANGE_ORDER, order)

@@ -219,7 +219,7 @@ def test_relic_all_comparisons_and_orders(gpu_ctx):
                 assert np.array_equal(got, ref), (order, ctas)
         assert all(int(ref[i]) == w for i, w in enumerate(want) if w is not None)
     finally:
-        gpu_ctx.set_tuning(L.TUNE_RANGE_ORDER, 0)
+        gpu_ctx.set_tuning(L.TUNE_RANGE_ORDER, 2)
         gpu_ctx.set_tuning(L.TUNE_RANGE_CTAS, 0)
 
 
@@ -262,3 +262,42 @@ def test_cumulative_rows_any_stride(gpu_ctx):
                 del B, idx
     finally:
         gpu_ctx.set_tuning(L.TUNE_CUM_STRIDE, 0)
+
+
+def test_row_id_orders_agree(gpu_ctx):
+    """A batch with row ids gives the same counts, ids and per-query starts
+    query by query (look-back) and in two tile-by-tile passes around a scan,
+    at every resident-CTA setting; ids equal the scan's."""
+    import libfastlib_b200 as L
+    rng = np.random.default_rng(17)
+    n = 1_000_003
+    c0 = rng.integers(0, 800, n).astype(np.uint32)
+    c1 = rng.normal(size=n).astype(np.float32)
+    i0 = L.Index.build(gpu_ctx, L.RELIC, c0)
+    i1 = L.Index.build(gpu_ctx, L.BIN, c1, nbins=300)
+    queries, want = [], []
+    for q in range(70):
+        a, b = sorted(rng.integers(0, 801, 2))
+        lo, hi = sorted(rng.normal(size=2))
+        if q % 10 == 3:
+            a, b = 900, 901  # no hits
+        terms = [i0.term(float(a), float(b) + 0.5)] + ([i1.term(float(lo), float(hi))] if q % 3 else [])
+        m = (c0 >= a) & (c0 < b + 0.5)
+        if q % 3:
+            m &= (c1.astype(np.float64) >= lo) & (c1.astype(np.float64) < hi)
+        queries.append(terms)
+        want.append(np.flatnonzero(m).astype(np.uint32))
+    B = L.Batch(gpu_ctx, queries, rid_cap=sum(len(w) for w in want))
+    try:
+        for order in (0, 2):
+            gpu_ctx.set_tuning(L.TUNE_RANGE_ORDER, order)
+            for ctas in (0, 1, 3):
+                gpu_ctx.set_tuning(L.TUNE_RANGE_CTAS, ctas)
+                B.run()
+                counts = B.counts()
+                for q, w in enumerate(want):
+                    assert int(counts[q]) == len(w), (order, ctas, q)
+                    assert np.array_equal(B.rids(q, len(w)), w), (order, ctas, q)
+    finally:
+        gpu_ctx.set_tuning(L.TUNE_RANGE_ORDER, 2)
+        gpu_ctx.set_tuning(L.TUNE_RANGE_CTAS, 0)

@@ -525,7 +525,7 @@ def _with_row_ids(L, tune, ctx, stream, queries, counts):
     assert [int(c) for c in got] == [int(c) for c in counts], "row-id batch counts differ"
     del g
     B.close()
-    ctx.set_tuning(L.TUNE_RANGE_ORDER, 2)
+    ctx.set_tuning(L.TUNE_RANGE_ORDER, 1)
     ctx.set_tuning(L.TUNE_RANGE_CTAS, 0)
     return {"queries": len(queries), "row_ids": total, "queries_per_s": len(queries) / (ms / 1e3), "ms_per_batch": ms,
             "row_ids_per_s": total / (ms / 1e3),
@@ -549,7 +549,7 @@ def _batched_vs_single(L, tune, ctx, stream, queries, nsingle, peak):
     counts = B.counts()
     del g
     nbytes = B.nbytes()
-    ctx.set_tuning(L.TUNE_RANGE_ORDER, 2)
+    ctx.set_tuning(L.TUNE_RANGE_ORDER, 1)
     ctx.set_tuning(L.TUNE_RANGE_CTAS, 0)
     singles = [L.Batch(ctx, [q], 0) for q in queries[:nsingle]]
     for b in singles[:4]:

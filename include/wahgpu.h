@@ -72,8 +72,8 @@ int64_t wahgpu_ctx_launches(wahgpu_ctx* ctx);
  * rejected with WAHGPU_EINVAL. */
 #define WAHGPU_TUNE_DENSE_TILE 1  /* groups per tile of the dense-path kernel: 1024 | 2048 | 4096 */
 #define WAHGPU_TUNE_DENSE_ENGINE 4 /* canonical-result operators: 0 auto, 1 group-space kernel, 2 word-space merge */
-#define WAHGPU_TUNE_RANGE_ORDER 2 /* batch work order: 0 query by query; 1 tile by tile for count-only batches, \
-                                     else query by query; 2 (default) tile by tile, row ids of several queries \
+#define WAHGPU_TUNE_RANGE_ORDER 2 /* batch work order: 0 query by query; 1 (default) tile by tile for count-only \
+                                     batches, else query by query; 2 tile by tile, row ids of several queries \
                                      placed by a count pass and a scan */
 #define WAHGPU_TUNE_RANGE_CTAS 3  /* resident CTAs per SM of the persistent range launch: 0 (all that fit) .. 32 */
 #define WAHGPU_TUNE_CUM_STRIDE 5  /* bitmaps per cumulative row of indexes built or attached later: 0 auto, 1 none, >= 2 that stride */

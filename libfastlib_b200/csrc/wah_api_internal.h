@@ -26,7 +26,7 @@ struct wahgpu_ctx {
     uint64_t launches = 0;
     uint32_t dense_tile = 2048;         // WAHGPU_TUNE_DENSE_TILE
     uint32_t dense_engine = 0;          // WAHGPU_TUNE_DENSE_ENGINE
-    uint32_t range_order = 2;           // WAHGPU_TUNE_RANGE_ORDER
+    uint32_t range_order = 1;           // WAHGPU_TUNE_RANGE_ORDER
     uint32_t range_ctas = 0;            // WAHGPU_TUNE_RANGE_CTAS (0: as many as fit)
     uint32_t cum_stride = 0;            // WAHGPU_TUNE_CUM_STRIDE (0 auto, 1 none)
 };

@@ -219,7 +219,7 @@ def test_relic_all_comparisons_and_orders(gpu_ctx):
                 assert np.array_equal(got, ref), (order, ctas)
         assert all(int(ref[i]) == w for i, w in enumerate(want) if w is not None)
     finally:
-        gpu_ctx.set_tuning(L.TUNE_RANGE_ORDER, 2)
+        gpu_ctx.set_tuning(L.TUNE_RANGE_ORDER, 1)
         gpu_ctx.set_tuning(L.TUNE_RANGE_CTAS, 0)
 
 
@@ -299,5 +299,5 @@ def test_row_id_orders_agree(gpu_ctx):
                     assert int(counts[q]) == len(w), (order, ctas, q)
                     assert np.array_equal(B.rids(q, len(w)), w), (order, ctas, q)
     finally:
-        gpu_ctx.set_tuning(L.TUNE_RANGE_ORDER, 2)
+        gpu_ctx.set_tuning(L.TUNE_RANGE_ORDER, 1)
         gpu_ctx.set_tuning(L.TUNE_RANGE_CTAS, 0)

@@ -228,8 +228,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--dense-tile", type=int, default=2048, choices=[1024, 2048, 4096],
                     help="groups per tile of the dense-path kernel")
-    ap.add_argument("--dense-engine", type=int, default=0, choices=[0, 1, 2],
-                    help="canonical-result operators: 0 auto, 1 group-space kernel, 2 word-space merge")
+    ap.add_argument("--dense-engine", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="canonical-result operators: 0 auto, 1 pipelined group-space kernel, 2 word-space merge, "
+                         "3 two-pass group-space kernels")
     ap.add_argument("--only-range", default=None,
                     help="ROWS:QUERIES — only the binned range case at that size, tile-major count batch run "
                          "warmup+steps times (for ncu)")
@@ -333,11 +334,13 @@ def main():
         ctx.set_stream(None)
         return
 
-    # per-call device time of each operator call (one kernel and its metadata
+    # per-call device time of each operator call (its kernels and metadata
     # memset): a graph of REPS back-to-back calls, timed by events.  The
-    # roofline line is for the dense-path kernel k_dense, which the reference's
-    # _d2 rule (|a|+|b|)*31 > nbits selects for the denser pairs and which
-    # takes most of the step.
+    # roofline line is for the dense-path calls, which the reference's _d2
+    # rule (|a|+|b|)*31 > nbits selects for the denser pairs and which take
+    # most of the step: by default the pipelined k_dense, with
+    # --dense-engine 3 the two-pass group-space kernels (k_gop, k_gscan,
+    # k_gpack).
     REPS = 10
     call_ms = {}
     dense_b = 0
@@ -368,7 +371,11 @@ def main():
     peak, peak_kind = peaks()
     achieved = dense_b / (dense_ms / 1e3) / 1e9 if dense_ms > 0 else None
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "k_dense_traffic.json")
+    engine_kernels = {0: "k_dense", 1: "k_dense", 3: "k_gop + k_gscan + k_gpack",
+                      2: "k_merge"}[args.dense_engine]
+    traffic_file = {0: "k_dense_traffic.json", 1: "k_dense_traffic.json", 3: "two_pass_traffic.json",
+                    2: "k_merge_traffic.json"}[args.dense_engine]
+    tp = os.path.join(ROOT, "profiles", traffic_file)
     if os.path.exists(tp):
         try:
             per = json.load(open(tp))["bytes_per_launch"]
@@ -450,10 +457,10 @@ def main():
             "config": _config(world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if achieved else None, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_dense (+ its metadata memset), per-call CUDA events over the dense-path calls "
-                                   + ", ".join(dense_calls),
-                         "traffic_source": "profiles/k_dense_traffic.json (ncu dram__bytes_read.sum + "
-                                           "dram__bytes_write.sum per launch)"},
+                         "kernel": engine_kernels + " (+ the metadata memset), per-call CUDA events over the "
+                                   "dense-path calls " + ", ".join(dense_calls),
+                         "traffic_source": f"profiles/{traffic_file} (ncu dram__bytes_read.sum + "
+                                           "dram__bytes_write.sum per operator call)"},
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "cpu_baseline": cpu,

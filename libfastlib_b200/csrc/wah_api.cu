@@ -4,7 +4,7 @@
 #include "wah_plan.h"
 #include "wah_merge.cuh"
 #include "wah_kernels.cuh"
-#include "wah_dense.cuh"
+#include "wah_gop.cuh"
 #include "wah_api_internal.h"
 
 #include <cuda_runtime.h>
@@ -166,7 +166,7 @@ extern "C" int wahgpu_ctx_set_tuning(wahgpu_ctx* ctx, int key, int64_t value) {
         ctx->dense_tile = (uint32_t)value;
         return WAHGPU_OK;
     case WAHGPU_TUNE_DENSE_ENGINE:
-        if (value < 0 || value > 2) return wg_fail(ctx, WAHGPU_EINVAL, "dense engine must be 0, 1 or 2");
+        if (value < 0 || value > 3) return wg_fail(ctx, WAHGPU_EINVAL, "dense engine must be 0, 1, 2 or 3");
         ctx->dense_engine = (uint32_t)value;
         return WAHGPU_OK;
     case WAHGPU_TUNE_RANGE_ORDER:
@@ -539,6 +539,68 @@ int wg_launch_dense(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_
     return WAHGPU_OK;
 }
 
+// Two-pass group-space engine (wah_gop.cuh): expand + operate into dense
+// result patterns, scan the tiles' head counts, pack the words.
+int wg_launch_gop(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t groups,
+                  uint32_t anb, uint32_t aval, wahgpu_bv* res) {
+    int rc = bv_reserve(res, (uint64_t)x->h.n + y->h.n);
+    if (rc) return rc;
+    rc = wg_gtile(x);
+    if (rc) return rc;
+    rc = wg_gtile(y);
+    if (rc) return rc;
+    const uint32_t ntiles = (groups + GT - 1) / GT;
+    uint32_t* R = static_cast<uint32_t*>(wg_alloc(ctx, (size_t)ntiles * GT * 4));
+    uint4* tiles = static_cast<uint4*>(wg_alloc(ctx, (size_t)ntiles * 16));
+    if (!R || !tiles) {
+        wg_free(ctx, R); wg_free(ctx, tiles);
+        return wg_fail(ctx, WAHGPU_ENOMEM, "allocation of %u tiles of result patterns failed", ntiles);
+    }
+    GopArgs a;
+    a.xw = x->words; a.xgt = x->gt; a.nx = x->h.n;
+    a.yw = y->words; a.ygt = y->gt; a.ny = y->h.n;
+    a.groups = groups; a.ntiles = ntiles;
+    a.R = R; a.tiles = tiles;
+    a.out = res->words; a.obp = res->bpos; a.meta = res->meta;
+    a.aval = aval; a.anb = anb;
+    cudaStream_t s = ctx->stream;
+    rc = WAHGPU_OK;
+    if (cudaMemsetAsync(res->meta, 0, sizeof(DevMeta), s) != cudaSuccess) rc = wg_fail(ctx, WAHGPU_ECUDA, "memset failed");
+    if (!rc) {
+        const uint32_t grid = (ntiles + GWARPS - 1) / GWARPS;
+        const size_t sm_op = GWARPS * sizeof(GopWarp), sm_pack = GWARPS * sizeof(GpackWarp);
+        static bool attrs = false;
+        if (!attrs) {
+            cudaFuncSetAttribute(k_gop<OP_AND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_op);
+            cudaFuncSetAttribute(k_gop<OP_OR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_op);
+            cudaFuncSetAttribute(k_gop<OP_XOR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_op);
+            cudaFuncSetAttribute(k_gop<OP_MINUS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_op);
+            cudaFuncSetAttribute(k_gpack, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pack);
+            attrs = true;
+        }
+        switch (op) {
+        case OP_AND: k_gop<OP_AND><<<grid, GTHREADS, sm_op, s>>>(a); break;
+        case OP_OR: k_gop<OP_OR><<<grid, GTHREADS, sm_op, s>>>(a); break;
+        case OP_XOR: k_gop<OP_XOR><<<grid, GTHREADS, sm_op, s>>>(a); break;
+        default: k_gop<OP_MINUS><<<grid, GTHREADS, sm_op, s>>>(a); break;
+        }
+        k_gscan<<<1, 1024, 0, s>>>(a);
+        k_gpack<<<grid, GTHREADS, sm_pack, s>>>(a);
+        ctx->launches += 3;
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = wg_fail(ctx, WAHGPU_ECUDA, "launch failed: %s", cudaGetErrorString(e));
+    }
+    // stream-ordered: the next user of these blocks on this context's
+    // stream runs after the launches above
+    wg_free(ctx, R);
+    wg_free(ctx, tiles);
+    if (rc) return rc;
+    res->h_valid = false;
+    res->gt_valid = false;
+    res->compressed_form = true;
+    return WAHGPU_OK;
+}
+
 // A one-word device bitvector holding the collapsed form of an all-zero
 // operand (do_cnt(), src/bitvector.cpp:601-604).
 static int collapsed_copy(wahgpu_ctx* ctx, const wahgpu_bv* src, wahgpu_bv** out) {
@@ -572,11 +634,15 @@ static OperandMeta opmeta(const wahgpu_bv* b) {
     return m;
 }
 
-// Engine for a canonical-result operator (WAHGPU_TUNE_DENSE_ENGINE): 1 group
-// space, 2 word space, 0 (default) group space — measured faster at every
-// density of the raw-WAH workload.
+// Engine for a canonical-result operator (WAHGPU_TUNE_DENSE_ENGINE): 1 the
+// pipelined group-space kernel, 2 the word-space merge, 3 the two-pass
+// group-space kernels; 0 (default) the pipelined kernel, measured fastest on
+// the raw-WAH workload.
 static bool dense_in_word_space(const wahgpu_ctx* ctx, const wahgpu_bv*, const wahgpu_bv*, uint32_t) {
     return ctx->dense_engine == 2;
+}
+static bool dense_two_pass(const wahgpu_ctx* ctx) {
+    return ctx->dense_engine == 3;
 }
 
 extern "C" int wahgpu_bv_binop_into(wahgpu_ctx* ctx, int op, int inplace, wahgpu_bv* a, wahgpu_bv* b,
@@ -614,6 +680,8 @@ extern "C" int wahgpu_bv_binop_into(wahgpu_ctx* ctx, int op, int inplace, wahgpu
         // (no step states) when the tuning asks for it
         if (dense_in_word_space(ctx, ca, cb, G))
             rc = wg_launch_merge(ctx, op, false, false, false, ca, cb, G, anb, aval, res);
+        else if (dense_two_pass(ctx))
+            rc = wg_launch_gop(ctx, op, ca, cb, G, anb, aval, res);
         else
             rc = wg_launch_dense(ctx, op, ca, cb, G, anb, aval, res);
         break;

@@ -1,0 +1,345 @@
+// Two-pass group-space engine for the operators whose result compress()
+// leaves canonical (the reference's _d2 / _d1 / _c1 / _c0 paths and the
+// all-literal loops, src/bitvector.cpp:2545-2830, 2981-3278, 3354-3619,
+// 3748-4079): after compress() the result words depend only on the result
+// bits, one word per maximal run of equal all-0 / all-1 groups (a fill when
+// the run holds two or more groups) and one literal per mixed group.
+//
+// Three launches, no look-back and no cross-CTA waits:
+//  * k_gop<OP>: one warp per tile of GT = 1024 groups (the stride of the
+//    operands' group-tile index, which gives each tile's word range).  Both
+//    operands' words over the tile are staged in shared memory at once with
+//    cp.async and expanded to one 31-bit pattern per group (a word-start
+//    marker per word and a warp max-scan find the word of every group, so a
+//    fill costs one marker whatever its length; an operand with one word per
+//    group is read directly); the result patterns R = a OP b are stored
+//    densely (4 bytes per group) and the tile's run heads (a mixed group, or
+//    a class change) are counted, with the first head's position and the
+//    popcount.  Warps never wait for one another.
+//  * k_gscan: one CTA turns the tiles' head counts into output offsets and
+//    each tile's next head position (a suffix minimum), and fills in the
+//    result's metadata.
+//  * k_gpack: one warp per tile with heads re-reads R, ranks the heads and
+//    writes the words in order: a mixed head's literal, or the run word
+//    whose length reaches the next head.
+// Lanes own groups in eight chunks of four consecutive groups (group
+// 128*j + 4*lane + e of the tile), so every global access of R is a
+// coalesced 16-byte vector and the chunk-major order is the group order.
+#ifndef WAH_GOP_CUH
+#define WAH_GOP_CUH
+#include "wah_dense.cuh"
+
+namespace wah {
+
+constexpr int GT = DT;                    // groups per tile: one warp's tile (the group-tile index stride)
+constexpr int GWARPS = 4;                 // warps (tiles) per CTA
+constexpr int GTHREADS = GWARPS * 32;
+constexpr int GWPL = 33;                  // staged words per lane when counting (odd: conflict-free)
+constexpr uint32_t GNONE = 0xFFFFFFFFu;   // no head in the tile
+static_assert(GT == 8 * 128 && GWPL * 32 >= GT, "tile shape");
+
+struct GopArgs {
+    const uint32_t* xw; const uint32_t* xgt; uint32_t nx;
+    const uint32_t* yw; const uint32_t* ygt; uint32_t ny;
+    uint32_t groups, ntiles;
+    uint32_t* R;          // ntiles * GT result patterns
+    uint4* tiles;         // per tile: k_gop {heads, first head, popcount, -}; k_gscan {offset, next head, heads, -}
+    uint32_t* out; uint32_t* obp; DevMeta* meta;
+    uint32_t aval, anb;
+};
+
+// per warp: both operands' words over its tile and the word-start markers
+struct GopWarp {
+    uint32_t ws[2][GWPL * 32];
+    uint16_t mk[GT];
+};
+// per warp: the tile's heads by rank
+struct GpackWarp {
+    uint32_t hp[GT];                      // head position | class << 30
+    uint32_t lv[GT];                      // a mixed head's literal
+};
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Word range of one operand over the tile [g0, g1): words [wi0, wend), the
+// first starting at group s0.  gt: the operand's group-tile index (entry
+// past the end = (n, G)).  Returns false for words the metadata scan would
+// have rejected (a tile word count that cannot be).
+__device__ __forceinline__ bool gop_range(const uint32_t* __restrict__ gt, uint32_t n, uint32_t g0, uint32_t g1,
+                                          uint32_t& wi0, uint32_t& s0, uint32_t& nw) {
+    const uint32_t e0 = g0 / DT, e1 = (g1 + DT - 1) / DT;
+    wi0 = __ldg(gt + 2 * e0); s0 = __ldg(gt + 2 * e0 + 1);
+    const uint32_t wi1 = __ldg(gt + 2 * e1), s1 = __ldg(gt + 2 * e1 + 1);
+    // the word covering g1 belongs to the tile when it starts before g1
+    const uint32_t wend = (wi1 < n && s1 < g1) ? wi1 + 1u : wi1;
+    nw = wend - wi0;
+    const bool ok = wi0 < n && wend <= n && wend > wi0 && nw <= (uint32_t)GT && !(g0 > 0 && s0 >= g0 && wi0 == 0);
+    if (!ok) nw = 0;
+    return ok;
+}
+
+// Places one operand's staged words: marks, at the first group of the tile
+// each word covers, the word's index + 1.  mk must be zero.
+__device__ __forceinline__ void gop_mark(const uint32_t* ws, uint16_t* mk, uint32_t nw, uint32_t s0, uint32_t g0,
+                                         uint32_t g1) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t k0 = lane * (uint32_t)GWPL;
+    uint32_t cnt = 0;
+    for (uint32_t i = 0; i < (uint32_t)GWPL; ++i) {
+        const uint32_t k = k0 + i;
+        if (k < nw) cnt += wgroups(ws[k]);
+    }
+    uint32_t x = cnt;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= (uint32_t)d) x += t;
+    }
+    uint32_t p = s0 + x - cnt;
+    for (uint32_t i = 0; i < (uint32_t)GWPL; ++i) {
+        const uint32_t k = k0 + i;
+        if (k >= nw) break;
+        const uint32_t c = wgroups(ws[k]);
+        if (p < g1 && p + c > g0) mk[max(p, g0) - g0] = (uint16_t)(k + 1u);
+        p += c;
+    }
+}
+
+// Patterns of chunk j (groups 128*j + 4*lane + e of the tile) of an impure
+// operand; carry = the last word index + 1 seen before the chunk.
+__device__ __forceinline__ uint4 gop_chunk(const uint32_t* ws, const uint16_t* mk, uint32_t j, uint32_t& carry) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint2 m = reinterpret_cast<const uint2*>(mk)[32 * j + lane];
+    const uint32_t r0 = m.x & 0xFFFFu, r1 = max(r0, m.x >> 16), r2 = max(r1, m.y & 0xFFFFu), r3 = max(r2, m.y >> 16);
+    uint32_t inc = r3;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, inc, d);
+        if (lane >= (uint32_t)d) inc = max(inc, t);
+    }
+    uint32_t ex = __shfl_up_sync(0xffffffffu, inc, 1);
+    if (lane == 0) ex = 0;
+    ex = max(ex, carry);
+    carry = max(carry, __shfl_sync(0xffffffffu, inc, 31));
+    const uint32_t i0 = max(ex, r0), i1 = max(ex, r1), i2 = max(ex, r2), i3 = max(ex, r3);  // >= 1 inside the tile
+    return make_uint4(wpattern(ws[i0 ? i0 - 1u : 0u]), wpattern(ws[i1 ? i1 - 1u : 0u]),
+                      wpattern(ws[i2 ? i2 - 1u : 0u]), wpattern(ws[i3 ? i3 - 1u : 0u]));
+}
+
+template <int OP>
+__global__ void __launch_bounds__(GTHREADS) k_gop(GopArgs A) {
+    extern __shared__ __align__(16) unsigned char gsm[];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t t = blockIdx.x * GWARPS + warp;
+    if (t >= A.ntiles) return;
+    GopWarp& W = reinterpret_cast<GopWarp*>(gsm)[warp];
+    const uint32_t G = A.groups;
+    const uint32_t g0 = t * (uint32_t)GT, g1 = min(g0 + (uint32_t)GT, G);
+    const uint32_t ng = g1 - g0;
+    uint32_t xi0, xs0, xn, yi0, ys0, yn;
+    const bool ok = gop_range(A.xgt, A.nx, g0, g1, xi0, xs0, xn) & gop_range(A.ygt, A.ny, g0, g1, yi0, ys0, yn);
+    if (!ok && lane == 0) atomicExch(&A.meta->status, DEV_ERR_FORMAT);
+    // both operands' words in flight at once
+    for (uint32_t i = lane; i < xn; i += 32) cp_async4(&W.ws[0][i], A.xw + xi0 + i);
+    for (uint32_t i = lane; i < yn; i += 32) cp_async4(&W.ws[1][i], A.yw + yi0 + i);
+    const bool xpure = xs0 == g0 && xn == ng, ypure = ys0 == g0 && yn == ng;
+    // the result before the tile (the words covering g0 - 1)
+    uint32_t prev = 0;
+    if (g0 > 0 && ok) {
+        const uint32_t xp = __ldg(A.xw + (xs0 < g0 ? xi0 : xi0 - 1u));
+        const uint32_t yp = __ldg(A.yw + (ys0 < g0 ? yi0 : yi0 - 1u));
+        prev = op2<OP>(wpattern(xp), wpattern(yp));
+    }
+    cp_async_wait_all();
+    __syncwarp();
+    uint32_t* R = A.R + g0;
+    uint32_t heads = 0, first = GNONE, popc = 0;
+    uint32_t xc = 0, yc = 0;
+    uint32_t before = prev;  // the result of the group before the current chunk
+    // an impure operand is placed first (its markers then its patterns);
+    // two impure operands share the marker array one after the other, so
+    // the second one's patterns are read in a second sweep
+    const bool both = !xpure && !ypure;
+    uint4 xb[8];
+    if (!xpure) {
+        reinterpret_cast<uint2*>(W.mk)[lane] = make_uint2(0u, 0u);
+#pragma unroll
+        for (int j = 1; j < 8; ++j) reinterpret_cast<uint2*>(W.mk)[32 * j + lane] = make_uint2(0u, 0u);
+        __syncwarp();
+        gop_mark(W.ws[0], W.mk, xn, xs0, g0, g1);
+        __syncwarp();
+        if (both) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) xb[j] = gop_chunk(W.ws[0], W.mk, j, xc);
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < 8; ++j) reinterpret_cast<uint2*>(W.mk)[32 * j + lane] = make_uint2(0u, 0u);
+            __syncwarp();
+        }
+    }
+    if (!ypure) {
+        if (xpure) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) reinterpret_cast<uint2*>(W.mk)[32 * j + lane] = make_uint2(0u, 0u);
+            __syncwarp();
+        }
+        if (xpure || both) {
+            gop_mark(W.ws[1], W.mk, yn, ys0, g0, g1);
+            __syncwarp();
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        uint4 a, b;
+        if (xpure) a = pattern4(reinterpret_cast<const uint4*>(W.ws[0])[32 * j + lane]);
+        else if (both) a = xb[j];
+        else a = gop_chunk(W.ws[0], W.mk, j, xc);
+        if (ypure) b = pattern4(reinterpret_cast<const uint4*>(W.ws[1])[32 * j + lane]);
+        else b = gop_chunk(W.ws[1], W.mk, j, yc);
+        const uint4 r = make_uint4(op2<OP>(a.x, b.x), op2<OP>(a.y, b.y), op2<OP>(a.z, b.z), op2<OP>(a.w, b.w));
+        reinterpret_cast<uint4*>(R)[32 * j + lane] = r;
+        uint32_t pb = __shfl_up_sync(0xffffffffu, r.w, 1);
+        if (lane == 0) pb = before;
+        before = __shfl_sync(0xffffffffu, r.w, 31);
+        const uint32_t rv[4] = {r.x, r.y, r.z, r.w};
+        uint32_t pc = cls_of(pb);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const uint32_t pos = 128u * j + 4u * lane + e;
+            const uint32_t c = cls_of(rv[e]);
+            if (pos < ng) {
+                if ((g0 + pos == 0u) || c == C_MIXED || c != pc) { ++heads; first = min(first, g0 + pos); }
+                popc += __popc(rv[e]);
+            }
+            pc = c;
+        }
+    }
+    heads = __reduce_add_sync(0xffffffffu, heads);
+    popc = __reduce_add_sync(0xffffffffu, popc);
+    first = __reduce_min_sync(0xffffffffu, first);
+    if (lane == 0) A.tiles[t] = make_uint4(heads, first, popc, 0u);
+}
+
+// Offsets and next heads of the tiles, and the result's metadata (one CTA of
+// 1024 threads; thread i owns a contiguous chunk of tiles).
+__global__ void __launch_bounds__(1024) k_gscan(GopArgs A) {
+    __shared__ uint32_t s_sum[1024], s_min[1024];
+    __shared__ unsigned long long s_pop;
+    const uint32_t tid = threadIdx.x, T = A.ntiles;
+    const uint32_t ch = (T + 1023u) / 1024u;
+    const uint32_t lo = min(tid * ch, T), hi = min(lo + ch, T);
+    uint32_t sum = 0, mn = GNONE;
+    unsigned long long pop = 0;
+    for (uint32_t i = lo; i < hi; ++i) {
+        const uint4 u = A.tiles[i];
+        sum += u.x; mn = min(mn, u.y); pop += u.z;
+    }
+    if (tid == 0) s_pop = 0;
+    s_sum[tid] = sum; s_min[tid] = mn;
+    __syncthreads();
+    if (pop) atomicAdd(&s_pop, pop);
+    // inclusive prefix sums and suffix minima over the threads (Hillis-Steele)
+    for (uint32_t d = 1; d < 1024u; d <<= 1) {
+        const uint32_t a = tid >= d ? s_sum[tid - d] : 0u;
+        const uint32_t b = tid + d < 1024u ? s_min[tid + d] : GNONE;
+        __syncthreads();
+        s_sum[tid] += a;
+        s_min[tid] = min(s_min[tid], b);
+        __syncthreads();
+    }
+    uint32_t off = s_sum[tid] - sum;
+    uint32_t nxt = tid + 1u < 1024u ? s_min[tid + 1] : GNONE;  // first head after this chunk
+    for (uint32_t i = hi; i > lo; --i) {
+        uint4 u = A.tiles[i - 1];
+        u.w = nxt;
+        nxt = min(nxt, u.y);
+        A.tiles[i - 1] = u;
+    }
+    for (uint32_t i = lo; i < hi; ++i) {
+        const uint4 u = A.tiles[i];
+        A.tiles[i] = make_uint4(off, u.w == GNONE ? A.groups : u.w, u.x, 0u);
+        off += u.x;
+    }
+    if (tid == 1023) {
+        const uint32_t n = s_sum[1023];
+        A.obp[(n + 31u) / 32u] = A.groups;
+        A.meta->n = n;
+        A.meta->groups = A.groups;
+        A.meta->nset = (uint32_t)s_pop;
+        A.meta->anb = A.anb;
+        A.meta->aval = A.aval;
+        if (n == 0) A.meta->w0 = 0;
+    }
+}
+
+// The words of one tile per warp, in order (tiles without heads have none).
+__global__ void __launch_bounds__(GTHREADS) k_gpack(GopArgs A) {
+    extern __shared__ __align__(16) unsigned char gsm[];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t t = blockIdx.x * GWARPS + warp;
+    if (t >= A.ntiles) return;
+    const uint4 info = A.tiles[t];
+    const uint32_t off = info.x, nxt = info.y, cnt = info.z;
+    if (cnt == 0) return;
+    GpackWarp& W = reinterpret_cast<GpackWarp*>(gsm)[warp];
+    const uint32_t G = A.groups;
+    const uint32_t g0 = t * (uint32_t)GT, g1 = min(g0 + (uint32_t)GT, G);
+    const uint32_t ng = g1 - g0;
+    const uint4* R4 = reinterpret_cast<const uint4*>(A.R + g0);
+    uint4 rv[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) rv[j] = R4[32 * j + lane];
+    uint32_t before = g0 > 0 ? A.R[g0 - 1] : 0u;
+    uint32_t rk = 0;  // heads before the chunk
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const uint32_t r[4] = {rv[j].x, rv[j].y, rv[j].z, rv[j].w};
+        uint32_t pb = __shfl_up_sync(0xffffffffu, r[3], 1);
+        if (lane == 0) pb = before;
+        before = __shfl_sync(0xffffffffu, r[3], 31);
+        uint32_t pc = cls_of(pb), m = 0;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const uint32_t pos = 128u * j + 4u * lane + e;
+            const uint32_t c = cls_of(r[e]);
+            if (pos < ng && ((g0 + pos == 0u) || c == C_MIXED || c != pc)) m |= 1u << e;
+            pc = c;
+        }
+        const uint32_t h = __popc(m);
+        uint32_t x = h;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t tt = __shfl_up_sync(0xffffffffu, x, d);
+            if (lane >= (uint32_t)d) x += tt;
+        }
+        uint32_t k = rk + x - h;
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            if ((m >> e) & 1u) {
+                W.hp[k] = (g0 + 128u * j + 4u * lane + e) | (cls_of(r[e]) << 30);
+                W.lv[k] = r[e];
+                ++k;
+            }
+        rk += __shfl_sync(0xffffffffu, x, 31);
+    }
+    __syncwarp();
+    bool fill = false;
+    for (uint32_t k = lane; k < cnt; k += 32) {
+        const uint32_t h = W.hp[k];
+        const uint32_t pos = h & 0x3FFFFFFFu, c = h >> 30;
+        const uint32_t next = k + 1u < cnt ? (W.hp[k + 1] & 0x3FFFFFFFu) : nxt;
+        const uint32_t wd = run_word(c, next - pos, W.lv[k], false);
+        const uint32_t o = off + k;
+        A.out[o] = wd;
+        if ((o & 31u) == 0u) A.obp[o >> 5] = pos;
+        if (o == 0u) A.meta->w0 = wd;
+        fill |= is_fill(wd);
+    }
+    if (__any_sync(0xffffffffu, fill) && lane == 0) atomicOr(&A.meta->nfill, 1u);
+}
+
+}  // namespace wah
+#endif

@@ -63,17 +63,23 @@ def test_full_size_dense_tiles(gpu_ctx, density, tile):
 
 
 class _tile:
+    """The pipelined group-space kernel (WAHGPU_TUNE_DENSE_ENGINE = 1) at a
+    given tile size."""
+
     def __init__(self, ctx, tile):
         self.ctx, self.tile = ctx, tile
 
     def __enter__(self):
         import libfastlib_b200 as L
         self.old = self.ctx.get_tuning(L.TUNE_DENSE_TILE)
+        self.old_engine = self.ctx.get_tuning(L.TUNE_DENSE_ENGINE)
         self.ctx.set_tuning(L.TUNE_DENSE_TILE, self.tile)
+        self.ctx.set_tuning(L.TUNE_DENSE_ENGINE, 1)
 
     def __exit__(self, *exc):
         import libfastlib_b200 as L
         self.ctx.set_tuning(L.TUNE_DENSE_TILE, self.old)
+        self.ctx.set_tuning(L.TUNE_DENSE_ENGINE, self.old_engine)
 
 
 def _full_size(gpu_ctx, density):
@@ -203,6 +209,44 @@ def test_dense_path_fuzz(gpu_ctx, tile):
                     ref, rc = oracle.binop(op, a, b, inplace=bool(ip))
                     w, c = _bin(gpu_ctx, op, a, b, ip)
                     assert c == rc and np.array_equal(w, ref), (trial, op, ip)
+
+
+@pytest.mark.parametrize("engine", [1, 3])
+def test_group_space_engines_fuzz(gpu_ctx, engine):
+    """Both group-space engines (1 pipelined, 3 two-pass): dense operands
+    with fills longer than a tile, pure and impure tiles, count-1
+    fill words among literals, partial last tiles."""
+    import libfastlib_b200 as L
+    rng = np.random.default_rng(78 + engine)
+    gpu_ctx.set_tuning(L.TUNE_DENSE_ENGINE, engine)
+    try:
+        for trial in range(12):
+            ng = int(rng.integers(1, 12)) * 4096 + int(rng.integers(0, 4096)) if trial % 3 else int(rng.integers(1, 5000))
+            wa, wb = _dense_words(rng, ng), _dense_words(rng, ng)
+            anb = int(rng.integers(0, 31))
+            a = G.serialize(wa, anb, int(rng.integers(0, 1 << 31)))
+            b = G.serialize(wb, anb, int(rng.integers(0, 1 << 31)))
+            if oracle.is_degenerate(a) or oracle.is_degenerate(b):
+                continue
+            for op in range(4):
+                for ip in (0, 1):
+                    ref, rc = oracle.binop(op, a, b, inplace=bool(ip))
+                    w, c = _bin(gpu_ctx, op, a, b, ip)
+                    assert c == rc and np.array_equal(w, ref), (trial, op, ip)
+    finally:
+        gpu_ctx.set_tuning(L.TUNE_DENSE_ENGINE, 0)
+
+
+@pytest.mark.parametrize("engine", [1, 3])
+@pytest.mark.parametrize("density", [0.1, 0.5])
+def test_group_space_engines_full_size(gpu_ctx, density, engine):
+    """Both group-space engines give the reference's words at 2^28 bits."""
+    import libfastlib_b200 as L
+    gpu_ctx.set_tuning(L.TUNE_DENSE_ENGINE, engine)
+    try:
+        _full_size(gpu_ctx, density)
+    finally:
+        gpu_ctx.set_tuning(L.TUNE_DENSE_ENGINE, 0)
 
 
 def test_dense_small_sizes(gpu_ctx):

@@ -338,9 +338,8 @@ def main():
     # memset): a graph of REPS back-to-back calls, timed by events.  The
     # roofline line is for the dense-path calls, which the reference's _d2
     # rule (|a|+|b|)*31 > nbits selects for the denser pairs and which take
-    # most of the step: by default the pipelined k_dense, with
-    # --dense-engine 3 the two-pass group-space kernels (k_gop, k_gscan,
-    # k_gpack).
+    # most of the step: by default the two-pass group-space kernels (k_gop,
+    # k_gpack), with --dense-engine 1 the pipelined k_dense.
     REPS = 10
     call_ms = {}
     dense_b = 0
@@ -371,9 +370,9 @@ def main():
     peak, peak_kind = peaks()
     achieved = dense_b / (dense_ms / 1e3) / 1e9 if dense_ms > 0 else None
     traffic = None
-    engine_kernels = {0: "k_dense", 1: "k_dense", 3: "k_gop + k_gscan + k_gpack",
+    engine_kernels = {0: "k_gop + k_gpack", 3: "k_gop + k_gpack", 1: "k_dense",
                       2: "k_merge"}[args.dense_engine]
-    traffic_file = {0: "k_dense_traffic.json", 1: "k_dense_traffic.json", 3: "two_pass_traffic.json",
+    traffic_file = {0: "two_pass_traffic.json", 3: "two_pass_traffic.json", 1: "k_dense_traffic.json",
                     2: "k_merge_traffic.json"}[args.dense_engine]
     tp = os.path.join(ROOT, "profiles", traffic_file)
     if os.path.exists(tp):

@@ -540,7 +540,7 @@ int wg_launch_dense(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_
 }
 
 // Two-pass group-space engine (wah_gop.cuh): expand + operate into dense
-// result patterns, scan the tiles' head counts, pack the words.
+// result patterns with per-tile head counts, then pack the words.
 int wg_launch_gop(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t groups,
                   uint32_t anb, uint32_t aval, wahgpu_bv* res) {
     int rc = bv_reserve(res, (uint64_t)x->h.n + y->h.n);
@@ -551,7 +551,8 @@ int wg_launch_gop(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t 
     if (rc) return rc;
     const uint32_t ntiles = (groups + GT - 1) / GT;
     uint32_t* R = static_cast<uint32_t*>(wg_alloc(ctx, (size_t)ntiles * GT * 4));
-    uint4* tiles = static_cast<uint4*>(wg_alloc(ctx, (size_t)ntiles * 16));
+    const uint32_t nseg = (ntiles + GSEG - 1) / GSEG;
+    uint4* tiles = static_cast<uint4*>(wg_alloc(ctx, ((size_t)ntiles + nseg) * 16));
     if (!R || !tiles) {
         wg_free(ctx, R); wg_free(ctx, tiles);
         return wg_fail(ctx, WAHGPU_ENOMEM, "allocation of %u tiles of result patterns failed", ntiles);
@@ -560,22 +561,23 @@ int wg_launch_gop(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t 
     a.xw = x->words; a.xgt = x->gt; a.nx = x->h.n;
     a.yw = y->words; a.ygt = y->gt; a.ny = y->h.n;
     a.groups = groups; a.ntiles = ntiles;
-    a.R = R; a.tiles = tiles;
+    a.R = R; a.tiles = tiles; a.segs = tiles + ntiles;
     a.out = res->words; a.obp = res->bpos; a.meta = res->meta;
     a.aval = aval; a.anb = anb;
     cudaStream_t s = ctx->stream;
     rc = WAHGPU_OK;
-    if (cudaMemsetAsync(res->meta, 0, sizeof(DevMeta), s) != cudaSuccess) rc = wg_fail(ctx, WAHGPU_ECUDA, "memset failed");
+    if (cudaMemsetAsync(res->meta, 0, sizeof(DevMeta), s) != cudaSuccess ||
+        cudaMemsetAsync(a.segs, 0, (size_t)nseg * 16, s) != cudaSuccess)
+        rc = wg_fail(ctx, WAHGPU_ECUDA, "memset failed");
     if (!rc) {
         const uint32_t grid = (ntiles + GWARPS - 1) / GWARPS;
-        const size_t sm_op = GWARPS * sizeof(GopWarp), sm_pack = GWARPS * sizeof(GpackWarp);
+        const size_t sm_op = GWARPS * sizeof(GopWarp);
         static bool attrs = false;
         if (!attrs) {
             cudaFuncSetAttribute(k_gop<OP_AND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_op);
             cudaFuncSetAttribute(k_gop<OP_OR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_op);
             cudaFuncSetAttribute(k_gop<OP_XOR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_op);
             cudaFuncSetAttribute(k_gop<OP_MINUS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_op);
-            cudaFuncSetAttribute(k_gpack, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pack);
             attrs = true;
         }
         switch (op) {
@@ -584,9 +586,8 @@ int wg_launch_gop(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t 
         case OP_XOR: k_gop<OP_XOR><<<grid, GTHREADS, sm_op, s>>>(a); break;
         default: k_gop<OP_MINUS><<<grid, GTHREADS, sm_op, s>>>(a); break;
         }
-        k_gscan<<<1, 1024, 0, s>>>(a);
-        k_gpack<<<grid, GTHREADS, sm_pack, s>>>(a);
-        ctx->launches += 3;
+        k_gpack<<<grid, GTHREADS, 0, s>>>(a);
+        ctx->launches += 2;
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) rc = wg_fail(ctx, WAHGPU_ECUDA, "launch failed: %s", cudaGetErrorString(e));
     }
@@ -636,13 +637,13 @@ static OperandMeta opmeta(const wahgpu_bv* b) {
 
 // Engine for a canonical-result operator (WAHGPU_TUNE_DENSE_ENGINE): 1 the
 // pipelined group-space kernel, 2 the word-space merge, 3 the two-pass
-// group-space kernels; 0 (default) the pipelined kernel, measured fastest on
-// the raw-WAH workload.
+// group-space kernels; 0 (default) the two-pass kernels, measured fastest
+// on the raw-WAH workload.
 static bool dense_in_word_space(const wahgpu_ctx* ctx, const wahgpu_bv*, const wahgpu_bv*, uint32_t) {
     return ctx->dense_engine == 2;
 }
 static bool dense_two_pass(const wahgpu_ctx* ctx) {
-    return ctx->dense_engine == 3;
+    return ctx->dense_engine == 0 || ctx->dense_engine == 3;
 }
 
 extern "C" int wahgpu_bv_binop_into(wahgpu_ctx* ctx, int op, int inplace, wahgpu_bv* a, wahgpu_bv* b,

@@ -5,7 +5,7 @@
 // bits, one word per maximal run of equal all-0 / all-1 groups (a fill when
 // the run holds two or more groups) and one literal per mixed group.
 //
-// Three launches, no look-back and no cross-CTA waits:
+// Two launches, no look-back and no cross-CTA waits:
 //  * k_gop<OP>: one warp per tile of GT = 1024 groups (the stride of the
 //    operands' group-tile index, which gives each tile's word range).  Both
 //    operands' words over the tile are staged in shared memory at once with
@@ -16,9 +16,7 @@
 //    densely (4 bytes per group) and the tile's run heads (a mixed group, or
 //    a class change) are counted, with the first head's position and the
 //    popcount.  Warps never wait for one another.
-//  * k_gscan: one CTA turns the tiles' head counts into output offsets and
-//    each tile's next head position (a suffix minimum), and fills in the
-//    result's metadata.
+//    Each tile's totals are also added into its segment of GSEG tiles.
 //  * k_gpack: one warp per tile with heads re-reads R, ranks the heads and
 //    writes the words in order: a mixed head's literal, or the run word
 //    whose length reaches the next head.
@@ -36,6 +34,7 @@ constexpr int GWARPS = 4;                 // warps (tiles) per CTA
 constexpr int GTHREADS = GWARPS * 32;
 constexpr int GWPL = 33;                  // staged words per lane when counting (odd: conflict-free)
 constexpr uint32_t GNONE = 0xFFFFFFFFu;   // no head in the tile
+constexpr uint32_t GSEG = 256;            // tiles per segment of the two-level prefix
 static_assert(GT == 8 * 128 && GWPL * 32 >= GT, "tile shape");
 
 struct GopArgs {
@@ -43,7 +42,8 @@ struct GopArgs {
     const uint32_t* yw; const uint32_t* ygt; uint32_t ny;
     uint32_t groups, ntiles;
     uint32_t* R;          // ntiles * GT result patterns
-    uint4* tiles;         // per tile: k_gop {heads, first head, popcount, -}; k_gscan {offset, next head, heads, -}
+    uint4* tiles;         // per tile: {heads, first head (GNONE: none), popcount, -}
+    uint4* segs;          // per GSEG tiles (zeroed before k_gop): {heads, GNONE - first head (0: none), popcount, -}
     uint32_t* out; uint32_t* obp; DevMeta* meta;
     uint32_t aval, anb;
 };
@@ -52,11 +52,6 @@ struct GopArgs {
 struct GopWarp {
     uint32_t ws[2][GWPL * 32];
     uint16_t mk[GT];
-};
-// per warp: the tile's heads by rank
-struct GpackWarp {
-    uint32_t hp[GT];                      // head position | class << 30
-    uint32_t lv[GT];                      // a mixed head's literal
 };
 
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
@@ -82,29 +77,32 @@ __device__ __forceinline__ bool gop_range(const uint32_t* __restrict__ gt, uint3
 }
 
 // Places one operand's staged words: marks, at the first group of the tile
-// each word covers, the word's index + 1.  mk must be zero.
+// each word covers, the word's index + 1.  mk must be zero.  The words are
+// taken 32 at a time, one per lane; a row of literals needs no scan.
 __device__ __forceinline__ void gop_mark(const uint32_t* ws, uint16_t* mk, uint32_t nw, uint32_t s0, uint32_t g0,
                                          uint32_t g1) {
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t k0 = lane * (uint32_t)GWPL;
-    uint32_t cnt = 0;
-    for (uint32_t i = 0; i < (uint32_t)GWPL; ++i) {
-        const uint32_t k = k0 + i;
-        if (k < nw) cnt += wgroups(ws[k]);
-    }
-    uint32_t x = cnt;
+    uint32_t carry = s0;  // first group of the row's first word
+    for (uint32_t base = 0; base < nw; base += 32) {
+        const uint32_t k = base + lane;
+        const bool in = k < nw;
+        const uint32_t wd = in ? ws[k] : 0u;
+        uint32_t p, c = 1;
+        if (__ballot_sync(0xffffffffu, in && is_fill(wd)) == 0u) {
+            p = carry + lane;
+            carry += min(32u, nw - base);
+        } else {
+            c = in ? wgroups(wd) : 0u;
+            uint32_t x = c;
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, x, d);
-        if (lane >= (uint32_t)d) x += t;
-    }
-    uint32_t p = s0 + x - cnt;
-    for (uint32_t i = 0; i < (uint32_t)GWPL; ++i) {
-        const uint32_t k = k0 + i;
-        if (k >= nw) break;
-        const uint32_t c = wgroups(ws[k]);
-        if (p < g1 && p + c > g0) mk[max(p, g0) - g0] = (uint16_t)(k + 1u);
-        p += c;
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, x, d);
+                if (lane >= (uint32_t)d) x += t;
+            }
+            p = carry + x - c;
+            carry += __shfl_sync(0xffffffffu, x, 31);
+        }
+        if (in && p < g1 && p + c > g0) mk[max(p, g0) - g0] = (uint16_t)(k + 1u);
     }
 }
 
@@ -220,72 +218,63 @@ __global__ void __launch_bounds__(GTHREADS) k_gop(GopArgs A) {
     heads = __reduce_add_sync(0xffffffffu, heads);
     popc = __reduce_add_sync(0xffffffffu, popc);
     first = __reduce_min_sync(0xffffffffu, first);
-    if (lane == 0) A.tiles[t] = make_uint4(heads, first, popc, 0u);
-}
-
-// Offsets and next heads of the tiles, and the result's metadata (one CTA of
-// 1024 threads; thread i owns a contiguous chunk of tiles).
-__global__ void __launch_bounds__(1024) k_gscan(GopArgs A) {
-    __shared__ uint32_t s_sum[1024], s_min[1024];
-    __shared__ unsigned long long s_pop;
-    const uint32_t tid = threadIdx.x, T = A.ntiles;
-    const uint32_t ch = (T + 1023u) / 1024u;
-    const uint32_t lo = min(tid * ch, T), hi = min(lo + ch, T);
-    uint32_t sum = 0, mn = GNONE;
-    unsigned long long pop = 0;
-    for (uint32_t i = lo; i < hi; ++i) {
-        const uint4 u = A.tiles[i];
-        sum += u.x; mn = min(mn, u.y); pop += u.z;
-    }
-    if (tid == 0) s_pop = 0;
-    s_sum[tid] = sum; s_min[tid] = mn;
-    __syncthreads();
-    if (pop) atomicAdd(&s_pop, pop);
-    // inclusive prefix sums and suffix minima over the threads (Hillis-Steele)
-    for (uint32_t d = 1; d < 1024u; d <<= 1) {
-        const uint32_t a = tid >= d ? s_sum[tid - d] : 0u;
-        const uint32_t b = tid + d < 1024u ? s_min[tid + d] : GNONE;
-        __syncthreads();
-        s_sum[tid] += a;
-        s_min[tid] = min(s_min[tid], b);
-        __syncthreads();
-    }
-    uint32_t off = s_sum[tid] - sum;
-    uint32_t nxt = tid + 1u < 1024u ? s_min[tid + 1] : GNONE;  // first head after this chunk
-    for (uint32_t i = hi; i > lo; --i) {
-        uint4 u = A.tiles[i - 1];
-        u.w = nxt;
-        nxt = min(nxt, u.y);
-        A.tiles[i - 1] = u;
-    }
-    for (uint32_t i = lo; i < hi; ++i) {
-        const uint4 u = A.tiles[i];
-        A.tiles[i] = make_uint4(off, u.w == GNONE ? A.groups : u.w, u.x, 0u);
-        off += u.x;
-    }
-    if (tid == 1023) {
-        const uint32_t n = s_sum[1023];
-        A.obp[(n + 31u) / 32u] = A.groups;
-        A.meta->n = n;
-        A.meta->groups = A.groups;
-        A.meta->nset = (uint32_t)s_pop;
-        A.meta->anb = A.anb;
-        A.meta->aval = A.aval;
-        if (n == 0) A.meta->w0 = 0;
+    if (lane == 0) {
+        A.tiles[t] = make_uint4(heads, first, popc, 0u);
+        uint4* sg = A.segs + t / GSEG;
+        if (heads) atomicAdd(&sg->x, heads);
+        if (first != GNONE) atomicMax(&sg->y, GNONE - first);
+        if (popc) atomicAdd(&sg->z, popc);
     }
 }
 
 // The words of one tile per warp, in order (tiles without heads have none).
+// The tile's first output index is the heads of the segments before its own
+// plus those of the tiles before it in its segment; the head after the tile
+// is the first head of the later tiles of its segment, else of the first
+// later segment holding one.  A head's word needs the next head's position:
+// the lanes find it with a suffix minimum over the lanes after them, chunks
+// taken last to first.  The warp of the last tile writes the metadata.
 __global__ void __launch_bounds__(GTHREADS) k_gpack(GopArgs A) {
-    extern __shared__ __align__(16) unsigned char gsm[];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t t = blockIdx.x * GWARPS + warp;
-    if (t >= A.ntiles) return;
-    const uint4 info = A.tiles[t];
-    const uint32_t off = info.x, nxt = info.y, cnt = info.z;
-    if (cnt == 0) return;
-    GpackWarp& W = reinterpret_cast<GpackWarp*>(gsm)[warp];
+    const uint32_t T = A.ntiles;
+    if (t >= T) return;
     const uint32_t G = A.groups;
+    const uint32_t sg = t / GSEG, nseg = (T + GSEG - 1) / GSEG;
+    uint32_t off = 0;
+    for (uint32_t i = lane; i < sg; i += 32) off += A.segs[i].x;
+    for (uint32_t i = sg * GSEG + lane; i < t; i += 32) off += A.tiles[i].x;
+    off = __reduce_add_sync(0xffffffffu, off);
+    const uint32_t cnt = A.tiles[t].x;
+    if (t == T - 1) {
+        uint32_t ones = 0;
+        for (uint32_t i = lane; i < nseg; i += 32) ones += A.segs[i].z;
+        ones = __reduce_add_sync(0xffffffffu, ones);
+        if (lane == 0) {
+            const uint32_t n = off + cnt;
+            A.obp[(n + 31u) / 32u] = G;
+            A.meta->n = n;
+            A.meta->groups = G;
+            A.meta->nset = ones;
+            A.meta->anb = A.anb;
+            A.meta->aval = A.aval;
+            if (n == 0) A.meta->w0 = 0;
+        }
+    }
+    if (cnt == 0) return;
+    uint32_t nxt = GNONE;
+    for (uint32_t i0 = t + 1; i0 < min(T, (sg + 1) * GSEG) && nxt == GNONE; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        const uint32_t v = i < min(T, (sg + 1) * GSEG) ? A.tiles[i].y : GNONE;
+        nxt = __reduce_min_sync(0xffffffffu, v);
+    }
+    for (uint32_t i0 = sg + 1; i0 < nseg && nxt == GNONE; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        const uint32_t v = i < nseg ? A.segs[i].y : 0u;
+        const uint32_t f = __reduce_max_sync(0xffffffffu, v);
+        if (f) nxt = GNONE - f;
+    }
+    if (nxt == GNONE) nxt = G;
     const uint32_t g0 = t * (uint32_t)GT, g1 = min(g0 + (uint32_t)GT, G);
     const uint32_t ng = g1 - g0;
     const uint4* R4 = reinterpret_cast<const uint4*>(A.R + g0);
@@ -293,7 +282,8 @@ __global__ void __launch_bounds__(GTHREADS) k_gpack(GopArgs A) {
 #pragma unroll
     for (int j = 0; j < 8; ++j) rv[j] = R4[32 * j + lane];
     uint32_t before = g0 > 0 ? A.R[g0 - 1] : 0u;
-    uint32_t rk = 0;  // heads before the chunk
+    uint32_t hm[8], base[8];
+    uint32_t acc = 0;  // heads before the chunk
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         const uint32_t r[4] = {rv[j].x, rv[j].y, rv[j].z, rv[j].w};
@@ -308,35 +298,48 @@ __global__ void __launch_bounds__(GTHREADS) k_gpack(GopArgs A) {
             if (pos < ng && ((g0 + pos == 0u) || c == C_MIXED || c != pc)) m |= 1u << e;
             pc = c;
         }
+        hm[j] = m;
+        base[j] = acc;
+        acc += __reduce_add_sync(0xffffffffu, __popc(m));
+    }
+    uint32_t later = nxt;  // the first head after the chunk
+    bool fill = false;
+#pragma unroll
+    for (int j = 7; j >= 0; --j) {
+        const uint32_t m = hm[j];
+        const uint32_t g = g0 + 128u * j + 4u * lane;
+        const uint32_t mine = m ? g + (__ffs(m) - 1u) : GNONE;
+        uint32_t y = mine;  // first head in this lane or the lanes after it
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t u = __shfl_down_sync(0xffffffffu, y, d);
+            if (lane + (uint32_t)d < 32u) y = min(y, u);
+        }
+        uint32_t after = __shfl_down_sync(0xffffffffu, y, 1);
+        if (lane == 31) after = GNONE;
+        after = min(after, later);
         const uint32_t h = __popc(m);
         uint32_t x = h;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t tt = __shfl_up_sync(0xffffffffu, x, d);
-            if (lane >= (uint32_t)d) x += tt;
+            const uint32_t u = __shfl_up_sync(0xffffffffu, x, d);
+            if (lane >= (uint32_t)d) x += u;
         }
-        uint32_t k = rk + x - h;
+        uint32_t o = off + base[j] + x - h;
+        const uint32_t r[4] = {rv[j].x, rv[j].y, rv[j].z, rv[j].w};
 #pragma unroll
         for (int e = 0; e < 4; ++e)
             if ((m >> e) & 1u) {
-                W.hp[k] = (g0 + 128u * j + 4u * lane + e) | (cls_of(r[e]) << 30);
-                W.lv[k] = r[e];
-                ++k;
+                const uint32_t rest = m >> (e + 1);
+                const uint32_t next = rest ? g + e + __ffs(rest) : after;
+                const uint32_t wd = run_word(cls_of(r[e]), next - (g + e), r[e], false);
+                A.out[o] = wd;
+                if ((o & 31u) == 0u) A.obp[o >> 5] = g + e;
+                if (o == 0u) A.meta->w0 = wd;
+                fill |= is_fill(wd);
+                ++o;
             }
-        rk += __shfl_sync(0xffffffffu, x, 31);
-    }
-    __syncwarp();
-    bool fill = false;
-    for (uint32_t k = lane; k < cnt; k += 32) {
-        const uint32_t h = W.hp[k];
-        const uint32_t pos = h & 0x3FFFFFFFu, c = h >> 30;
-        const uint32_t next = k + 1u < cnt ? (W.hp[k + 1] & 0x3FFFFFFFu) : nxt;
-        const uint32_t wd = run_word(c, next - pos, W.lv[k], false);
-        const uint32_t o = off + k;
-        A.out[o] = wd;
-        if ((o & 31u) == 0u) A.obp[o >> 5] = pos;
-        if (o == 0u) A.meta->w0 = wd;
-        fill |= is_fill(wd);
+        later = min(later, __shfl_sync(0xffffffffu, y, 0));
     }
     if (__any_sync(0xffffffffu, fill) && lane == 0) atomicOr(&A.meta->nfill, 1u);
 }

@@ -243,7 +243,13 @@ __global__ void __launch_bounds__(GTHREADS) k_gpack(GopArgs A) {
     const uint32_t sg = t / GSEG, nseg = (T + GSEG - 1) / GSEG;
     uint32_t off = 0;
     for (uint32_t i = lane; i < sg; i += 32) off += A.segs[i].x;
-    for (uint32_t i = sg * GSEG + lane; i < t; i += 32) off += A.tiles[i].x;
+    // the tiles before this one in its segment: at most GSEG / 32 per lane,
+    // loaded together
+#pragma unroll
+    for (uint32_t k = 0; k < GSEG / 32u; ++k) {
+        const uint32_t i = sg * GSEG + lane + 32u * k;
+        if (i < t) off += A.tiles[i].x;
+    }
     off = __reduce_add_sync(0xffffffffu, off);
     const uint32_t cnt = A.tiles[t].x;
     if (t == T - 1) {

@@ -191,6 +191,25 @@ int wahgpu_index_set_values(wahgpu_index* idx, int vtype, const void* values, ui
  * in compress() form. */
 int wahgpu_index_build(wahgpu_ctx* ctx, int kind, int vtype, const void* dev_values, uint64_t nrows,
                        uint32_t nbins, wahgpu_index** out);
+/* Index files.  wahgpu_index_read replaces relic::read(const char*) and
+ * bin::read(const char*) (src/irelic.cpp:690-786, src/ibin.cpp:468-540) for
+ * the .idx files relic::write / bin::write produce (src/irelic.cpp:354-642,
+ * src/ibin.cpp:5530-5834; index types RELIC and BINNING, 4- or 8-byte
+ * bitmap offsets): the file is read on the host and attached like a
+ * triple.  The raw column for bin edge checks still comes from
+ * wahgpu_index_set_values.  Errors: WAHGPU_EINVAL (cannot open or read),
+ * WAHGPU_EFORMAT (not such a file, or its offsets are inconsistent). */
+int wahgpu_index_read(wahgpu_ctx* ctx, const char* path, wahgpu_index** out);
+/* The same from a file image already in host memory (a mapped file). */
+int wahgpu_index_from_file_image(wahgpu_ctx* ctx, const void* data, uint64_t bytes, wahgpu_index** out);
+/* Host only, no device: the triple an index file image holds, in the layout
+ * wahgpu_index_from_triple takes (kind, nrows, keys, word offsets, bitmaps;
+ * a bitmap the writer left out stays zero words long).
+ * Sizes are always reported; the arrays are filled when all three are given
+ * (WAHGPU_ESIZE when a capacity is short).  Errors: wahgpu_last_error(NULL). */
+int wahgpu_idxfile_parse(const void* data, uint64_t bytes, int* kind, uint64_t* nrows, double* keys,
+                         uint64_t kcap, uint64_t* nkeys, int64_t* offsets, uint64_t ocap, uint64_t* noffsets,
+                         uint32_t* bitmaps, uint64_t bcap, uint64_t* nbitmaps);
 /* A copy of bitmap j as a bitvector (index::getBitvector, src/index.h). */
 int wahgpu_index_bitmap(wahgpu_index* idx, uint32_t j, wahgpu_bv** out);
 /* The index's keys in the triple's layout (relic: values; bin: minval then

@@ -21,6 +21,7 @@
 #define WAHGPU_HPP
 #include <cctype>
 #include <cstdint>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -275,6 +276,16 @@ protected:
     index(context& c, int kind, int vtype, const void* dev_values, uint64_t nrows, uint32_t nbins) : ctx_(&c) {
         ctx_->check(wahgpu_index_build(ctx_->get(), kind, vtype, dev_values, nrows, nbins, &h_));
     }
+    /* From a .idx file whose index type byte (header[5]) must be `type`. */
+    index(context& c, const char* f, int type) : ctx_(&c) {
+        char header[8] = {0};
+        std::FILE* fp = f ? std::fopen(f, "rb") : nullptr;
+        const bool ok = fp && std::fread(header, 1, 8, fp) == 8;
+        if (fp) std::fclose(fp);
+        if (!ok) throw error(WAHGPU_EINVAL, std::string("cannot read index file ") + (f ? f : "(null)"));
+        if (header[5] != type) throw error(WAHGPU_EFORMAT, std::string("index file of another type: ") + f);
+        ctx_->check(wahgpu_index_read(ctx_->get(), f, &h_));
+    }
     context* ctx_;
     wahgpu_index* h_ = nullptr;
 };
@@ -288,6 +299,9 @@ public:
     /* relic::construct over a column in device memory. */
     relic(int vtype, const void* dev_values, uint64_t nrows, context& c = context::standard())
         : index(c, WAHGPU_RELIC, vtype, dev_values, nrows, 0) {}
+    /* relic(col, f): the index file f written by relic::write
+     * (src/irelic.cpp:354, read 690). */
+    explicit relic(const char* f, context& c = context::standard()) : index(c, f, 7) {}
 };
 
 class bin : public index {
@@ -298,6 +312,9 @@ public:
     /* <binning nbins=N equal_weight/> over a column in device memory. */
     bin(int vtype, const void* dev_values, uint64_t nrows, uint32_t nbins, context& c = context::standard())
         : index(c, WAHGPU_BIN, vtype, dev_values, nrows, nbins) {}
+    /* bin(col, f): the index file f written by bin::write (src/ibin.cpp:5530,
+     * read 468); the raw column for edge checks comes from setValues. */
+    explicit bin(const char* f, context& c = context::standard()) : index(c, f, 0) {}
 };
 
 /* ibis::countQuery over named columns: a WHERE clause that is an AND of

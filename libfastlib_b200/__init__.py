@@ -104,6 +104,14 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
                                                     ctypes.c_uint64, ctypes.POINTER(ctypes.c_int64), ctypes.c_uint64,
                                                     U32P, ctypes.c_uint64, ctypes.POINTER(P)]),
         "wahgpu_index_set_values": (ctypes.c_int, [P, ctypes.c_int, P, ctypes.c_uint64]),
+        "wahgpu_index_read": (ctypes.c_int, [P, ctypes.c_char_p, ctypes.POINTER(P)]),
+        "wahgpu_index_from_file_image": (ctypes.c_int, [P, P, ctypes.c_uint64, ctypes.POINTER(P)]),
+        "wahgpu_idxfile_parse": (ctypes.c_int, [P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int),
+                                                ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_double),
+                                                ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64),
+                                                ctypes.POINTER(ctypes.c_int64), ctypes.c_uint64,
+                                                ctypes.POINTER(ctypes.c_uint64), U32P, ctypes.c_uint64,
+                                                ctypes.POINTER(ctypes.c_uint64)]),
         "wahgpu_index_free": (ctypes.c_int, [P]),
         "wahgpu_index_build": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, P, ctypes.c_uint64, ctypes.c_uint32,
                                               ctypes.POINTER(P)]),
@@ -351,6 +359,32 @@ class Index:
         ctx._live.add(self)
         return self
 
+    @classmethod
+    def read(cls, ctx: Context, path: str, values=None) -> "Index":
+        """A FastBit .idx file written by relic::write / bin::write."""
+        h = ctypes.c_void_p()
+        ctx.check(ctx.lib.wahgpu_index_read(ctx.h, os.fsencode(path), ctypes.byref(h)))
+        return cls._adopt(ctx, h, values)
+
+    @classmethod
+    def from_file_image(cls, ctx: Context, data: bytes, values=None) -> "Index":
+        """The same from the bytes of such a file already in host memory."""
+        buf = np.frombuffer(data, dtype=np.uint8)
+        h = ctypes.c_void_p()
+        ctx.check(ctx.lib.wahgpu_index_from_file_image(ctx.h, buf.ctypes.data_as(ctypes.c_void_p), len(buf),
+                                                       ctypes.byref(h)))
+        return cls._adopt(ctx, h, values)
+
+    @classmethod
+    def _adopt(cls, ctx, h, values):
+        self = cls.__new__(cls)
+        self.ctx, self.h = ctx, h
+        self.nrows = int(ctx.lib.wahgpu_index_nrows(h))
+        ctx._live.add(self)
+        if values is not None:
+            self.set_values(values)
+        return self
+
     def nbitmaps(self) -> int:
         return self.ctx.check(int(self.ctx.lib.wahgpu_index_nbitmaps(self.h)))
 
@@ -390,6 +424,29 @@ class Index:
             self.close()
         except Exception:
             pass
+
+
+def parse_index_file(data: bytes):
+    """Host only (no device): the (kind, nrows, keys, word offsets, bitmaps)
+    triple that a FastBit .idx file image holds, as the library reads it."""
+    lib = load_library()
+    buf = np.frombuffer(data, dtype=np.uint8)
+    kind, nrows = ctypes.c_int(), ctypes.c_uint64()
+    nk, no, nb = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+    ptr = buf.ctypes.data_as(ctypes.c_void_p)
+    rc = lib.wahgpu_idxfile_parse(ptr, len(buf), ctypes.byref(kind), ctypes.byref(nrows), None, 0, ctypes.byref(nk),
+                                  None, 0, ctypes.byref(no), None, 0, ctypes.byref(nb))
+    if rc < 0:
+        raise WahError(rc, (lib.wahgpu_last_error(None) or b"").decode())
+    keys = np.empty(nk.value, np.float64)
+    offs = np.empty(no.value, np.int64)
+    bms = np.empty(nb.value, np.uint32)
+    rc = lib.wahgpu_idxfile_parse(ptr, len(buf), None, None, keys.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                  len(keys), None, offs.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), len(offs),
+                                  None, bms.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), len(bms), None)
+    if rc < 0:
+        raise WahError(rc, (lib.wahgpu_last_error(None) or b"").decode())
+    return kind.value, nrows.value, keys, offs, bms
 
 
 def evaluate(ctx: Context, terms, want_rids: bool = True, want_hits: bool = False):

@@ -38,7 +38,7 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
            "-o", out, os.path.join(HERE, "csrc", "wah_api.cu"),
            os.path.join(HERE, "csrc", "wah_index.cu"), os.path.join(HERE, "csrc", "wah_build.cu"),
            os.path.join(HERE, "csrc", "wah_server.cu"),
-           os.path.join(HERE, "csrc", "wah_noalloc.cu")]
+           os.path.join(HERE, "csrc", "wah_noalloc.cu"), os.path.join(HERE, "csrc", "wah_idxfile.cu")]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

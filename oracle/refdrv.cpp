@@ -30,6 +30,13 @@
 //        per query osr(x >= lo) AND osr(x < hi), evaluate and
 //        get_coordinates (src/iapi.cpp:2062, 1285, 1383, 1517);
 //        reply: the triple like 5, then per query: status count nrids rids
+//  10 kind plen path[plen] nrows vals[nrows] nbins -> writes the index file
+//        the reference's own writer produces: kind 1 ibis::relic over the
+//        uint32 column (construct(array_t), irelic.cpp:879; write(".idx"),
+//        irelic.cpp:354-642), kind 2 ibis::bin over the column as float32
+//        through fastbit_iapi_build_index("<binning nbins=N equal_weight/>")
+//        and its triple (bin ctor, ibin.cpp:358; write, ibin.cpp:5530-5834);
+//        reply: status (0 ok)
 //   8 nthreads reps nops (op na a[na] nb b[nb])[nops] -> times the reference's
 //        operators: each of nthreads threads builds its own operand copies,
 //        then runs its share of the ops (round robin) reps times, each as
@@ -39,6 +46,7 @@
 #include "ibis.h"
 #include "irelic.h"
 #include "iapi.h"
+#include "ibin.h"
 #include "bitvector.h"
 #include <cstdio>
 #include <cstdlib>
@@ -48,6 +56,13 @@
 #include <time.h>
 
 static FILE *fin, *fout;
+
+// ibis::bin rebuilt from a triple; the index keeps its row count in a
+// protected member, which the ctor from a triple leaves 0 without a column
+struct BinFromTriple : public ibis::bin {
+    BinFromTriple(uint32_t nb, double* keys, int64_t* offs, uint32_t* bms, uint32_t rows)
+        : ibis::bin(0, nb, keys, offs, bms) { nrows = rows; }
+};
 static uint32_t rd32() { uint32_t v; if (fread(&v, 4, 1, fin) != 1) exit(3); return v; }
 static uint64_t rd64() { uint64_t v; if (fread(&v, 8, 1, fin) != 1) exit(3); return v; }
 static double rdf64() { double v; if (fread(&v, 8, 1, fin) != 1) exit(3); return v; }
@@ -242,6 +257,39 @@ int main(int argc, char** argv) {
             }
             delete [] keys; delete [] offs; delete [] bms;
             fastbit_iapi_free_all();
+        } else if (kind == 10) {
+            const uint32_t ik = rd32(), plen = rd32();
+            std::vector<char> path(plen + 1, 0);
+            if (plen && fread(&path[0], 1, plen, fin) != plen) exit(3);
+            const uint32_t nrows = rd32();
+            std::vector<uint32_t> raw(nrows);
+            for (uint32_t i = 0; i < nrows; ++i) raw[i] = rd32();
+            const uint32_t nbins = rd32();
+            int ierr = -1;
+            if (ik == 1) {
+                ibis::array_t<uint32_t> vals(nrows);
+                for (uint32_t i = 0; i < nrows; ++i) vals[i] = raw[i];
+                ibis::relic rel(0);
+                rel.construct(vals);
+                ierr = rel.write(&path[0]);
+            } else if (ik == 2) {
+                std::vector<float> vals(nrows);
+                for (uint32_t i = 0; i < nrows; ++i) memcpy(&vals[i], &raw[i], 4);
+                fastbit_iapi_register_array("x", FastBitDataTypeFloat, &vals[0], nrows);
+                char spec[128];
+                snprintf(spec, sizeof spec, "<binning nbins=%u equal_weight/>", nbins);
+                ierr = fastbit_iapi_build_index("x", spec);
+                double* keys = 0; int64_t* offs = 0; uint32_t* bms = 0;
+                uint64_t nk = 0, no = 0, nb = 0;
+                if (ierr >= 0) ierr = fastbit_iapi_deconstruct_index("x", &keys, &nk, &offs, &no, &bms, &nb);
+                if (ierr >= 0) {
+                    BinFromTriple b((uint32_t)(no - 1), keys, offs, bms, nrows);
+                    ierr = b.write(&path[0]);
+                }
+                delete [] keys; delete [] offs; delete [] bms;
+                fastbit_iapi_free_all();
+            }
+            wr32(ierr < 0 ? 1u : 0u);
         } else {
             fprintf(stderr, "refdrv: unknown request %u\n", kind);
             return 4;

@@ -99,5 +99,21 @@ int main(int argc, char** argv) {
     }
     cudaFree(da);
     cudaFree(db);
+    // 4. a relic read from its .idx file (argv[3]), and a bin file (argv[4])
+    //    refused as a relic
+    if (argc > 4) {
+        relic rf(argv[3]);
+        bitvector hits;
+        const long c = rf.evaluate(qContinuousRange(10, qContinuousRange::OP_LE, 30, qContinuousRange::OP_LT), hits);
+        wr(out, (uint64_t)c);
+        wrv(out, hits.rows());
+        int refused = 0;
+        try {
+            relic wrong(argv[4]);
+        } catch (const error& e) {
+            refused = e.code() == WAHGPU_EFORMAT ? 1 : 2;
+        }
+        wr(out, (uint64_t)refused);
+    }
     return 0;
 }

@@ -86,7 +86,9 @@ def test_cpp_shim(gpu_ctx):
         exe = _build(td)
         fi, fo = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
         open(fi, "wb").write(data)
-        subprocess.run([exe, fi, fo], check=True)
+        gold = os.path.join(ROOT, "tests", "golden")
+        subprocess.run([exe, fi, fo, os.path.join(gold, "relic_3001.idx"), os.path.join(gold, "bin_5000.idx")],
+                       check=True)
         R = _R(open(fo, "rb").read())
     for k, (op, ip, a, b, res, cnt) in enumerate(cases):
         assert np.array_equal(R.vec(), res), k
@@ -108,3 +110,9 @@ def test_cpp_shim(gpu_ctx):
     m = (fa >= 10) & (fa < 20)
     assert R.u64() == m.sum() and R.u64() == m.sum()
     assert np.array_equal(R.vec(), np.flatnonzero(m))
+    # relic read from the reference-written file; a bin file refused as relic
+    rv = load_golden("idxfile_inputs.npz")["relic_vals"].astype(np.float64)
+    m = (rv >= 10) & (rv < 30)
+    assert R.u64() == m.sum()
+    assert np.array_equal(R.vec(), np.flatnonzero(m))
+    assert R.u64() == 1

@@ -317,40 +317,60 @@ public:
     explicit bin(const char* f, context& c = context::standard()) : index(c, f, 0) {}
 };
 
-/* ibis::countQuery over named columns: a WHERE clause that is an AND of
- * range conditions — "a >= 3 and a < 10", "2.5 <= b < 7", "c between 1
- * and 4", "d = 5" — (the qContinuousRange leaves of countQuery::evaluate,
- * src/countQuery.cpp:953-1036). */
+/* ibis::countQuery over named columns.  A WHERE clause combines range
+ * conditions — "a >= 3", "2.5 <= b < 7", "c between 1 and 4", "d = 5",
+ * "d != 5" — with AND, OR, NOT (also &&, ||, !) and parentheses, as
+ * countQuery::doEvaluate does with its LOGICAL_AND / OR / NOT nodes over
+ * qContinuousRange leaves (src/countQuery.cpp:929-1036): an AND of ranges
+ * is one fused evaluation; other nodes combine the hit bitvectors of their
+ * children with the bitvector operators (OR |=, NOT flip()), on the device. */
 class countQuery {
 public:
     explicit countQuery(context& c = context::standard()) : ctx_(&c) {}
     void addColumn(const std::string& name, const index& idx) { cols_[lower(name)] = &idx; }
     /* setWhereClause(const char*) (src/countQuery.cpp:81); 0 on success, a
-     * negative code when the clause is not an AND of ranges on known
-     * columns. */
+     * negative code when the clause does not parse or names an unknown
+     * column. */
     int setWhereClause(const char* clause) {
+        nodes_.clear();
         terms_.clear();
+        root_ = -1;
         hits_ = -1;
         rows_.clear();
         try {
-            parse(clause ? clause : "");
+            Lexer L{clause ? clause : "", std::string(), false, 0.0};
+            while (L.next()) { toks_.push_back(L.tok); vals_.push_back(L.val); nums_.push_back(L.num); }
+            pos_ = 0;
+            root_ = parse_or();
+            if (pos_ != toks_.size()) throw error(WAHGPU_EINVAL, "unexpected '" + toks_[pos_] + "'");
         } catch (const error& e) {
-            terms_.clear();
+            nodes_.clear();
+            root_ = -1;
+            toks_.clear(); vals_.clear(); nums_.clear();
             return e.code();
         }
-        return terms_.empty() ? WAHGPU_EINVAL : 0;
+        toks_.clear(); vals_.clear(); nums_.clear();
+        // a plain AND of ranges keeps the fused single-launch path
+        if (!leaves_of_and(root_, terms_)) terms_.clear();
+        return 0;
     }
     /* evaluate() (src/countQuery.cpp:292); getNumHits (376); getHitRows
      * (387-410). */
     int evaluate() {
-        if (terms_.empty()) return WAHGPU_EINVAL;
-        // the count first, then the row ids into a buffer of that size
-        const int64_t n = ctx_->check(wahgpu_evaluate(ctx_->get(), terms_.data(), (uint32_t)terms_.size(),
-                                                      nullptr, 0, nullptr));
-        rows_.resize((size_t)n);
-        if (n) ctx_->check(wahgpu_evaluate(ctx_->get(), terms_.data(), (uint32_t)terms_.size(), rows_.data(),
-                                           rows_.size(), nullptr));
-        hits_ = n;
+        if (root_ < 0) return WAHGPU_EINVAL;
+        if (!terms_.empty()) {
+            // the count first, then the row ids into a buffer of that size
+            const int64_t n = ctx_->check(wahgpu_evaluate(ctx_->get(), terms_.data(), (uint32_t)terms_.size(),
+                                                          nullptr, 0, nullptr));
+            rows_.resize((size_t)n);
+            if (n) ctx_->check(wahgpu_evaluate(ctx_->get(), terms_.data(), (uint32_t)terms_.size(), rows_.data(),
+                                               rows_.size(), nullptr));
+            hits_ = n;
+            return 0;
+        }
+        bitvector h = eval(root_);
+        hits_ = (int64_t)h.cnt();
+        rows_ = h.rows();
         return 0;
     }
     long getNumHits() const { return (long)hits_; }
@@ -358,9 +378,16 @@ public:
         rids = rows_;
         return (long)rids.size();
     }
+    /* The range terms of a clause that is an AND of ranges (else empty). */
     const std::vector<wahgpu_term>& terms() const { return terms_; }
 
 private:
+    enum Kind { LEAF, AND, OR, NOT };
+    struct Node {
+        Kind kind;
+        wahgpu_term term;          // LEAF
+        std::vector<int> kids;     // AND, OR: two or more; NOT: one
+    };
     static std::string lower(std::string s) {
         for (char& ch : s) ch = (char)std::tolower((unsigned char)ch);
         return s;
@@ -386,7 +413,8 @@ private:
                 const char* s = p;
                 while (*p && (std::isalnum((unsigned char)*p) || *p == '_' || *p == '.')) ++p;
                 tok.assign(s, (size_t)(p - s));
-            } else if ((c == '<' || c == '>' || c == '=' || c == '!') && p[1] == '=') {
+            } else if (((c == '<' || c == '>' || c == '=' || c == '!') && p[1] == '=') ||
+                       (c == '&' && p[1] == '&') || (c == '|' && p[1] == '|')) {
                 tok.assign(p, 2);
                 p += 2;
             } else {
@@ -401,70 +429,136 @@ private:
         if (it == cols_.end()) throw error(WAHGPU_EINVAL, "unknown column " + name);
         return it->second;
     }
-    void add(const index* idx, int lop, double lo, int rop, double hi) {
-        wahgpu_term t;
-        t.idx = idx->handle(); t.lop = lop; t.lo = lo; t.rop = rop; t.hi = hi;
-        terms_.push_back(t);
+    int leaf(const index* idx, int lop, double lo, int rop, double hi) {
+        Node n{LEAF, wahgpu_term(), {}};
+        n.term.idx = idx->handle(); n.term.lop = lop; n.term.lo = lo; n.term.rop = rop; n.term.hi = hi;
+        nodes_.push_back(n);
+        return (int)nodes_.size() - 1;
     }
-    // one condition: name op num | num op name [op num] | name between a and b
-    void parse(const char* s) {
-        Lexer L{s, std::string(), false, 0.0};
-        std::vector<std::string> toks;
-        std::vector<double> vals;
-        std::vector<bool> nums;
-        while (L.next()) { toks.push_back(L.tok); vals.push_back(L.val); nums.push_back(L.num); }
-        size_t i = 0;
-        auto is_cmp = [&](size_t k) {
-            return k < toks.size() && (toks[k] == "<" || toks[k] == "<=" || toks[k] == ">" || toks[k] == ">=" ||
-                                       toks[k] == "=" || toks[k] == "==");
-        };
-        while (i < toks.size()) {
-            if (!nums[i] && i + 1 < toks.size() && lower(toks[i + 1]) == "between") {
-                if (i + 4 >= toks.size() || !nums[i + 2] || lower(toks[i + 3]) != "and" || !nums[i + 4])
-                    throw error(WAHGPU_EINVAL, "bad BETWEEN");
-                add(column(toks[i]), WAHGPU_CMP_LE, vals[i + 2], WAHGPU_CMP_LE, vals[i + 4]);
-                i += 5;
-            } else if (!nums[i] && is_cmp(i + 1) && i + 2 < toks.size() && nums[i + 2]) {
-                const std::string& op = toks[i + 1];
-                const double v = vals[i + 2];
-                const index* c = column(toks[i]);
-                if (op == "<") add(c, WAHGPU_CMP_NONE, 0, WAHGPU_CMP_LT, v);
-                else if (op == "<=") add(c, WAHGPU_CMP_NONE, 0, WAHGPU_CMP_LE, v);
-                else if (op == ">") add(c, WAHGPU_CMP_LT, v, WAHGPU_CMP_NONE, 0);
-                else if (op == ">=") add(c, WAHGPU_CMP_LE, v, WAHGPU_CMP_NONE, 0);
-                else add(c, WAHGPU_CMP_LE, v, WAHGPU_CMP_LE, v);
-                i += 3;
-            } else if (nums[i] && is_cmp(i + 1) && i + 2 < toks.size() && !nums[i + 2]) {
-                const std::string& op = toks[i + 1];
-                const double v = vals[i];
-                const index* c = column(toks[i + 2]);
-                int lop = WAHGPU_CMP_LE, rop = WAHGPU_CMP_NONE;
-                double hi = 0;
-                if (op == "<") lop = WAHGPU_CMP_LT;
-                else if (op == "<=") lop = WAHGPU_CMP_LE;
-                else if (op == ">") { lop = WAHGPU_CMP_NONE; rop = WAHGPU_CMP_LT; hi = v; }
-                else if (op == ">=") { lop = WAHGPU_CMP_NONE; rop = WAHGPU_CMP_LE; hi = v; }
-                else { rop = WAHGPU_CMP_LE; hi = v; }
-                i += 3;
-                if ((op == "<" || op == "<=") && is_cmp(i) && i + 1 < toks.size() && nums[i + 1] &&
-                    (toks[i] == "<" || toks[i] == "<=")) {
-                    rop = toks[i] == "<" ? WAHGPU_CMP_LT : WAHGPU_CMP_LE;
-                    hi = vals[i + 1];
-                    i += 2;
-                }
-                add(c, lop, lop == WAHGPU_CMP_NONE ? 0 : v, rop, hi);
-            } else {
-                throw error(WAHGPU_EINVAL, "not a range condition near '" + toks[i] + "'");
-            }
-            if (i < toks.size()) {
-                if (lower(toks[i]) != "and") throw error(WAHGPU_EINVAL, "only AND of ranges is supported");
-                ++i;
-            }
+    int inner(Kind k, std::vector<int> kids) {
+        nodes_.push_back(Node{k, wahgpu_term(), std::move(kids)});
+        return (int)nodes_.size() - 1;
+    }
+    bool at(const char* w) const { return pos_ < toks_.size() && lower(toks_[pos_]) == w; }
+    bool is_cmp(size_t k) const {
+        return k < toks_.size() && (toks_[k] == "<" || toks_[k] == "<=" || toks_[k] == ">" || toks_[k] == ">=" ||
+                                    toks_[k] == "=" || toks_[k] == "==" || toks_[k] == "!=");
+    }
+    int parse_or() {
+        std::vector<int> kids{parse_and()};
+        while (at("or") || at("||")) { ++pos_; kids.push_back(parse_and()); }
+        return kids.size() == 1 ? kids[0] : inner(OR, kids);
+    }
+    int parse_and() {
+        std::vector<int> kids{parse_unary()};
+        while (at("and") || at("&&")) { ++pos_; kids.push_back(parse_unary()); }
+        return kids.size() == 1 ? kids[0] : inner(AND, kids);
+    }
+    int parse_unary() {
+        if (at("not") || at("!")) { ++pos_; return inner(NOT, {parse_unary()}); }
+        if (at("(")) {
+            ++pos_;
+            const int e = parse_or();
+            if (!at(")")) throw error(WAHGPU_EINVAL, "missing ')'");
+            ++pos_;
+            return e;
         }
+        return parse_condition();
+    }
+    // name op num | num op name [op num] | name between a and b
+    int parse_condition() {
+        const size_t i = pos_;
+        const auto& T = toks_;
+        if (i >= T.size()) throw error(WAHGPU_EINVAL, "missing condition");
+        if (!nums_[i] && i + 1 < T.size() && lower(T[i + 1]) == "between") {
+            if (i + 4 >= T.size() || !nums_[i + 2] || lower(T[i + 3]) != "and" || !nums_[i + 4])
+                throw error(WAHGPU_EINVAL, "bad BETWEEN");
+            pos_ = i + 5;
+            return leaf(column(T[i]), WAHGPU_CMP_LE, vals_[i + 2], WAHGPU_CMP_LE, vals_[i + 4]);
+        }
+        if (!nums_[i] && is_cmp(i + 1) && i + 2 < T.size() && nums_[i + 2]) {
+            const std::string& op = T[i + 1];
+            const double v = vals_[i + 2];
+            const index* c = column(T[i]);
+            pos_ = i + 3;
+            if (op == "<") return leaf(c, WAHGPU_CMP_NONE, 0, WAHGPU_CMP_LT, v);
+            if (op == "<=") return leaf(c, WAHGPU_CMP_NONE, 0, WAHGPU_CMP_LE, v);
+            if (op == ">") return leaf(c, WAHGPU_CMP_LT, v, WAHGPU_CMP_NONE, 0);
+            if (op == ">=") return leaf(c, WAHGPU_CMP_LE, v, WAHGPU_CMP_NONE, 0);
+            const int eq = leaf(c, WAHGPU_CMP_LE, v, WAHGPU_CMP_LE, v);
+            return op == "!=" ? inner(NOT, {eq}) : eq;
+        }
+        if (nums_[i] && is_cmp(i + 1) && T[i + 1] != "!=" && i + 2 < T.size() && !nums_[i + 2]) {
+            const std::string& op = T[i + 1];
+            const double v = vals_[i];
+            const index* c = column(T[i + 2]);
+            int lop = WAHGPU_CMP_LE, rop = WAHGPU_CMP_NONE;
+            double hi = 0;
+            if (op == "<") lop = WAHGPU_CMP_LT;
+            else if (op == "<=") lop = WAHGPU_CMP_LE;
+            else if (op == ">") { lop = WAHGPU_CMP_NONE; rop = WAHGPU_CMP_LT; hi = v; }
+            else if (op == ">=") { lop = WAHGPU_CMP_NONE; rop = WAHGPU_CMP_LE; hi = v; }
+            else { rop = WAHGPU_CMP_LE; hi = v; }
+            pos_ = i + 3;
+            if ((op == "<" || op == "<=") && pos_ + 1 < T.size() && nums_[pos_ + 1] &&
+                (T[pos_] == "<" || T[pos_] == "<=")) {
+                rop = T[pos_] == "<" ? WAHGPU_CMP_LT : WAHGPU_CMP_LE;
+                hi = vals_[pos_ + 1];
+                pos_ += 2;
+            }
+            return leaf(c, lop, lop == WAHGPU_CMP_NONE ? 0 : v, rop, hi);
+        }
+        throw error(WAHGPU_EINVAL, "not a range condition near '" + T[i] + "'");
+    }
+    // the terms of a node that is a leaf or an AND of leaves
+    bool leaves_of_and(int n, std::vector<wahgpu_term>& out) const {
+        const Node& x = nodes_[(size_t)n];
+        if (x.kind == LEAF) { out.push_back(x.term); return true; }
+        if (x.kind != AND) return false;
+        for (int k : x.kids)
+            if (nodes_[(size_t)k].kind != LEAF) { out.clear(); return false; }
+        for (int k : x.kids) out.push_back(nodes_[(size_t)k].term);
+        return true;
+    }
+    bitvector eval_terms(const std::vector<wahgpu_term>& t) {
+        wahgpu_bv* h = nullptr;
+        ctx_->check(wahgpu_evaluate(ctx_->get(), t.data(), (uint32_t)t.size(), nullptr, 0, &h));
+        return bitvector::adopt(h, *ctx_);
+    }
+    bitvector eval(int n) {
+        const Node& x = nodes_[(size_t)n];
+        if (x.kind == LEAF) return eval_terms({x.term});
+        if (x.kind == NOT) {
+            bitvector h = eval(x.kids[0]);
+            h.flip();
+            return h;
+        }
+        if (x.kind == AND) {
+            // the range leaves of the AND in one fused evaluation
+            std::vector<wahgpu_term> t;
+            for (int k : x.kids)
+                if (nodes_[(size_t)k].kind == LEAF) t.push_back(nodes_[(size_t)k].term);
+            std::vector<bitvector> parts;
+            if (!t.empty()) parts.push_back(eval_terms(t));
+            for (int k : x.kids)
+                if (nodes_[(size_t)k].kind != LEAF) parts.push_back(eval(k));
+            bitvector acc = std::move(parts[0]);
+            for (size_t k = 1; k < parts.size(); ++k) acc &= parts[k];
+            return acc;
+        }
+        bitvector acc = eval(x.kids[0]);
+        for (size_t k = 1; k < x.kids.size(); ++k) acc |= eval(x.kids[k]);
+        return acc;
     }
 
     context* ctx_;
     std::map<std::string, const index*> cols_;
+    std::vector<Node> nodes_;
+    int root_ = -1;
+    std::vector<std::string> toks_;
+    std::vector<double> vals_;
+    std::vector<bool> nums_;
+    size_t pos_ = 0;
     std::vector<wahgpu_term> terms_;
     std::vector<uint32_t> rows_;
     int64_t hits_ = -1;

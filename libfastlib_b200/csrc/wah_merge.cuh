@@ -27,8 +27,14 @@
 
 namespace wah {
 
-constexpr int MERGE_THREADS = 512;
-constexpr int TILE_BLOCKS = 128;                              // bpos entries per tile
+#ifndef WAH_MERGE_THREADS
+#define WAH_MERGE_THREADS 256
+#endif
+#ifndef WAH_MERGE_TILE_BLOCKS
+#define WAH_MERGE_TILE_BLOCKS 64
+#endif
+constexpr int MERGE_THREADS = WAH_MERGE_THREADS;
+constexpr int TILE_BLOCKS = WAH_MERGE_TILE_BLOCKS;             // bpos entries per tile
 constexpr int TILE_WORDS = 32 * (TILE_BLOCKS + 2);            // max words held per operand
 // events per thread: a tile holds at most TILE_WORDS words of both operands together
 constexpr int SEG_PER_THREAD = (TILE_WORDS + MERGE_THREADS - 1) / MERGE_THREADS;

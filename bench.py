@@ -53,11 +53,10 @@ def peaks():
 
 def make_operands(rank: int, device: str):
     from libfastlib_b200 import workloads as W
+    from libfastlib_b200.replicas import operand_seeds
     ops = []
-    for i, d in enumerate(DENSITIES):
-        a = W.raw_wah_operand(1000 * rank + 2 * i + 1, NBITS, d, device)
-        b = W.raw_wah_operand(1000 * rank + 2 * i + 2, NBITS, d, device)
-        ops.append((a, b))
+    for d, (sa, sb) in zip(DENSITIES, operand_seeds(rank, len(DENSITIES))):
+        ops.append((W.raw_wah_operand(sa, NBITS, d, device), W.raw_wah_operand(sb, NBITS, d, device)))
     return ops
 
 
@@ -249,6 +248,7 @@ def main():
     import torch
     import torch.distributed as dist
     import libfastlib_b200 as L
+    from libfastlib_b200.replicas import max_over_ranks, whole_job_rate
 
     if args.only_range:
         run_only_range(args)
@@ -320,13 +320,10 @@ def main():
     # kernels per step were counted while capturing; replays launch the same set
     launches = (ctx.launches - l0) + args.steps * launches_per_step
     clocks = clk.stop()
-    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(e0.elapsed_time(e1), f"cuda:{local}")
     if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
-    value = world * nbytes * args.steps / (ms / 1e3) / 1e9
+    value = whole_job_rate(nbytes, args.steps, ms, world)
     if args.only:
         if rank == 0:
             print(json.dumps({"only": args.only, "value": value, "unit": "GB/s", "ms_per_call": ms / args.steps,
@@ -418,12 +415,8 @@ def main():
         h2d, d2h = e2e_step()
     q1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = max(q0.elapsed_time(q1), (time.perf_counter() - t0) * 1e3)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * nbytes * args.e2e_steps / (e2e_ms / 1e3) / 1e9
+    e2e_ms = max_over_ranks(max(q0.elapsed_time(q1), (time.perf_counter() - t0) * 1e3), f"cuda:{local}")
+    e2e_value = whole_job_rate(nbytes, args.e2e_steps, e2e_ms, world)
 
     cpu = None
     if rank == 0 and world == 1:

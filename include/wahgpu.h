@@ -13,6 +13,11 @@
  * 2283-2313, write(array_t<word_t>&)): the whole 32-bit WAH words of m_vec,
  * then the active word's value if it holds any bits, then the active word's
  * bit count.  Row ids are uint32 positions, ascending.
+ *
+ * A context belongs to one device (wahgpu_ctx_create makes it current);
+ * like the CUDA runtime's own libraries, its calls run on the calling
+ * thread's current device, so a process that drives several GPUs makes the
+ * context's device current (cudaSetDevice) before calling into it.
  */
 #ifndef WAHGPU_H
 #define WAHGPU_H

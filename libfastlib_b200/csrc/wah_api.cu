@@ -486,13 +486,9 @@ static int wg_gtile(wahgpu_bv* b) {
 
 template <int OP, int TG, int NCW>
 static void launch_dense_op(const wahgpu_ctx* ctx, uint32_t ntiles, cudaStream_t s, const DenseArgs& a) {
-    static int per_sm = 0;
+    static PerDeviceSetup setup;
     const size_t sm = sizeof(DShared<TG, NCW>);
-    if (!per_sm) {
-        cudaFuncSetAttribute(k_dense<OP, TG, NCW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense<OP, TG, NCW>, (NCW + 1) * 32, sm);
-        if (per_sm < 1) per_sm = 1;
-    }
+    const int per_sm = wg_kernel_setup(setup, ctx->device, k_dense<OP, TG, NCW>, (NCW + 1) * 32, sm);
     // persistent: at most one wave of resident CTAs
     const uint32_t grid = std::min<uint32_t>(ntiles, (uint32_t)(per_sm * ctx->sm_count));
     k_dense<OP, TG, NCW><<<grid, (NCW + 1) * 32, sm, s>>>(a);
@@ -572,14 +568,11 @@ int wg_launch_gop(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t 
     if (!rc) {
         const uint32_t grid = (ntiles + GWARPS - 1) / GWARPS;
         const size_t sm_op = GWARPS * sizeof(GopWarp);
-        static bool attrs = false;
-        if (!attrs) {
-            cudaFuncSetAttribute(k_gop<OP_AND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_op);
-            cudaFuncSetAttribute(k_gop<OP_OR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_op);
-            cudaFuncSetAttribute(k_gop<OP_XOR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_op);
-            cudaFuncSetAttribute(k_gop<OP_MINUS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_op);
-            attrs = true;
-        }
+        static PerDeviceSetup setup[4];
+        wg_kernel_setup(setup[0], ctx->device, k_gop<OP_AND>, GTHREADS, sm_op);
+        wg_kernel_setup(setup[1], ctx->device, k_gop<OP_OR>, GTHREADS, sm_op);
+        wg_kernel_setup(setup[2], ctx->device, k_gop<OP_XOR>, GTHREADS, sm_op);
+        wg_kernel_setup(setup[3], ctx->device, k_gop<OP_MINUS>, GTHREADS, sm_op);
         switch (op) {
         case OP_AND: k_gop<OP_AND><<<grid, GTHREADS, sm_op, s>>>(a); break;
         case OP_OR: k_gop<OP_OR><<<grid, GTHREADS, sm_op, s>>>(a); break;

@@ -2,6 +2,7 @@
 #ifndef WAH_API_INTERNAL_H
 #define WAH_API_INTERNAL_H
 #include <cuda_runtime.h>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <string>
@@ -44,6 +45,24 @@ struct wahgpu_bv {
     bool compressed_form = false;  // words are as compress() leaves them
 };
 
+// A kernel's launch setup on each device (the dynamic shared-memory limit is
+// a per-device setting): resident CTAs per SM once set up, 0 before.
+struct PerDeviceSetup {
+    std::atomic<int> per_sm[64];
+};
+// Sets the kernel's dynamic shared-memory limit on the current device the
+// first time it launches there; returns its resident CTAs per SM.
+template <class Kernel>
+int wg_kernel_setup(PerDeviceSetup& s, int device, Kernel k, int threads, size_t smem) {
+    const int d = device >= 0 && device < 64 ? device : 0;
+    int v = s.per_sm[d].load(std::memory_order_relaxed);
+    if (v) return v;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k, threads, smem);
+    if (v < 1) v = 1;
+    s.per_sm[d].store(v, std::memory_order_relaxed);
+    return v;
+}
 int wg_fail(wahgpu_ctx* ctx, int code, const char* fmt, ...);
 void* wg_alloc(wahgpu_ctx* ctx, size_t bytes);
 void wg_free(wahgpu_ctx* ctx, void* p);

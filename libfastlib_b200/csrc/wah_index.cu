@@ -441,13 +441,9 @@ extern "C" int wahgpu_batch_run(wahgpu_batch* B) {
         }
         if (B->d_dense) CUDA_TRY(ctx, cudaMemsetAsync(B->d_dense, 0, ((size_t)B->groups + 1) * 4, ctx->stream));
     }
-    static int per_sm = 0;
+    static PerDeviceSetup setup;
     const size_t sm = sizeof(RangeShared);
-    if (!per_sm) {
-        cudaFuncSetAttribute(k_range, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_range, RTHREADS, sm);
-        if (per_sm < 1) per_sm = 1;
-    }
+    const int per_sm = wg_kernel_setup(setup, ctx->device, k_range, RTHREADS, sm);
     const uint32_t ctas = ctx->range_ctas ? std::min<uint32_t>(ctx->range_ctas, (uint32_t)per_sm) : (uint32_t)per_sm;
     const uint32_t grid = std::min<uint32_t>(nitems, ctas * (uint32_t)ctx->sm_count);
     if (two_pass) {

@@ -119,7 +119,9 @@ const uint32_t* wahgpu_bv_device_words(wahgpu_bv* bv);
  * the words equal the reference's operator output after compress()
  * (src/bitvector.cpp:1194-1838, kernels 2419-4079, compress 378-469).
  * For inplace the result is also returned in *res (a is not modified: the
- * device keeps operands immutable).
+ * device keeps operands immutable).  Operands of different sizes are handled
+ * as the reference does: the shorter one is padded with 0 bits (adjustSize,
+ * src/bitvector.cpp:4086) and the operator runs in its OP= form.
  *
  * Operands whose every word covers one 31-bit group while some word is a
  * fill (a count-1 fill word) make the reference take its uncompressed loops

@@ -639,6 +639,98 @@ static bool dense_two_pass(const wahgpu_ctx* ctx) {
     return ctx->dense_engine == 0 || ctx->dense_engine == 3;
 }
 
+// adjustSize(0, nt) of a copy of b (src/bitvector.cpp:4086-4108): the copy
+// grows by appendFill(0, nt - size()) (src/bitvector.h:800-831), whose
+// append_active / append_counter (699-760) may merge into b's last word, so
+// the copy keeps b's words up to the last one and the rest is rebuilt here.
+static int padded_copy(wahgpu_ctx* ctx, wahgpu_bv* b, uint64_t nt, wahgpu_bv** out) {
+    *out = nullptr;
+    const uint32_t n = b->h.n;
+    std::vector<uint32_t> t;  // b's last word, then the appended words
+    if (n) {
+        uint32_t last = 0;
+        CUDA_TRY(ctx, cudaMemcpyAsync(&last, b->words + n - 1, 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        t.push_back(last);
+    }
+    // append_active of a literal (bitvector.h:699-737)
+    auto push_active = [&](uint32_t v) {
+        if (t.empty()) { t.push_back(v); return; }
+        uint32_t& bk = t.back();
+        if (v == 0) {
+            if (bk == 0) bk = HEADER0 + 2;
+            else if (bk >= HEADER0 && bk < HEADER1) ++bk;
+            else t.push_back(v);
+        } else if (v == ALLONES) {
+            if (bk == ALLONES) bk = HEADER1 | 2;
+            else if (bk >= HEADER1) ++bk;
+            else t.push_back(v);
+        } else {
+            t.push_back(v);
+        }
+    };
+    // append_counter(0, cnt) (bitvector.h:741-760)
+    auto push_zeros = [&](uint32_t cnt) {
+        const uint32_t w = HEADER0 + cnt;
+        if (t.empty()) { t.push_back(w); return; }
+        uint32_t& bk = t.back();
+        if ((bk >> 30) == 2u) bk += cnt;
+        else if (bk == 0) bk = w + 1;
+        else t.push_back(w);
+    };
+    uint32_t anb = b->h.anb, aval = b->h.aval;
+    uint64_t need = nt - ((uint64_t)b->h.groups * MAXBITS + anb);
+    if (anb > 0) {
+        const uint32_t k = (uint32_t)std::min<uint64_t>(MAXBITS - anb, need);
+        anb += k;
+        aval <<= k;
+        need -= k;
+        if (anb >= MAXBITS) { push_active(aval); anb = 0; aval = 0; }
+    }
+    if (need >= MAXBITS) {
+        const uint64_t cnt = need / MAXBITS;
+        if (cnt > MAXCNT) return wg_fail(ctx, WAHGPU_ERANGE, "padding of %llu groups", (unsigned long long)cnt);
+        if (cnt > 1) push_zeros((uint32_t)cnt);
+        else push_active(0);
+        need -= cnt * MAXBITS;
+    }
+    if (need > 0) { anb = (uint32_t)need; aval = 0; }
+    const uint32_t keep = n ? n - 1 : 0;
+    const uint64_t m = (uint64_t)keep + t.size();
+    wahgpu_bv* p = wg_bv_new(ctx);
+    if (!p) return wg_fail(ctx, WAHGPU_ENOMEM, "allocation failed");
+    int rc = bv_reserve(p, m);
+    if (!rc && keep && cudaMemcpyAsync(p->words, b->words, (size_t)keep * 4, cudaMemcpyDeviceToDevice, ctx->stream))
+        rc = wg_fail(ctx, WAHGPU_ECUDA, "copy failed");
+    if (!rc && !t.empty() && (cudaMemcpyAsync(p->words + keep, t.data(), t.size() * 4, cudaMemcpyHostToDevice,
+                                              ctx->stream) || cudaStreamSynchronize(ctx->stream)))
+        rc = wg_fail(ctx, WAHGPU_ECUDA, "copy failed");
+    if (!rc) rc = wg_scan_meta(p, (uint32_t)m, anb, aval);
+    if (!rc) rc = wg_bv_meta(p);
+    if (rc) { wahgpu_bv_free(p); return rc; }
+    *out = p;
+    return WAHGPU_OK;
+}
+
+// Operands of different sizes (src/bitvector.cpp:1194-1838): the shorter
+// one is padded with 0 bits and the operator runs in its OP= form — for
+// a OP b with a longer a: res = b padded, res OP= a (& | ^) or res = a,
+// res -= b padded (-); with a shorter a: res = a padded, res OP= b; for
+// a OP= b: a OP= (b padded), or (a padded) OP= b.
+static int binop_unequal(wahgpu_ctx* ctx, int op, bool inplace, wahgpu_bv* a, wahgpu_bv* b, wahgpu_bv* res) {
+    const uint64_t sa = (uint64_t)a->h.groups * MAXBITS + a->h.anb;
+    const uint64_t sb = (uint64_t)b->h.groups * MAXBITS + b->h.anb;
+    wahgpu_bv* pad = nullptr;
+    int rc = padded_copy(ctx, sa > sb ? b : a, sa > sb ? sa : sb, &pad);
+    if (rc) return rc;
+    if (sa < sb) rc = wahgpu_bv_binop_into(ctx, op, 1, pad, b, res);
+    else if (inplace || op == OP_MINUS) rc = wahgpu_bv_binop_into(ctx, op, 1, a, pad, res);
+    else rc = wahgpu_bv_binop_into(ctx, op, 1, pad, a, res);
+    cudaStreamSynchronize(ctx->stream);
+    wahgpu_bv_free(pad);
+    return rc;
+}
+
 extern "C" int wahgpu_bv_binop_into(wahgpu_ctx* ctx, int op, int inplace, wahgpu_bv* a, wahgpu_bv* b,
                                     wahgpu_bv* res) {
     if (!ctx || !a || !b || !res || op < 0 || op > 3) return wg_fail(ctx, WAHGPU_EINVAL, "bad argument");
@@ -649,9 +741,23 @@ extern "C" int wahgpu_bv_binop_into(wahgpu_ctx* ctx, int op, int inplace, wahgpu
     if (rc) return rc;
     OperandMeta ma = effective(opmeta(a)), mb = effective(opmeta(b));
     Plan p = plan_binop(op, inplace != 0, ma, mb);
-    if (p.kind == PK_UNEQUAL)
-        return wg_fail(ctx, WAHGPU_EINVAL, "operands of different sizes (%llu, %llu bits) are not supported",
-                       (unsigned long long)a->h.groups * 31 + a->h.anb, (unsigned long long)b->h.groups * 31 + b->h.anb);
+    if (p.kind == PK_UNEQUAL) {
+        // pad the operands the reference would hold (an all-0 one collapsed
+        // by do_cnt, src/bitvector.cpp:601-604)
+        wahgpu_bv* ea = a;
+        wahgpu_bv* eb = b;
+        wahgpu_bv* ta = nullptr;
+        wahgpu_bv* tb = nullptr;
+        if (ma.n != a->h.n) { rc = collapsed_copy(ctx, a, &ta); if (rc) return rc; ea = ta; }
+        if (mb.n != b->h.n) { rc = collapsed_copy(ctx, b, &tb); if (rc) { if (ta) wahgpu_bv_free(ta); return rc; } eb = tb; }
+        rc = binop_unequal(ctx, op, inplace != 0, ea, eb, res);
+        if (ta || tb) {
+            cudaStreamSynchronize(ctx->stream);
+            if (ta) wahgpu_bv_free(ta);
+            if (tb) wahgpu_bv_free(tb);
+        }
+        return rc;
+    }
     const uint32_t G = ma.groups;
     if (G >= 2 && ((ma.n == G && a->h.nfill && ma.n == a->h.n) || (mb.n == G && b->h.nfill && mb.n == b->h.n)))
         return wg_fail(ctx, WAHGPU_EDEGENERATE,

@@ -12,6 +12,10 @@ Outputs (all seeded, compressed .npz):
   binop_geom.npz    appendFill-built 2^20-bit operands with alternating
                     geometric 0/1 runs at densities 1e-4..0.5 (the raw-WAH
                     workload at reduced length), all ops, both forms
+  binop_unequal.npz 400 operand pairs of DIFFERENT sizes (the shorter one is
+                    padded by adjustSize inside the reference's operators),
+                    some ending in a literal 0, a 0-fill or a 1-fill, the
+                    four operators in both forms: reference words and cnt()
   unary.npz         compress(), decompress(), flip() and the indexSet row
                     ids of random bitvectors
   relic_small.npz   relic index over 20000 uint32 values in [0,100) and 40
@@ -51,10 +55,43 @@ def unpack(flat, offs, i):
     return flat[offs[i]:offs[i + 1]]
 
 
+def unequal(td):
+    """Pairs of different sizes, every operator in both forms."""
+    rng = np.random.default_rng(404)
+    styles = ["mixed", "short", "sparse", "canon", "dense"]
+    A, B, ops, inpl = [], [], [], []
+    while len(A) < 400:
+        k = len(A)
+        wa = G.random_words(rng, int(rng.integers(1, 3000)), styles[k % 5])
+        wb = G.random_words(rng, int(rng.integers(1, 3000)), styles[(k + 2) % 5])
+        if k % 6 == 1:
+            wa = list(wa[:-1]) + [0]
+        if k % 6 == 2:
+            wb = list(wb) + [G.fill(0, 5)]
+        if k % 6 == 3:
+            wa = list(wa) + [G.fill(1, 3)]
+        a = G.serialize(wa, int(rng.integers(0, 31)), int(rng.integers(0, 1 << 31)))
+        b = G.serialize(wb, int(rng.integers(0, 31)), int(rng.integers(0, 1 << 31)))
+        if G.groups_of(wa) == G.groups_of(wb) or oracle.is_degenerate(a) or oracle.is_degenerate(b):
+            continue
+        A.append(a); B.append(b)
+        ops.append(int(rng.integers(0, 4))); inpl.append(int(rng.integers(0, 2)))
+    R = G.run_refdrv(oracle.REFDRV, [G.req_binop(o, i, 1, a, b) for o, i, a, b in zip(ops, inpl, A, B)], td)
+    res, cnt, st = [], [], []
+    for _ in A:
+        s, c, w = R.bv()
+        st.append(s); cnt.append(c); res.append(w)
+    fa, oa = pack(A); fb, ob = pack(B); fr, orr = pack(res)
+    np.savez_compressed(os.path.join(HERE, "binop_unequal.npz"), a=fa, a_off=oa, b=fb, b_off=ob,
+                        res=fr, res_off=orr, cnt=np.array(cnt, np.uint64), status=np.array(st, np.uint32),
+                        op=np.array(ops, np.int32), inplace=np.array(inpl, np.int32))
+
+
 def main():
     if not oracle.build_reference():
         sys.exit("the reference library could not be built (needs the reference sources)")
     td = tempfile.mkdtemp()
+    unequal(td)
 
     # ---- random operand pairs
     rng = np.random.default_rng(20241203)

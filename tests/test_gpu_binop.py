@@ -275,3 +275,44 @@ def test_word_space_engine_same_words(gpu_ctx, density):
         _full_size(gpu_ctx, density)
     finally:
         gpu_ctx.set_tuning(L.TUNE_DENSE_ENGINE, 0)
+
+
+def test_unequal_sizes_golden(gpu_ctx):
+    """Operands of different sizes against the reference's own answers."""
+    g = load_golden("binop_unequal.npz")
+    for i in range(len(g["op"])):
+        a, b = unpack(g, "a", i), unpack(g, "b", i)
+        w, c = _bin(gpu_ctx, int(g["op"][i]), a, b, int(g["inplace"][i]))
+        assert c == int(g["cnt"][i]) and np.array_equal(w, unpack(g, "res", i)), i
+
+
+def test_unequal_sizes(gpu_ctx):
+    """Operands of different sizes: the shorter one is padded with 0 bits
+    (adjustSize) and the operator runs in the OP= form, as the reference
+    does; tails that end in a literal 0, a 0-fill, a 1-fill or active bits
+    exercise the merges of the padding."""
+    rng = np.random.default_rng(405)
+    styles = ["mixed", "short", "sparse", "canon", "dense"]
+    checked = 0
+    for trial in range(60):
+        ga = int(rng.integers(1, 3000))
+        gb = int(rng.integers(1, 3000))
+        wa = G.random_words(rng, ga, styles[trial % 5])
+        wb = G.random_words(rng, gb, styles[(trial + 2) % 5])
+        if trial % 6 == 1:
+            wa = list(wa[:-1]) + [0]               # ends in a literal 0
+        if trial % 6 == 2:
+            wb = list(wb) + [G.fill(0, 5)]         # ends in a 0-fill
+        if trial % 6 == 3:
+            wa = list(wa) + [G.fill(1, 3)]         # ends in a 1-fill
+        a = G.serialize(wa, int(rng.integers(0, 31)), int(rng.integers(0, 1 << 31)))
+        b = G.serialize(wb, int(rng.integers(0, 31)), int(rng.integers(0, 1 << 31)))
+        if oracle.is_degenerate(a) or oracle.is_degenerate(b):
+            continue
+        for op in range(4):
+            for ip in (0, 1):
+                ref, rc = oracle.binop(op, a, b, inplace=bool(ip))
+                w, c = _bin(gpu_ctx, op, a, b, ip)
+                assert c == rc and np.array_equal(w, ref), (trial, op, ip, len(a), len(b))
+                checked += 1
+    assert checked > 300

@@ -21,6 +21,17 @@ def test_binop_random_word_exact():
     assert bad == 0
 
 
+def test_binop_unequal_sizes_word_exact():
+    """Operands of different sizes: the padding inside the reference's
+    operators (adjustSize) restated by the oracle."""
+    g = load_golden("binop_unequal.npz")
+    assert len(g["op"]) == 400
+    for i in range(len(g["op"])):
+        assert g["status"][i] == 0
+        w, c = oracle.binop(int(g["op"][i]), unpack(g, "a", i), unpack(g, "b", i), inplace=bool(g["inplace"][i]))
+        assert c == int(g["cnt"][i]) and np.array_equal(w, unpack(g, "res", i)), i
+
+
 def test_binop_geometric_word_exact():
     g = load_golden("binop_geom.npz")
     for k, (di, op, ip) in enumerate(g["case"]):

@@ -225,6 +225,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-threads", type=int, default=4,
+                    help="host threads (one context each) sharing the end-to-end leg's calls")
     ap.add_argument("--dense-tile", type=int, default=2048, choices=[1024, 2048, 4096],
                     help="groups per tile of the dense-path kernel")
     ap.add_argument("--dense-engine", type=int, default=0, choices=[0, 1, 2, 3],
@@ -380,29 +382,53 @@ def main():
         except Exception:
             traffic = None
 
-    # end to end through the C ABI with host (pinned) buffers
+    # end to end through the C ABI with host (pinned) buffers: the step's
+    # calls are shared by E2E_THREADS host threads, each with its own
+    # context (stream), as a multi-threaded caller would use the library, so
+    # one call's upload overlaps another's readback and kernels
+    import ctypes
     pinned = []
     for a, b in pairs:
         ta = torch.from_numpy(a).pin_memory()
         tb = torch.from_numpy(b).pin_memory()
         pinned.append((ta.numpy(), tb.numpy(), ta, tb))
-    outbufs = [torch.empty(len(a) + len(b) + 4, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
-               for a, b in pairs]
+    ectx = [ctx] + [L.Context(local) for _ in range(args.e2e_threads - 1)]
+    for c in ectx[1:]:
+        c.set_tuning(L.TUNE_DENSE_TILE, args.dense_tile)
+        c.set_tuning(L.TUNE_DENSE_ENGINE, args.dense_engine)
+    outbufs = [[torch.empty(len(a) + len(b) + 4, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+                for a, b in pairs] for _ in ectx]
+    calls = [(op, i) for op in OPS for i in range(len(pinned))]
 
-    def e2e_step():
-        h2d = d2h = 0
-        for op in OPS:
-            for i, (a, b, _ta, _tb) in enumerate(pinned):
-                A = ctx.bitvector(a)
-                B = ctx.bitvector(b)
+    def e2e_calls(k, out):
+        c, h2d, d2h = ectx[k], 0, 0
+        try:
+            for op, i in calls[k::len(ectx)]:
+                a, b = pinned[i][0], pinned[i][1]
+                A = c.bitvector(a)
+                B = c.bitvector(b)
                 R = A._binop(op, B, False)
-                n = ctx.check(ctx.lib.wahgpu_bv_write(R.h, outbufs[i].ctypes.data_as(
-                    __import__("ctypes").POINTER(__import__("ctypes").c_uint32)), len(outbufs[i])))
+                buf = outbufs[k][i]
+                n = c.check(c.lib.wahgpu_bv_write(R.h, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), len(buf)))
                 R.cnt()
                 h2d += 4 * (len(a) + len(b))
                 d2h += 4 * n
                 del A, B, R
-        return h2d, d2h
+            out[k] = (h2d, d2h)
+        except BaseException as e:  # surfaced by the caller
+            out[k] = e
+
+    def e2e_step():
+        out = [None] * len(ectx)
+        ts = [threading.Thread(target=e2e_calls, args=(k, out)) for k in range(len(ectx))]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        for r in out:
+            if isinstance(r, BaseException):
+                raise r
+        return sum(r[0] for r in out), sum(r[1] for r in out)
 
     e2e_step()
     torch.cuda.synchronize()
@@ -454,7 +480,8 @@ def main():
                          "traffic_source": f"profiles/{traffic_file} (ncu dram__bytes_read.sum + "
                                            "dram__bytes_write.sum per operator call)"},
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h, "host_threads": len(ectx),
+                    "timing": "wall clock around the calls, device synchronized, max over ranks"},
             "cpu_baseline": cpu,
             "clocks": clocks,
             "gpu_launches": launches,

@@ -15,14 +15,19 @@
 // OR order (a heap ordered by pointer values) changes only the words of its
 // intermediate results, never the bits.
 //
-// Work item = (query, tile of RT groups), claimed in order.  For each term
-// the warps of the CTA OR the covered bitmaps' words for the tile into a
-// shared-memory accumulator (bitmap b goes to warp b % warps; each warp walks
-// its bitmap's words 32 at a time, positions by ballot / scan), the edge bins'
-// rows are checked against the raw column, and the term result is AND'ed
-// into the query result.  Hit counts and row ids follow; row-id positions come
-// from one decoupled look-back over the items in claim order, so each query's
-// ids are contiguous and ascending.
+// Work item = (query, tile of RT groups), claimed in query-major order
+// (row ids by a decoupled look-back in claim order, so each query's ids are
+// contiguous and ascending), tile-major order (the queries of a batch share
+// each tile's words in L2; counts only, or two passes around a scan of the
+// items' hits for row ids).  For each term, warp 0 stages the term and its
+// index in shared memory; a span covering whole blocks of the index's
+// cumulative rows starts as C(k1) & ~C(k0) read as 16-byte vectors, and the
+// remaining bitmaps (the edges of such a span, a short span, or the tile's
+// list of bitmaps holding a 1 bit in it) form one job list with the edge
+// bins' row checks: each warp walks a bitmap's words for the tile 128 at a
+// time (positions by ballot / scan) into a shared-memory accumulator.  The
+// term result is AND'ed into the query result; a tile whose AND is empty
+// skips the query's remaining terms.
 #ifndef WAH_RANGE_CUH
 #define WAH_RANGE_CUH
 #include "wah_dev.cuh"

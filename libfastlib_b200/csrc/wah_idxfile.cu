@@ -92,13 +92,13 @@ const char* parse(const void* data, uint64_t bytes, Triple& t) {
     std::vector<uint64_t> off(nobs + 1ull);
     for (uint64_t i = 0; i <= nobs; ++i) {
         if (osz == 4) {
-            int32_t v;
-            get(p, bytes, offpos + 4 * i, v);
+            int32_t v = 0;
+            if (!get(p, bytes, offpos + 4 * i, v)) return "truncated bitmap offsets";
             if (v < 0) return "negative bitmap offset";
             off[i] = (uint64_t)v;
         } else {
-            int64_t v;
-            get(p, bytes, offpos + 8 * i, v);
+            int64_t v = 0;
+            if (!get(p, bytes, offpos + 8 * i, v)) return "truncated bitmap offsets";
             if (v < 0) return "negative bitmap offset";
             off[i] = (uint64_t)v;
         }

@@ -1,6 +1,7 @@
 """WHERE clauses over named columns (the Python face of ibis::countQuery,
 src/countQuery.cpp:81-410): range conditions — ``a >= 3``, ``2.5 <= b < 7``,
-``c between 1 and 4``, ``d = 5``, ``d != 5`` — combined with AND, OR, NOT
+``c between 1 and 4``, ``d = 5``, ``d != 5``, ``e in (1, 4, 9)`` (a
+qDiscreteRange, evaluated as an OR of equalities) — combined with AND, OR, NOT
 (also ``&&``, ``||``, ``!``) and parentheses, as countQuery::doEvaluate
 combines qContinuousRange leaves (src/countQuery.cpp:929-1036).
 
@@ -19,7 +20,7 @@ from . import AND, CMP_LE, CMP_LT, OR, evaluate
 
 _TOKEN = re.compile(r"\s*(?:(?P<num>[-+]?(?:\d+\.?\d*|\.\d+)(?:[eE][-+]?\d+)?)"
                     r"|(?P<name>[A-Za-z_][A-Za-z0-9_.]*)"
-                    r"|(?P<op><=|>=|==|!=|&&|\|\||[<>=()!]))")
+                    r"|(?P<op><=|>=|==|!=|&&|\|\||[<>=()!,]))")
 
 
 class QueryError(ValueError):
@@ -105,6 +106,23 @@ class _Parser:
         def val(k):
             return t[k][1] if k < len(t) else None
 
+        if (kind(i) == "name" and kind(i + 1) == "name" and str(val(i + 1)).lower() == "in"
+                and kind(i + 2) == "op" and val(i + 2) == "("):
+            # x in (v1, v2, ...): qDiscreteRange as an OR of equalities
+            idx, k, vals = self._col(val(i)), i + 3, []
+            while True:
+                if kind(k) != "num":
+                    raise QueryError("bad IN list")
+                vals.append(val(k))
+                if kind(k + 1) == "op" and val(k + 1) == ",":
+                    k += 2
+                    continue
+                if kind(k + 1) == "op" and val(k + 1) == ")":
+                    break
+                raise QueryError("bad IN list")
+            self.i = k + 2
+            leaves = [("leaf", idx.term(v, v, lop=CMP_LE, rop=CMP_LE)) for v in vals]
+            return leaves[0] if len(leaves) == 1 else ("or", leaves)
         if kind(i) == "name" and kind(i + 1) == "name" and str(val(i + 1)).lower() == "between":
             if kind(i + 2) != "num" or str(val(i + 3)).lower() != "and" or kind(i + 4) != "num":
                 raise QueryError("bad BETWEEN")

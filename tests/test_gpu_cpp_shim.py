@@ -73,7 +73,8 @@ def test_cpp_shim(gpu_ctx):
     clauses = ["a >= 10 and a < 20", "a between 5 and 7 and b < 0.5", "0.25 <= b < 1.5", "b > -0.3 and a = 42",
                "A <= 3", "a < 50 and b >= 0 and a > 40", "c < 3", "a < 5 or b < -1", "not a < 50",
                "a != 42 and b < 0", "(a < 10 or a >= 90) and not (b between -0.5 and 0.5)", "!(a >= 3) || b > 2",
-               "a < 5 or", "(a < 3", "a < 20 and (b < -1 or b > 1) and a >= 10"]
+               "a < 5 or", "(a < 3", "a < 20 and (b < -1 or b > 1) and a >= 10", "a in (3, 17, 42) or b > 2.5",
+               "a in (3, 17"]
     data = struct.pack("<I", len(cases))
     for op, ip, a, b, _, _ in cases:
         data += struct.pack("<II", op, ip) + _u32v(a) + _u32v(b)
@@ -102,7 +103,8 @@ def test_cpp_shim(gpu_ctx):
     want = [(fa >= 10) & (fa < 20), (fa >= 5) & (fa <= 7) & (fb < 0.5), (fb >= 0.25) & (fb < 1.5),
             (fb > -0.3) & (fa == 42), fa <= 3, (fa < 50) & (fb >= 0) & (fa > 40), None, (fa < 5) | (fb < -1),
             ~(fa < 50), (fa != 42) & (fb < 0), ((fa < 10) | (fa >= 90)) & ~((fb >= -0.5) & (fb <= 0.5)),
-            ~(fa >= 3) | (fb > 2), None, None, (fa < 20) & ((fb < -1) | (fb > 1)) & (fa >= 10)]
+            ~(fa >= 3) | (fb > 2), None, None, (fa < 20) & ((fb < -1) | (fb > 1)) & (fa >= 10),
+            np.isin(fa, [3, 17, 42]) | (fb > 2.5), None]
     for c, m in zip(clauses, want):
         rc = struct.unpack("<q", struct.pack("<Q", R.u64()))[0]
         if m is None:

@@ -27,6 +27,7 @@ def test_where_equals_scan(gpu_ctx):
         ("!(a >= 3) || b > 2", ~(fa >= 3) | (fb > 2)),
         ("a < 20 and (b < -1 or b > 1) and a >= 10", (fa < 20) & ((fb < -1) | (fb > 1)) & (fa >= 10)),
         ("90 <= a", fa >= 90),
+        ("a in (3, 17, 42) and b > 0", np.isin(fa, [3, 17, 42]) & (fb > 0)),
     ]
     for clause, m in cases:
         cnt, rows = where(gpu_ctx, clause, cols)

@@ -31,6 +31,11 @@ def leaf(*t):
     ("a < 1 or b > -0.5 and not a <= 9",
      ("or", [leaf("a", CMP_NONE, None, CMP_LT, 1.0),
              ("and", [leaf("b", CMP_LT, -0.5, CMP_NONE, None), ("not", leaf("a", CMP_NONE, None, CMP_LE, 9.0))])])),
+    ("a in (3, 5.5, 7)", ("or", [leaf("a", CMP_LE, 3.0, CMP_LE, 3.0), leaf("a", CMP_LE, 5.5, CMP_LE, 5.5),
+                                  leaf("a", CMP_LE, 7.0, CMP_LE, 7.0)])),
+    ("b in (2) and not a in (1, 2)",
+     ("and", [leaf("b", CMP_LE, 2.0, CMP_LE, 2.0),
+              ("not", ("or", [leaf("a", CMP_LE, 1.0, CMP_LE, 1.0), leaf("a", CMP_LE, 2.0, CMP_LE, 2.0)]))])),
     ("!(a >= 3) || (b < 1 && a > 2)",
      ("or", [("not", leaf("a", CMP_LE, 3.0, CMP_NONE, None)),
              ("and", [leaf("b", CMP_NONE, None, CMP_LT, 1.0), leaf("a", CMP_LT, 2.0, CMP_NONE, None)])])),
@@ -39,7 +44,8 @@ def test_trees(clause, tree):
     assert parse(clause, COLS) == tree
 
 
-@pytest.mark.parametrize("clause", ["c < 3", "a < 5 or", "(a < 3", "a between 1 4", "a <", "a < 3 b < 4", "a @ 3"])
+@pytest.mark.parametrize("clause", ["c < 3", "a < 5 or", "(a < 3", "a between 1 4", "a <", "a < 3 b < 4", "a @ 3",
+                                    "a in (1, 2", "a in ()", "a in (1 2)"])
 def test_refused(clause):
     with pytest.raises(QueryError):
         parse(clause, COLS)

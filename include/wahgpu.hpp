@@ -125,6 +125,26 @@ public:
         release();
         upload(w.data(), w.size());
     }
+    /* adjustSize(nv, nt) (src/bitvector.cpp:4086-4108) when it grows the
+     * vector: bits up to position nv become 1, the rest up to nt become 0,
+     * through appendFill as in the reference.  Shrinking is not supported. */
+    void adjustSize(uint32_t nv, uint32_t nt) {
+        const uint64_t sz = size();
+        if (nt == sz) return;
+        if (nt < sz) throw error(WAHGPU_EINVAL, "adjustSize cannot shrink a vector here");
+        if (nv > nt) nv = nt;
+        if (nv > sz) {
+            appendFill(1, (uint32_t)(nv - sz));
+            if (nt > nv) appendFill(0, nt - nv);
+        } else {
+            appendFill(0, (uint32_t)(nt - sz));
+        }
+    }
+    /* count(mask) (src/bitvector.h:1089-1124): the 1 bits of *this & mask. */
+    uint64_t count(const bitvector& mask) const {
+        std::unique_ptr<bitvector> r(*this & mask);
+        return r->cnt();
+    }
     void setBit(uint32_t i, int val) {
         const uint64_t n = size();
         if (i < n) throw error(WAHGPU_EINVAL, "setBit inside the vector is not supported; append in row order");

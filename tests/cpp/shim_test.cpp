@@ -61,6 +61,11 @@ int main(int argc, char** argv) {
         b.write(w);
         wrv(out, w);
         wrv(out, b.rows());
+        // adjustSize: 45 more 0 bits; count(mask) of the vector with itself
+        b.adjustSize(0, nbits + 45);
+        b.write(w);
+        wrv(out, w);
+        wr(out, b.count(b));
     }
     // 3. countQuery over two device-built indexes
     const uint32_t n = rd(in);

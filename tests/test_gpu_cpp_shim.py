@@ -99,6 +99,8 @@ def test_cpp_shim(gpu_ctx):
     for nbits, rows in builds:
         assert np.array_equal(R.vec(), canonical_words(rows, nbits)), nbits
         assert np.array_equal(R.vec(), rows), nbits
+        assert np.array_equal(R.vec(), canonical_words(rows, nbits + 45)), nbits
+        assert R.u64() == len(rows), nbits
     fa, fb = ca.astype(np.float64), cb.astype(np.float64)
     want = [(fa >= 10) & (fa < 20), (fa >= 5) & (fa <= 7) & (fb < 0.5), (fb >= 0.25) & (fb < 1.5),
             (fb > -0.3) & (fa == 42), fa <= 3, (fa < 50) & (fb >= 0) & (fa > 40), None, (fa < 5) | (fb < -1),

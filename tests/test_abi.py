@@ -57,3 +57,37 @@ def test_cpp_header_compiles():
         open(src, "w").write('#define WAHGPU_AS_IBIS\n#include "wahgpu.hpp"\nint main() { return 0; }\n')
         subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-fsyntax-only",
                         "-I" + os.path.join(root, "include"), src], check=True)
+
+
+def test_null_handles_are_refused():
+    """Every handle-taking entry point answers a NULL handle with a negative
+    status (no device needed, nothing dereferenced)."""
+    import libfastlib_b200 as L
+    lib = L.load_library()
+    calls = [
+        lambda: lib.wahgpu_bv_binop(None, 0, 0, None, None, None),
+        lambda: lib.wahgpu_bv_binop_into(None, 0, 0, None, None, None),
+        lambda: lib.wahgpu_bv_cnt(None),
+        lambda: lib.wahgpu_bv_size(None),
+        lambda: lib.wahgpu_bv_write(None, None, 0),
+        lambda: lib.wahgpu_bv_compress(None),
+        lambda: lib.wahgpu_bv_flip(None),
+        lambda: lib.wahgpu_bv_rids(None, None, 0),
+        lambda: lib.wahgpu_bv_free(None),
+        lambda: lib.wahgpu_bv_from_serial(None, None, 0, None),
+        lambda: lib.wahgpu_index_read(None, None, None),
+        lambda: lib.wahgpu_index_from_file_image(None, None, 0, None),
+        lambda: lib.wahgpu_index_from_triple(None, 1, 0, None, 0, None, 0, None, 0, None),
+        lambda: lib.wahgpu_index_free(None),
+        lambda: lib.wahgpu_index_nbitmaps(None),
+        lambda: lib.wahgpu_evaluate(None, None, 0, None, 0, None),
+        lambda: lib.wahgpu_batch_create(None, None, None, 0, 0, 0, None),
+        lambda: lib.wahgpu_batch_run(None),
+        lambda: lib.wahgpu_batch_free(None),
+        lambda: lib.wahgpu_ctx_set_tuning(None, 1, 1024),
+        lambda: lib.wahgpu_ctx_destroy(None),
+        lambda: lib.wahgpu_server_free(None),
+        lambda: lib.wahgpu_idxfile_parse(None, 0, None, None, None, 0, None, None, 0, None, None, 0, None),
+    ]
+    for k, f in enumerate(calls):
+        assert f() < 0, k

@@ -105,6 +105,12 @@ const char* parse(const void* data, uint64_t bytes, Triple& t) {
     }
     if (off[0] != first) return "first bitmap offset does not follow the keys";
     if (off[nobs] > bytes) return "bitmaps run past the end of the file";
+    // the whole table before any copy: every offset inside the file and
+    // none smaller than the one before it
+    for (uint64_t i = 0; i < nobs; ++i) {
+        if (off[i + 1] < off[i]) return "bitmap offsets decrease";
+        if (off[i + 1] > bytes) return "bitmaps run past the end of the file";
+    }
     t.nrows = nrows;
     t.keys = a;
     t.keys.insert(t.keys.end(), b.begin(), b.end());

@@ -101,3 +101,14 @@ def test_malformed_files_are_rejected(defect):
     with pytest.raises(L.WahError) as e:
         L.parse_index_file(bytes(img))
     assert e.value.code == -5  # WAHGPU_EFORMAT
+
+
+def test_offset_table_checked_before_any_copy():
+    """A middle offset past the end of the file, with the last one inside
+    it (offsets [first, bytes + 4096, bytes]): the parser rejects the table
+    before it copies a bitmap, instead of reading past the image."""
+    img = bytearray(_relic_image(62, [1.0, 2.0], [[0x80000002, 0], [0x80000002, 0]]))
+    struct.pack_into("<i", img, 44, len(img) + 4096)
+    with pytest.raises(L.WahError) as e:
+        L.parse_index_file(bytes(img))
+    assert e.value.code == -5

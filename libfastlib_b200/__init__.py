@@ -52,7 +52,7 @@ RELIC, BIN = 1, 2
 TUNE_DENSE_TILE = 1
 TUNE_RANGE_ORDER = 2
 TUNE_RANGE_CTAS = 3
-TUNE_DENSE_ENGINE = 4  # 0 auto (= 3), 1 pipelined group space, 2 word space, 3 two-pass group space
+TUNE_DENSE_ENGINE = 4  # 0 auto (= 4), 1 pipelined group space, 2 word space, 3 two-pass group space, 4 single-pass group space
 TUNE_CUM_STRIDE = 5
 DENSE_TILES = (1024, 2048, 4096)
 CMP_NONE, CMP_LT, CMP_LE = 0, 1, 2

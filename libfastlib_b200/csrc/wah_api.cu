@@ -5,6 +5,7 @@
 #include "wah_merge.cuh"
 #include "wah_kernels.cuh"
 #include "wah_gop.cuh"
+#include "wah_fuse.cuh"
 #include "wah_api_internal.h"
 
 #include <cuda_runtime.h>
@@ -166,7 +167,7 @@ extern "C" int wahgpu_ctx_set_tuning(wahgpu_ctx* ctx, int key, int64_t value) {
         ctx->dense_tile = (uint32_t)value;
         return WAHGPU_OK;
     case WAHGPU_TUNE_DENSE_ENGINE:
-        if (value < 0 || value > 3) return wg_fail(ctx, WAHGPU_EINVAL, "dense engine must be 0, 1, 2 or 3");
+        if (value < 0 || value > 4) return wg_fail(ctx, WAHGPU_EINVAL, "dense engine must be 0, 1, 2, 3 or 4");
         ctx->dense_engine = (uint32_t)value;
         return WAHGPU_OK;
     case WAHGPU_TUNE_RANGE_ORDER:
@@ -318,7 +319,13 @@ extern "C" int wahgpu_bv_from_device_serial(wahgpu_ctx* ctx, const uint32_t* dev
     if (!b) return wg_fail(ctx, WAHGPU_ENOMEM, "allocation failed");
     int rc = bv_reserve(b, n);
     if (rc) { wahgpu_bv_free(b); return rc; }
-    if (n) CUDA_TRY(ctx, cudaMemcpyAsync(b->words, dev_words, (size_t)n * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (n) {
+        const cudaError_t e = cudaMemcpyAsync(b->words, dev_words, (size_t)n * 4, cudaMemcpyDeviceToDevice, ctx->stream);
+        if (e != cudaSuccess) {
+            wahgpu_bv_free(b);
+            return wg_fail(ctx, WAHGPU_ECUDA, "device copy failed: %s", cudaGetErrorString(e));
+        }
+    }
     rc = wg_scan_meta(b, n, anb, aval);
     if (rc) { wahgpu_bv_free(b); return rc; }
     b->compressed_form = false;
@@ -595,6 +602,54 @@ int wg_launch_gop(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t 
     return WAHGPU_OK;
 }
 
+// Single-pass group-space engine (wah_fuse.cuh): one launch per call,
+// operands read once, words written once.  Needs 16-byte-aligned word arrays
+// (every block of the allocator is); the two-pass engine runs otherwise.
+static bool fuse_applies(const wahgpu_bv* x, const wahgpu_bv* y, const wahgpu_bv* res, uint32_t groups) {
+    auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+    return groups > 0 && al(x->words) && al(y->words) && al(res->words);
+}
+template <int OP>
+static void launch_fuse_op(const wahgpu_ctx* ctx, uint32_t ntiles, cudaStream_t s, const FuseArgs& a) {
+    static PerDeviceSetup setup;
+    wg_kernel_setup(setup, ctx->device, k_gfuse<OP>, FTHREADS, 0);
+    k_gfuse<OP><<<ntiles, FTHREADS, 0, s>>>(a);
+}
+int wg_launch_fuse(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t groups,
+                   uint32_t anb, uint32_t aval, wahgpu_bv* res) {
+    int rc = bv_reserve(res, (uint64_t)x->h.n + y->h.n);
+    if (rc) return rc;
+    if (!fuse_applies(x, y, res, groups)) return wg_launch_gop(ctx, op, x, y, groups, anb, aval, res);
+    rc = wg_gtile(x);
+    if (rc) return rc;
+    rc = wg_gtile(y);
+    if (rc) return rc;
+    const uint32_t ntiles = (groups + FT - 1) / FT;
+    TileRec* recs; LaunchSync* sync;
+    rc = wg_scratch(ctx, ntiles, &recs, &sync);
+    if (rc) return rc;
+    FuseArgs a;
+    a.xw = x->words; a.xgt = x->gt; a.nx = x->h.n;
+    a.yw = y->words; a.ygt = y->gt; a.ny = y->h.n;
+    a.groups = groups; a.ntiles = ntiles;
+    a.out = res->words; a.obp = res->bpos; a.meta = res->meta; a.cap = res->cap;
+    a.recs = recs; a.sync = sync;
+    a.aval = aval; a.anb = anb;
+    CUDA_TRY(ctx, cudaMemsetAsync(res->meta, 0, sizeof(DevMeta), ctx->stream));
+    switch (op) {
+    case OP_AND: launch_fuse_op<OP_AND>(ctx, ntiles, ctx->stream, a); break;
+    case OP_OR: launch_fuse_op<OP_OR>(ctx, ntiles, ctx->stream, a); break;
+    case OP_XOR: launch_fuse_op<OP_XOR>(ctx, ntiles, ctx->stream, a); break;
+    default: launch_fuse_op<OP_MINUS>(ctx, ntiles, ctx->stream, a); break;
+    }
+    ctx->launches++;
+    CUDA_TRY(ctx, cudaGetLastError());
+    res->h_valid = false;
+    res->gt_valid = false;
+    res->compressed_form = true;
+    return WAHGPU_OK;
+}
+
 // A one-word device bitvector holding the collapsed form of an all-zero
 // operand (do_cnt(), src/bitvector.cpp:601-604).
 static int collapsed_copy(wahgpu_ctx* ctx, const wahgpu_bv* src, wahgpu_bv** out) {
@@ -630,13 +685,16 @@ static OperandMeta opmeta(const wahgpu_bv* b) {
 
 // Engine for a canonical-result operator (WAHGPU_TUNE_DENSE_ENGINE): 1 the
 // pipelined group-space kernel, 2 the word-space merge, 3 the two-pass
-// group-space kernels; 0 (default) the two-pass kernels, measured fastest
-// on the raw-WAH workload.
+// group-space kernels, 4 the single-pass group-space kernel; 0 (default)
+// the single-pass kernel.
 static bool dense_in_word_space(const wahgpu_ctx* ctx, const wahgpu_bv*, const wahgpu_bv*, uint32_t) {
     return ctx->dense_engine == 2;
 }
 static bool dense_two_pass(const wahgpu_ctx* ctx) {
-    return ctx->dense_engine == 0 || ctx->dense_engine == 3;
+    return ctx->dense_engine == 3;
+}
+static bool dense_fused(const wahgpu_ctx* ctx) {
+    return ctx->dense_engine == 0 || ctx->dense_engine == 4;
 }
 
 // adjustSize(0, nt) of a copy of b (src/bitvector.cpp:4086-4108): the copy
@@ -780,6 +838,8 @@ extern "C" int wahgpu_bv_binop_into(wahgpu_ctx* ctx, int op, int inplace, wahgpu
         // (no step states) when the tuning asks for it
         if (dense_in_word_space(ctx, ca, cb, G))
             rc = wg_launch_merge(ctx, op, false, false, false, ca, cb, G, anb, aval, res);
+        else if (dense_fused(ctx))
+            rc = wg_launch_fuse(ctx, op, ca, cb, G, anb, aval, res);
         else if (dense_two_pass(ctx))
             rc = wg_launch_gop(ctx, op, ca, cb, G, anb, aval, res);
         else

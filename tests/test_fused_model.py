@@ -1,0 +1,238 @@
+"""A CPU model of the single-pass group-space engine (libfastlib_b200/csrc/
+wah_fuse.cuh: k_gfuse) checked against the oracle.  It follows the kernel
+thread by thread: the word slots loaded from the 16-byte boundary below each
+tile's first word, the clipped word lengths and their packed (16-bit halves)
+block scan, the painting of patterns into the transposed group arrays, the
+group phase's heads and popcount with the group before each thread, the
+{heads, last head, ones} scan and look-back, and the write phase in which
+the next head writes a uniform run's word (deferred across tiles) and the
+last tile the final run.  Every shared-memory and global index is asserted
+in range, so a change to that arithmetic can be tried here before it runs
+on a GPU."""
+import numpy as np
+import pytest
+
+import oracle
+from oracle import wahgen as G
+
+ALL, H0, H1, MAXC = 0x7FFFFFFF, 0x80000000, 0xC0000000, 0x3FFFFFFF
+DT = 1024
+FT, FWARPS, FWPT, FGPT = 2048, 9, 8, 8
+FTHREADS, FGTHREADS, FROWS = FWARPS * 32, FT // FGPT, FT // FGPT
+C_ZERO, C_ONE, C_MIXED = 0, 1, 2
+
+
+def wgroups(w):
+    return (w & MAXC) if w > ALL else 1
+
+
+def wpattern(w):
+    return (ALL if w >= H1 else 0) if w > ALL else w
+
+
+def cls_of(v):
+    return C_ZERO if v == 0 else (C_ONE if v == ALL else C_MIXED)
+
+
+def op2(op, a, b):
+    return [a & b, a | b, a ^ b, a & ~b & ALL][op]
+
+
+def fidx(q):
+    assert 0 <= q < FT
+    return (q % FGPT) * FROWS + q // FGPT
+
+
+def gtile(w, groups):
+    starts = np.concatenate([[0], np.cumsum([wgroups(int(x)) for x in w])]).astype(np.int64)
+    nt = (groups + DT - 1) // DT
+    out = []
+    for k in range(nt + 1):
+        g = k * DT
+        if g >= groups:
+            out.append((len(w), groups))
+        else:
+            i = int(np.searchsorted(starts, g, side="right") - 1)
+            out.append((i, int(starts[i])))
+    return out
+
+
+def fuse_range(gt, n, g0, g1):
+    wi0, s0 = gt[g0 // DT]
+    wi1, s1 = gt[(g1 + DT - 1) // DT]
+    wend = wi1 + 1 if (wi1 < n and s1 < g1) else wi1
+    nw = wend - wi0
+    assert wi0 < n and wend <= n and wend > wi0 and nw <= FT and s0 <= g0 and not (g0 > 0 and s0 == g0 and wi0 == 0)
+    return wi0, s0, nw
+
+
+def fuse_len(w, k, wi0, nw, s0, g0, g1):
+    if k < wi0 or k - wi0 >= nw:
+        return 0
+    c = wgroups(w)
+    if k == wi0:
+        c = min(s0 + c, g1) - g0
+    return min(c, FT)
+
+
+def run_word(c, ln):
+    return ((H1 if c else H0) | ln) if ln >= 2 else (ALL if c else 0)
+
+
+def model(op, xw, yw, groups):
+    """The words k_gfuse writes, and the popcount of m_vec."""
+    xw = [int(v) for v in xw]
+    yw = [int(v) for v in yw]
+    nx, ny = len(xw), len(yw)
+    gx, gy = gtile(xw, groups), gtile(yw, groups)
+    ntiles = (groups + FT - 1) // FT
+    cap = nx + ny
+    out = [None] * cap
+    recs = []  # inclusive prefix per tile (the look-back result)
+    for t in range(ntiles):
+        g0 = t * FT
+        g1 = min(g0 + FT, groups)
+        ng = g1 - g0
+        xi0, xs0, xn = fuse_range(gx, nx, g0, g1)
+        yi0, ys0, yn = fuse_range(gy, ny, g0, g1)
+        pat = [[None] * FT, [None] * FT]
+        run = 0
+        for tid in range(FTHREADS):
+            kx = (xi0 & ~3) + tid * FWPT
+            ky = (yi0 & ~3) + tid * FWPT
+            for j in range(FWPT):
+                wxv = xw[kx + j] if kx + j < xi0 + xn else 0
+                wyv = yw[ky + j] if ky + j < yi0 + yn else 0
+                packed = fuse_len(wxv, kx + j, xi0, xn, xs0, g0, g1) | (fuse_len(wyv, ky + j, yi0, yn, ys0, g0, g1) << 16)
+                ex = run
+                run += packed
+                assert (run & 0xFFFF) <= 2 * FT and (run >> 16) <= 2 * FT
+                for o, (w, ln, q) in enumerate(((wxv, packed & 0xFFFF, ex & 0xFFFF), (wyv, packed >> 16, ex >> 16))):
+                    if ln and q < ng:
+                        for e in range(min(ln, ng - q)):
+                            pat[o][fidx(q + e)] = wpattern(w)
+        for q in range(ng):
+            assert pat[0][fidx(q)] is not None and pat[1][fidx(q)] is not None, (t, q)
+        thr = []
+        for tid in range(FGTHREADS):
+            q0 = tid * FGPT
+            if tid > 0:
+                pr = op2(op, pat[0][fidx(q0 - 1)] or 0, pat[1][fidx(q0 - 1)] or 0)
+            elif g0 > 0:
+                pr = op2(op, wpattern(xw[xi0 if xs0 < g0 else xi0 - 1]), wpattern(yw[yi0 if ys0 < g0 else yi0 - 1]))
+            else:
+                pr = 0
+            pc = cls_of(pr)
+            hm, ones, lasth, r = 0, 0, 0, []
+            for e in range(FGPT):
+                q = q0 + e
+                inr = q < ng
+                rv = op2(op, pat[0][fidx(q)] if inr else 0, pat[1][fidx(q)] if inr else 0)
+                r.append(rv)
+                c = cls_of(rv)
+                if inr:
+                    if g0 + q == 0 or c == C_MIXED or c != pc:
+                        hm |= 1 << e
+                        lasth = ((g0 + q + 1) << 2) | c
+                    ones += bin(rv).count("1")
+                pc = c
+            thr.append((hm, ones, lasth, r))
+        exs = []
+        acc = (0, 0, 0)
+        for hm, ones, lasth, r in thr:
+            exs.append(acc)
+            acc = (acc[0] + bin(hm).count("1"), max(acc[1], lasth), acc[2] + ones)
+        tot = acc
+        pre = recs[-1] if recs else (0, 0, 0)
+        recs.append((pre[0] + tot[0], max(pre[1], tot[1]), pre[2] + tot[2]))
+        assert pre[0] + tot[0] <= cap
+        obase, oal = pre[0], pre[0] & ~3
+        last_tile = t == ntiles - 1
+        sout = [None] * (FT + 4)
+        deferred = {}
+
+        def emit(idx, wd):
+            if idx >= obase:
+                assert 0 <= idx - oal < FT + 4
+                sout[idx - oal] = wd
+            else:
+                assert idx == obase - 1
+                deferred[idx] = wd
+
+        for tid, (hm, ones, lasth, r) in enumerate(thr):
+            if not (hm or (last_tile and tid == 0 and tot[0] == 0)):
+                continue
+            o = obase + exs[tid][0]
+            prevh = max(pre[1], exs[tid][1])
+            for e in range(FGPT):
+                if (hm >> e) & 1:
+                    q = g0 + tid * FGPT + e
+                    if prevh and (prevh & 3) != C_MIXED:
+                        emit(o - 1, run_word(prevh & 3, q - ((prevh >> 2) - 1)))
+                    c = cls_of(r[e])
+                    if c == C_MIXED:
+                        emit(o, r[e])
+                    prevh = ((q + 1) << 2) | c
+                    o += 1
+            if last_tile and exs[tid][0] + bin(hm).count("1") == tot[0] and prevh and (prevh & 3) != C_MIXED:
+                emit(o - 1, run_word(prevh & 3, groups - ((prevh >> 2) - 1)))
+        cnt = tot[0] - (1 if (not last_tile and tot[0] and (tot[1] & 3) != C_MIXED) else 0)
+        for i in range(cnt):
+            assert sout[obase + i - oal] is not None, (t, i)
+            out[obase + i] = sout[obase + i - oal]
+        for k, v in deferred.items():
+            out[k] = v
+    n = recs[-1][0]
+    assert all(v is not None for v in out[:n])
+    return np.array(out[:n], dtype=np.uint32), recs[-1][2]
+
+
+def _split(ser):
+    w = np.asarray(ser, dtype=np.uint32)
+    if 0 < w[-1] < 31:
+        return w[:-2]
+    return w[:-1]
+
+
+def _expect(op, a, b):
+    """The oracle's result bits in canonical words (the form compress()
+    leaves on the dense paths: no count-1 fill)."""
+    ref, _ = oracle.binop(op, a, b, inplace=True)
+    g = []
+    for w in _split(ref):
+        w = int(w)
+        if w > ALL:
+            g.extend([ALL if w >= H1 else 0] * (w & MAXC))
+        else:
+            g.append(w)
+    return G.canonicalize(g), g
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_model_equals_oracle(seed):
+    rng = np.random.default_rng(100 + seed)
+    styles = ["dense", "mixed", "short", "sparse", "canon"]
+    ng = int(rng.integers(1, 3 * FT + 700)) if seed else 5 * FT
+    wa = G.random_words(rng, ng, styles[seed % 5])
+    wb = G.random_words(rng, ng, styles[(seed + 2) % 5])
+    if seed == 3:
+        wa = [G.fill(1, ng)]  # one fill over every tile
+    a, b = G.serialize(wa), G.serialize(wb)
+    for op in range(4):
+        want, groups = _expect(op, a, b)
+        got, ones = model(op, wa, wb, ng)
+        assert np.array_equal(got, np.asarray(want, np.uint32)), (seed, op)
+        assert ones == sum(bin(v).count("1") for v in groups)
+
+
+def test_model_geometric_runs():
+    """The raw-WAH workload's form (appendFill of geometric runs) at 2^17 bits."""
+    for d in (0.1, 0.5):
+        a = oracle.build_runs(G.geometric_runs(5, 1 << 17, d))
+        b = oracle.build_runs(G.geometric_runs(6, 1 << 17, d))
+        ba, bb = _split(a), _split(b)
+        groups = sum(wgroups(int(w)) for w in ba)
+        for op in range(4):
+            want, _ = _expect(op, a, b)
+            got, _ = model(op, ba, bb, groups)
+            assert np.array_equal(got, np.asarray(want, np.uint32)), (d, op)

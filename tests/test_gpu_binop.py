@@ -97,6 +97,38 @@ def _full_size(gpu_ctx, density):
             assert np.array_equal(w, ref), (op, ip)
 
 
+class _engine:
+    """A given engine for canonical-result operators
+    (WAHGPU_TUNE_DENSE_ENGINE): 3 two-pass, 4 single-pass (the default)."""
+
+    def __init__(self, ctx, engine):
+        self.ctx, self.engine = ctx, engine
+
+    def __enter__(self):
+        import libfastlib_b200 as L
+        self.old = self.ctx.get_tuning(L.TUNE_DENSE_ENGINE)
+        self.ctx.set_tuning(L.TUNE_DENSE_ENGINE, self.engine)
+
+    def __exit__(self, *exc):
+        import libfastlib_b200 as L
+        self.ctx.set_tuning(L.TUNE_DENSE_ENGINE, self.old)
+
+
+@pytest.mark.parametrize("engine", [3, 4])
+@pytest.mark.parametrize("density", [0.1, 0.5])
+def test_full_size_group_space_engines(gpu_ctx, density, engine):
+    """The two-pass and the single-pass group-space engines give the same
+    words at full size."""
+    with _engine(gpu_ctx, engine):
+        _full_size(gpu_ctx, density)
+
+
+@pytest.mark.parametrize("engine", [3, 4])
+def test_many_tiles_fuzz_engines(gpu_ctx, engine):
+    with _engine(gpu_ctx, engine):
+        _fuzz(gpu_ctx)
+
+
 @pytest.mark.parametrize("tile", [1024, 2048, 4096])
 def test_many_tiles_fuzz(gpu_ctx, tile):
     """Operands of ~10^5 words of mixed forms so results span many tiles and

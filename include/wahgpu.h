@@ -288,20 +288,25 @@ int wahgpu_server_free(wahgpu_server* s);
 
 /* ---- allocation-free row ids -------------------------------------------
  * No counterpart in the reference: an addition for callers that cannot
- * allocate device memory while they run — code issuing work during CUDA
- * graph capture (cudaMalloc is not allowed there), pipelines driven from
- * host callbacks, and runtimes that own all device memory through their own
- * pool.  Computes the ascending row ids of the serialized bitvector at
- * dev_serial (nwords words in device memory, the write(array_t&) layout)
- * into dev_rids (room for cap ids) and its count into *dev_count (device
- * memory; UINT64_MAX if a device-side wait gave up), on `stream`, without
- * allocating anything: its scratch is a fixed area of about 197 KiB
- * compiled into the library, held by every device that loads it.
- * Limit: at most 16,777,216 whole words (WAHGPU_ESIZE beyond).  The first
- * call on a device looks up the scratch area's device address
- * (cudaGetSymbolAddress) — make it before any stream capture.  All calls
- * share the scratch area: calls whose kernels overlap on the GPU race, so
- * order them (one stream).  Errors: wahgpu_last_error(NULL). */
+ * allocate device memory while they run — pipelines driven from host
+ * callbacks (which may not call CUDA API functions such as cudaMalloc),
+ * runtimes that own all device memory through their own pool and do not let
+ * a library allocate behind their back, and latency-bound paths that cannot
+ * afford the device-wide synchronisation an allocation may cause.  Computes
+ * the ascending row ids of the serialized bitvector at dev_serial (nwords
+ * words in device memory, the write(array_t&) layout) into dev_rids (room
+ * for cap ids; ids past cap are dropped, the count is still the full count)
+ * and its count into *dev_count (device memory), on `stream`, without
+ * allocating anything: its scratch is a fixed area of about 197 KiB compiled
+ * into the library, held by every device that loads it until the process
+ * exits.  *dev_count reads UINT64_MAX when a device-side wait gave up or the
+ * bitvector holds more bits than 32-bit row ids can number (the reference's
+ * nbits limit).  Limit: at most 16,777,216 whole words (WAHGPU_ESIZE
+ * beyond).  The first call on a device looks up the scratch area's device
+ * address (cudaGetSymbolAddress) — make it before any stream capture.  All
+ * calls share the scratch area and it keeps the last call's contents (each
+ * call clears what must start at zero): calls whose kernels overlap on the
+ * GPU race, so order them (one stream).  Errors: wahgpu_last_error(NULL). */
 int wahgpu_rids_noalloc(const uint32_t* dev_serial, uint64_t nwords, uint32_t* dev_rids,
                         uint64_t cap, unsigned long long* dev_count, void* stream);
 

@@ -2,18 +2,20 @@
 // allocation anywhere on the call path.
 //
 // Who needs it: callers that must not allocate device memory while they
-// work — code running while a CUDA graph is being captured (cudaMalloc is
-// not allowed inside a capture), GPU-side pipelines driven from host
-// callbacks, and embedding runtimes that own every device byte through their
+// work — GPU pipelines driven from host callbacks (a callback may not call
+// cudaMalloc), embedding runtimes that own every device byte through their
 // own memory pool and forbid a library from calling cudaMalloc behind their
-// back.  They pass device pointers for the input words and for the output,
-// and this entry point computes into them using only a fixed scratch area
-// compiled into the library.
+// back, and latency-bound paths that cannot take the device-wide
+// synchronisation an allocation may bring.  They pass device pointers for
+// the input words and for the output, and this entry point computes into
+// them using only a fixed scratch area compiled into the library.
 //
 // The scratch is one file-scope static __device__ array of NOALLOC_SCRATCH
 // bytes; every device that loads the library holds it until the process
-// exits.  All calls share it, so calls whose kernels overlap on the GPU race
-// with each other: issue them on one stream, or order them.
+// exits.  All calls share it and it keeps the last call's contents (each
+// call clears the words that must start at zero), so calls whose kernels
+// overlap on the GPU race with each other: issue them on one stream, or
+// order them.
 #include "../../include/wahgpu.h"
 #include "wah_dev.cuh"
 #include "wah_api_internal.h"
@@ -45,11 +47,18 @@ constexpr size_t NOALLOC_SCRATCH = sizeof(NoAllocScratch);  // about 197 KiB
 // cudaGetSymbolAddress below.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH];
 
-// 64-bit ones count + 32-bit group count, combined by addition
+// Row ids are 32-bit (the reference's nbits is a 32-bit count), so a
+// bitvector may cover at most 0xFFFFFFFF / 31 = 138,547,332 whole groups.
+// Group counts saturate here in the look-back: above that limit, below the
+// point where the sum of two could wrap.
+constexpr uint32_t NA_GROUP_SAT = 0x7FFFFFFFu;
+
+// 64-bit ones count + group count saturating at NA_GROUP_SAT (saturating
+// addition is associative, so the look-back may combine in any grouping)
 struct PosComb {
     __device__ __forceinline__ uint4 operator()(uint4 a, uint4 b) const {
         const uint64_t s = ((uint64_t)a.y << 32 | a.x) + ((uint64_t)b.y << 32 | b.x);
-        return make_uint4((uint32_t)s, (uint32_t)(s >> 32), a.z + b.z, a.w | b.w);
+        return make_uint4((uint32_t)s, (uint32_t)(s >> 32), min(a.z + b.z, NA_GROUP_SAT), a.w | b.w);
     }
 };
 
@@ -68,7 +77,8 @@ k_rids_serial(const uint32_t* __restrict__ ser, uint64_t nser, uint32_t* __restr
     __shared__ uint32_t tile_grp;
     __shared__ uint32_t fq_n;
     __shared__ uint64_t fq_off[NA_TILE / 2];
-    __shared__ uint32_t fq_row[NA_TILE / 2], fq_len[NA_TILE / 2];
+    __shared__ uint32_t fq_row[NA_TILE / 2];
+    __shared__ uint64_t fq_len[NA_TILE / 2];
     if (threadIdx.x == 0) {
         hdr[0] = claim_tile(&S0->sync);
         hdr[1] = ld_cg(&S0->sync.epoch);
@@ -86,7 +96,7 @@ k_rids_serial(const uint32_t* __restrict__ ser, uint64_t nser, uint32_t* __restr
     const uint32_t base = t * NA_TILE + threadIdx.x * NA_WPT;
     uint32_t v[NA_WPT];
     uint64_t ones = 0;
-    uint32_t grp = 0;
+    uint64_t grp = 0;
 #pragma unroll
     for (int q = 0; q < NA_WPT; ++q) {
         const bool in = base + q < n;
@@ -107,7 +117,8 @@ k_rids_serial(const uint32_t* __restrict__ ser, uint64_t nser, uint32_t* __restr
     const uint64_t ones_ex = block_exscan64(ones, sh_ones, ones_tot);
     const uint64_t grp_ex = block_exscan64(grp, sh_grp, grp_tot);
     if (threadIdx.x < 32) {
-        const uint4 mine = make_uint4((uint32_t)ones_tot, (uint32_t)(ones_tot >> 32), (uint32_t)grp_tot, 0u);
+        const uint4 mine = make_uint4((uint32_t)ones_tot, (uint32_t)(ones_tot >> 32),
+                                      (uint32_t)min(grp_tot, (uint64_t)NA_GROUP_SAT), 0u);
         uint4 pre = make_uint4(0, 0, 0, 0);
         bool ok = true;
         if (t == 0) {
@@ -126,12 +137,20 @@ k_rids_serial(const uint32_t* __restrict__ ser, uint64_t nser, uint32_t* __restr
             tile_ones = (uint64_t)pre.y << 32 | pre.x;
             tile_grp = pre.z;
             if (t == ntiles - 1) {
-                // the active word's rows follow the last whole group
-                uint64_t off = tile_ones + ones_tot;
-                const uint32_t rbase = (tile_grp + (uint32_t)grp_tot) * 31u;
-                for (uint32_t b = 0; b < anb; ++b)
-                    if ((aval >> (anb - 1u - b)) & 1u) { if (off < cap) out[off] = rbase + b; ++off; }
-                atomicMax(count, (unsigned long long)off);
+                const uint64_t groups = (uint64_t)tile_grp + grp_tot;
+                if (groups * 31u + anb > 0xFFFFFFFFull) {
+                    // more bits than 32-bit row ids can number: the count
+                    // reads UINT64_MAX, as for a wait that gave up
+                    atomicExch(&S0->status.status, DEV_ERR_RANGE);
+                    atomicMax(count, ~0ull);
+                } else {
+                    // the active word's rows follow the last whole group
+                    uint64_t off = tile_ones + ones_tot;
+                    const uint32_t rbase = (uint32_t)groups * 31u;
+                    for (uint32_t b = 0; b < anb; ++b)
+                        if ((aval >> (anb - 1u - b)) & 1u) { if (off < cap) out[off] = rbase + b; ++off; }
+                    atomicMax(count, (unsigned long long)off);
+                }
             }
         }
     }
@@ -145,11 +164,16 @@ k_rids_serial(const uint32_t* __restrict__ ser, uint64_t nser, uint32_t* __restr
             if (x > ALLONES) {
                 const uint32_t c = x & MAXCNT;
                 if (x >= HEADER1) {
-                    const uint32_t slot = atomicAdd(&fq_n, 1u);
-                    if (slot < (uint32_t)(NA_TILE / 2)) {
-                        fq_off[slot] = off; fq_row[slot] = g * 31u; fq_len[slot] = c * 31u;
-                    } else {  // list full: this thread writes the fill
-                        for (uint32_t r = 0; r < c * 31u; ++r) if (off + r < cap) out[off + r] = g * 31u + r;
+                    // only the ids that fit below cap are written; the
+                    // count comes from the look-back, not from these loops
+                    const uint64_t len = off < cap ? min((uint64_t)c * 31u, cap - off) : 0ull;
+                    if (len) {
+                        const uint32_t slot = atomicAdd(&fq_n, 1u);
+                        if (slot < (uint32_t)(NA_TILE / 2)) {
+                            fq_off[slot] = off; fq_row[slot] = g * 31u; fq_len[slot] = len;
+                        } else {  // list full: this thread writes the fill
+                            for (uint64_t r = 0; r < len; ++r) out[off + r] = g * 31u + (uint32_t)r;
+                        }
                     }
                     off += (uint64_t)c * 31u;
                 }
@@ -169,10 +193,9 @@ k_rids_serial(const uint32_t* __restrict__ ser, uint64_t nser, uint32_t* __restr
     __syncthreads();
     const uint32_t nfq = min(fq_n, (uint32_t)(NA_TILE / 2));
     for (uint32_t k = 0; k < nfq; ++k) {
-        const uint64_t o = fq_off[k];
-        const uint32_t r0 = fq_row[k], len = fq_len[k];
-        for (uint32_t r = threadIdx.x; r < len; r += NA_THREADS)
-            if (o + r < cap) out[o + r] = r0 + r;
+        const uint64_t o = fq_off[k], len = fq_len[k];  // o + len <= cap
+        const uint32_t r0 = fq_row[k];
+        for (uint64_t r = threadIdx.x; r < len; r += NA_THREADS) out[o + r] = r0 + (uint32_t)r;
     }
     __syncthreads();
     if (threadIdx.x == 0) finish_tile(&S0->sync, ntiles);

@@ -224,11 +224,38 @@ int wahgpu_index_bitmap(wahgpu_index* idx, uint32_t j, wahgpu_bv** out);
  * maxval); returns their count, WAHGPU_ESIZE if cap is too small. */
 int64_t wahgpu_index_keys(wahgpu_index* idx, double* out, uint64_t cap);
 
+/* The index as the reference's serialized triple, the layout
+ * wahgpu_index_from_triple takes and relic::write(keys, starts, bitmaps) /
+ * bin::write(keys, starts, bitmaps) produce (src/irelic.cpp:644-667,
+ * src/ibin.cpp:5836-5859; fastbit_iapi_deconstruct_index,
+ * src/iapi.cpp:1915): keys (relic: values; bin: minval then maxval), the
+ * nobs + 1 word offsets, the bitmaps' serialized words.  Sizes are always
+ * reported; the arrays are filled when all three are given (WAHGPU_ESIZE
+ * when a capacity is short).  A triple from here attaches to the reference
+ * with fastbit_iapi_attach_full_index (src/iapi.cpp:2018). */
+int wahgpu_index_deconstruct(wahgpu_index* idx, double* keys, uint64_t kcap, uint64_t* nkeys,
+                             int64_t* offsets, uint64_t ocap, uint64_t* noffsets, uint32_t* bitmaps,
+                             uint64_t bcap, uint64_t* nbitmaps);
+
 int wahgpu_index_free(wahgpu_index* idx);
 int64_t wahgpu_index_nbitmaps(wahgpu_index* idx);
 int64_t wahgpu_index_nrows(wahgpu_index* idx);
 /* estimate(count) without a range: all 1 bits (src/irelic.cpp:1843). */
 int64_t wahgpu_index_total_ones(wahgpu_index* idx);
+
+/* index::estimate(expr, lower, upper) (src/index.h:191) for one term:
+ * *lower = the rows certainly hit, *upper = a superset of the hits, both as
+ * new bitvectors (compress() form).  relic (src/irelic.h:58-62): lower =
+ * the hits, upper empty.  bin (src/ibin.cpp:6722-6829): lower = the bins
+ * wholly inside the range, upper = those and the edge bins, empty when no
+ * bin straddles an end.  An empty upper means lower is exact (the
+ * reference's convention).  Needs no raw values. */
+int wahgpu_estimate(wahgpu_ctx* ctx, const wahgpu_term* term, wahgpu_bv** lower, wahgpu_bv** upper);
+/* index::estimate(expr) (src/index.h:196): an upper bound of one term's hit
+ * count — relic: exact (src/irelic.cpp:1843-1854); bin: the 1 bits of the
+ * bins wholly inside and of the edge bins (src/ibin.cpp:6832-6889).
+ * Computed on the host from per-bitmap counts. */
+int64_t wahgpu_estimate_count(wahgpu_ctx* ctx, const wahgpu_term* term);
 
 /* Evaluates the AND of nterms range terms (countQuery::evaluate,
  * src/countQuery.cpp:292-332, whose terms go through relic::evaluate /
@@ -254,6 +281,12 @@ const uint32_t* wahgpu_batch_device_rids(wahgpu_batch* batch);
  * ORs (or their complement), of its edge bitmaps and the raw values of the
  * edge bitmaps' rows; 8 per query for the count. */
 int64_t wahgpu_batch_bytes(wahgpu_batch* batch);
+/* Bytes any evaluation of the batch must move, whatever the index layout:
+ * per term the words of the bitmaps sumBins ORs — the covered set, or its
+ * complement when that is smaller (src/index.cpp:6450-6520) — plus the edge
+ * bitmaps' words and one raw value per edge row (bin::checkBin,
+ * src/ibin.cpp:2220); 8 bytes per count.  (Row ids add 4 bytes each.) */
+int64_t wahgpu_batch_min_bytes(wahgpu_batch* batch);
 int wahgpu_batch_free(wahgpu_batch* batch);
 
 

@@ -117,11 +117,17 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
                                               ctypes.POINTER(P)]),
         "wahgpu_index_bitmap": (ctypes.c_int, [P, ctypes.c_uint32, ctypes.POINTER(P)]),
         "wahgpu_index_keys": (ctypes.c_int64, [P, ctypes.POINTER(ctypes.c_double), ctypes.c_uint64]),
+        "wahgpu_index_deconstruct": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_double), ctypes.c_uint64,
+                                                    ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int64),
+                                                    ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64), U32P,
+                                                    ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
         "wahgpu_index_nbitmaps": (ctypes.c_int64, [P]),
         "wahgpu_index_nrows": (ctypes.c_int64, [P]),
         "wahgpu_index_total_ones": (ctypes.c_int64, [P]),
         "wahgpu_evaluate": (ctypes.c_int64, [P, ctypes.POINTER(_Term), ctypes.c_uint32, U32P, ctypes.c_uint64,
                                              ctypes.POINTER(P)]),
+        "wahgpu_estimate": (ctypes.c_int, [P, ctypes.POINTER(_Term), ctypes.POINTER(P), ctypes.POINTER(P)]),
+        "wahgpu_estimate_count": (ctypes.c_int64, [P, ctypes.POINTER(_Term)]),
         "wahgpu_batch_create": (ctypes.c_int, [P, ctypes.POINTER(_Term), U32P, ctypes.c_uint32, ctypes.c_uint64,
                                                ctypes.c_int, ctypes.POINTER(P)]),
         "wahgpu_batch_run": (ctypes.c_int, [P]),
@@ -130,6 +136,7 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "wahgpu_batch_device_rids": (P, [P]),
         "wahgpu_batch_free": (ctypes.c_int, [P]),
         "wahgpu_batch_bytes": (ctypes.c_int64, [P]),
+        "wahgpu_batch_min_bytes": (ctypes.c_int64, [P]),
         "wahgpu_server_create": (ctypes.c_int, [P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(P)]),
         "wahgpu_server_submit": (ctypes.c_int64, [P, ctypes.POINTER(_Term), ctypes.c_uint32, ctypes.c_uint64]),
         "wahgpu_server_wait": (ctypes.c_int64, [P, ctypes.c_int64, ctypes.POINTER(ctypes.c_uint64), U32P,
@@ -395,6 +402,22 @@ class Index:
             self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cap)))
         return out[:n]
 
+    def deconstruct(self):
+        """The reference's (keys, offsets, bitmaps) triple of this index
+        (relic::write / bin::write to arrays, fastbit_iapi_deconstruct_index)."""
+        lib, h = self.ctx.lib, self.h
+        nk, no, nb = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        self.ctx.check(lib.wahgpu_index_deconstruct(h, None, 0, ctypes.byref(nk), None, 0, ctypes.byref(no),
+                                                    None, 0, ctypes.byref(nb)))
+        keys = np.empty(nk.value, np.float64)
+        offs = np.empty(no.value, np.int64)
+        bms = np.empty(max(nb.value, 1), np.uint32)
+        self.ctx.check(lib.wahgpu_index_deconstruct(
+            h, keys.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(keys), ctypes.byref(nk),
+            offs.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), len(offs), ctypes.byref(no),
+            bms.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), len(bms), ctypes.byref(nb)))
+        return keys, offs, bms[:nb.value]
+
     def bitmap(self, j: int) -> "Bitvector":
         h = ctypes.c_void_p()
         self.ctx.check(self.ctx.lib.wahgpu_index_bitmap(self.h, j, ctypes.byref(h)))
@@ -468,6 +491,23 @@ def evaluate(ctx: Context, terms, want_rids: bool = True, want_hits: bool = Fals
     return n, (rids[:n].copy() if want_rids else None), hits
 
 
+def estimate(ctx: Context, term):
+    """index::estimate(expr, lower, upper): (lower, upper) Bitvectors — the
+    rows certainly hit and a superset of the hits (upper is empty when
+    lower is exact)."""
+    lo, up = ctypes.c_void_p(), ctypes.c_void_p()
+    t = _Term(term.idx, term.lop, term.lo, term.rop, term.hi)
+    ctx.check(ctx.lib.wahgpu_estimate(ctx.h, ctypes.byref(t), ctypes.byref(lo), ctypes.byref(up)))
+    return Bitvector(ctx, lo), Bitvector(ctx, up)
+
+
+def estimate_count(ctx: Context, term) -> int:
+    """index::estimate(expr): an upper bound of the hit count (relic:
+    exact; bin: the bins wholly inside and the edge bins)."""
+    t = _Term(term.idx, term.lop, term.lo, term.rop, term.hi)
+    return ctx.check(int(ctx.lib.wahgpu_estimate_count(ctx.h, ctypes.byref(t))))
+
+
 class Batch:
     """Queries prepared once and run as one kernel launch (capturable in a
     CUDA graph).  queries: list of lists of terms."""
@@ -491,6 +531,11 @@ class Batch:
     def nbytes(self) -> int:
         """Algorithmic bytes of one run (bitmap words read, edge-row values)."""
         return self.ctx.check(int(self.ctx.lib.wahgpu_batch_bytes(self.h)))
+
+    def min_bytes(self) -> int:
+        """Bytes any evaluation must move: the bitmaps sumBins ORs (covered
+        set or complement), edge bitmaps and edge rows, 8 per count."""
+        return self.ctx.check(int(self.ctx.lib.wahgpu_batch_min_bytes(self.h)))
 
     def counts(self) -> np.ndarray:
         out = np.zeros(self.nq, dtype=np.uint64)

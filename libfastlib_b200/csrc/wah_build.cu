@@ -381,3 +381,46 @@ extern "C" int64_t wahgpu_index_keys(wahgpu_index* x, double* out, uint64_t cap)
     std::copy(x->keys.begin(), x->keys.end(), out);
     return (int64_t)n;
 }
+
+// The index as the reference's serialized triple (relic::write(keys, starts,
+// bitmaps), src/irelic.cpp:644-667; bin::write, src/ibin.cpp:5836-5859;
+// fastbit_iapi_deconstruct_index, src/iapi.cpp:1915): keys (relic: values;
+// bin: minval then maxval), nobs + 1 word offsets, and every bitmap's
+// serialized words (write(array_t&)) one after the other.
+extern "C" int wahgpu_index_deconstruct(wahgpu_index* x, double* keys, uint64_t kcap, uint64_t* nkeys,
+                                        int64_t* offsets, uint64_t ocap, uint64_t* noffsets, uint32_t* bitmaps,
+                                        uint64_t bcap, uint64_t* nbitmaps) {
+    if (!x) return WAHGPU_EINVAL;
+    wahgpu_ctx* ctx = x->ctx;
+    std::vector<BitmapMeta> bm(x->nobs);
+    cudaError_t e = cudaSuccess;
+    if (x->nobs) e = cudaMemcpyAsync(bm.data(), x->d_bm, sizeof(BitmapMeta) * x->nobs, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return wg_fail(ctx, WAHGPU_ECUDA, "reading bitmap metadata failed: %s", cudaGetErrorString(e));
+    std::vector<int64_t> off(x->nobs + 1ull, 0);
+    uint64_t pool = 0;
+    for (uint32_t j = 0; j < x->nobs; ++j) {
+        off[j + 1] = off[j] + (int64_t)bm[j].n + (bm[j].anb ? 2 : 1);
+        pool = std::max<uint64_t>(pool, bm[j].wstart + bm[j].n);
+    }
+    if (nkeys) *nkeys = x->keys.size();
+    if (noffsets) *noffsets = off.size();
+    if (nbitmaps) *nbitmaps = (uint64_t)off.back();
+    if (!(keys && offsets && bitmaps)) return WAHGPU_OK;
+    if (kcap < x->keys.size() || ocap < off.size() || bcap < (uint64_t)off.back())
+        return wg_fail(ctx, WAHGPU_ESIZE, "output arrays too small for the triple");
+    std::vector<uint32_t> w(pool);
+    if (pool) e = cudaMemcpyAsync(w.data(), x->d_words, pool * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return wg_fail(ctx, WAHGPU_ECUDA, "reading the bitmaps failed: %s", cudaGetErrorString(e));
+    std::copy(x->keys.begin(), x->keys.end(), keys);
+    std::copy(off.begin(), off.end(), offsets);
+    for (uint32_t j = 0; j < x->nobs; ++j) {
+        uint32_t* d = bitmaps + off[j];
+        std::copy(w.begin() + bm[j].wstart, w.begin() + bm[j].wstart + bm[j].n, d);
+        d += bm[j].n;
+        if (bm[j].anb) *d++ = bm[j].aval;
+        *d = bm[j].anb;
+    }
+    return WAHGPU_OK;
+}

@@ -260,7 +260,15 @@ static bool pass_h(double v, int lop, double lo, int rop, double hi) {
 // value.  relic (src/irelic.cpp:1416-1809): a bitmap per key; bin
 // (src/ibin.cpp:7596-8460): a bin whose [minval, maxval] lies inside the
 // range passes whole, one that straddles an end is checked.
-static int locate(wahgpu_ctx* ctx, const wahgpu_index* x, const wahgpu_term* t, DevTerm& out) {
+// Term modes: the hits (LOC_HITS); the rows certainly hit, i.e. the
+// bitmaps wholly inside without the edge bins (LOC_LOWER); the candidate
+// rows, the wholly-inside bitmaps and the edge bins OR'ed whole (LOC_UPPER)
+// — the lower and upper bounds of bin::estimate(expr, lower, upper),
+// src/ibin.cpp:6722-6829.
+enum LocMode { LOC_HITS = 0, LOC_LOWER = 1, LOC_UPPER = 2 };
+
+static int locate(wahgpu_ctx* ctx, const wahgpu_index* x, const wahgpu_term* t, DevTerm& out,
+                  int mode = LOC_HITS) {
     out = DevTerm{};
     out.lop = (uint32_t)t->lop; out.rop = (uint32_t)t->rop; out.lo = t->lo; out.hi = t->hi;
     uint32_t h0 = 0, h1 = 0, nc = 0;
@@ -303,6 +311,15 @@ static int locate(wahgpu_ctx* ctx, const wahgpu_index* x, const wahgpu_term* t, 
             else if (cls[j] == 2)
                 return wg_fail(ctx, WAHGPU_EINVAL, "bitmaps wholly inside the range are not contiguous");
     }
+    if (mode == LOC_LOWER) {
+        nc = 0;
+    } else if (mode == LOC_UPPER && nc > 0) {
+        // the edge bins join the span (they are adjacent to it: every bin
+        // between two straddling bins lies wholly inside)
+        uint32_t a = h1 > h0 ? h0 : out.cand[0], b = h1 > h0 ? h1 : out.cand[0] + 1u;
+        for (uint32_t c = 0; c < nc; ++c) { a = std::min(a, out.cand[c]); b = std::max(b, out.cand[c] + 1u); }
+        h0 = a; h1 = b; nc = 0;
+    }
     if (nc > 0 && !x->d_values)
         return wg_fail(ctx, WAHGPU_EINVAL, "range needs row checks but the index has no raw values attached");
     out.h0 = h0; out.h1 = h1; out.ncand = nc;
@@ -336,8 +353,16 @@ static uint64_t term_estimate(const wahgpu_index* x, const DevTerm& d) {
 }
 
 // ------------------------------------------------------------------ batches
+static int batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, const uint32_t* query_offsets,
+                        uint32_t nq, uint64_t rid_cap, int dense_first, int mode, wahgpu_batch** out);
+
 extern "C" int wahgpu_batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, const uint32_t* query_offsets,
                                    uint32_t nq, uint64_t rid_cap, int dense_first, wahgpu_batch** out) {
+    return batch_create(ctx, terms, query_offsets, nq, rid_cap, dense_first, LOC_HITS, out);
+}
+
+static int batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, const uint32_t* query_offsets,
+                        uint32_t nq, uint64_t rid_cap, int dense_first, int mode, wahgpu_batch** out) {
     if (!ctx || !out || !terms || !query_offsets || nq == 0) return wg_fail(ctx, WAHGPU_EINVAL, "bad argument");
     *out = nullptr;
     const uint32_t nt = query_offsets[nq];
@@ -346,11 +371,11 @@ extern "C" int wahgpu_batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, co
     if (!x0) return wg_fail(ctx, WAHGPU_EINVAL, "term without an index");
     std::vector<const wahgpu_index*> idx;
     std::vector<DevTerm> dt(nt);
-    uint64_t bytes = 0;
+    uint64_t bytes = 0, min_bytes = 0;
     for (uint32_t i = 0; i < nt; ++i) {
         const wahgpu_index* x = terms[i].idx;
         if (!x || x->nrows != x0->nrows) return wg_fail(ctx, WAHGPU_EINVAL, "term %u: indexes of one batch must share their row count", i);
-        int rc = locate(ctx, x, &terms[i], dt[i]);
+        int rc = locate(ctx, x, &terms[i], dt[i], mode);
         if (rc) return rc;
         auto it = std::find(idx.begin(), idx.end(), x);
         dt[i].index = (uint32_t)(it - idx.begin());
@@ -366,6 +391,12 @@ extern "C" int wahgpu_batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, co
             bytes += 4 * (dt[i].flip ? x->cum_words[x->nobs] - in : in);
         for (uint32_t c = 0; c < dt[i].ncand; ++c)
             bytes += 4 * (x->bwords[dt[i].cand[c]] + x->bones[dt[i].cand[c]]);
+        // what sumBins itself must read: the covered bitmaps or, when they
+        // hold more than half the words, their complement
+        // (src/index.cpp:6490), plus the edge bitmaps and their rows
+        min_bytes += 4 * std::min(in, x->cum_words[x->nobs] - in);
+        for (uint32_t c = 0; c < dt[i].ncand; ++c)
+            min_bytes += 4 * (x->bwords[dt[i].cand[c]] + x->bones[dt[i].cand[c]]);
     }
     std::vector<DevQuery> dq(nq);
     for (uint32_t q = 0; q < nq; ++q) {
@@ -381,6 +412,7 @@ extern "C" int wahgpu_batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, co
     wahgpu_batch* B = new wahgpu_batch();
     B->ctx = ctx; B->nq = nq; B->nterms = nt; B->nidx = (uint32_t)idx.size();
     B->bytes = bytes + 8ull * nq;
+    B->min_bytes = min_bytes + 8ull * nq;
     B->groups = x0->groups; B->anb = x0->anb; B->ntiles = x0->ntiles;
     B->d_idx = static_cast<DevIndex*>(wg_alloc(ctx, di.size() * sizeof(DevIndex)));
     B->d_terms = static_cast<DevTerm*>(wg_alloc(ctx, nt * sizeof(DevTerm)));
@@ -506,6 +538,11 @@ extern "C" const uint32_t* wahgpu_batch_device_rids(wahgpu_batch* B) { return B 
 // (or of their complement), of its edge bitmaps and the raw values of the
 // edge bitmaps' rows; 8 per query for its count.
 extern "C" int64_t wahgpu_batch_bytes(wahgpu_batch* B) { return B ? (int64_t)B->bytes : WAHGPU_EINVAL; }
+// Bytes any evaluation of the batch must move, whatever its index layout:
+// per term the words of the bitmaps sumBins ORs (the covered set, or its
+// complement when that is smaller, src/index.cpp:6490), the edge bitmaps'
+// words and one raw value per edge row; 8 bytes per count.
+extern "C" int64_t wahgpu_batch_min_bytes(wahgpu_batch* B) { return B ? (int64_t)B->min_bytes : WAHGPU_EINVAL; }
 
 extern "C" int wahgpu_batch_free(wahgpu_batch* B) {
     if (!B) return WAHGPU_EINVAL;
@@ -522,12 +559,59 @@ extern "C" int wahgpu_batch_free(wahgpu_batch* B) {
 // One conjunctive query (countQuery::evaluate, src/countQuery.cpp:292):
 // returns the hit count; row ids into host memory when out is given; the hit
 // bitvector (compress()ed) when hits is given.
+static int64_t evaluate_mode(wahgpu_ctx* ctx, const wahgpu_term* terms, uint32_t nterms, uint32_t* rids,
+                             uint64_t cap, wahgpu_bv** hits, int mode);
+
 extern "C" int64_t wahgpu_evaluate(wahgpu_ctx* ctx, const wahgpu_term* terms, uint32_t nterms,
                                    uint32_t* rids, uint64_t cap, wahgpu_bv** hits) {
+    return evaluate_mode(ctx, terms, nterms, rids, cap, hits, LOC_HITS);
+}
+
+// index::estimate(expr, lower, upper) (src/index.h:191; relic,
+// src/irelic.h:58-62: lower = the hits, upper empty; bin,
+// src/ibin.cpp:6722-6829: lower = the bins wholly inside, upper = lower and
+// the edge bins, empty when there is no edge bin).  An empty upper means
+// lower is exact, the reference's convention.
+extern "C" int wahgpu_estimate(wahgpu_ctx* ctx, const wahgpu_term* term, wahgpu_bv** lower, wahgpu_bv** upper) {
+    if (!ctx || !term || !term->idx || !lower || !upper) return wg_fail(ctx, WAHGPU_EINVAL, "bad argument");
+    *lower = nullptr;
+    *upper = nullptr;
+    DevTerm dl, du;  // no edge bin when the two spans agree
+    int rc = locate(ctx, term->idx, term, dl, LOC_LOWER);
+    if (!rc) rc = locate(ctx, term->idx, term, du, LOC_UPPER);
+    if (rc) return rc;
+    const bool exact = dl.h0 == du.h0 && dl.h1 == du.h1;
+    int64_t n = evaluate_mode(ctx, term, 1, nullptr, 0, lower, LOC_LOWER);
+    if (n < 0) return (int)n;
+    if (exact) {
+        rc = wahgpu_bv_create(ctx, 1, upper);
+    } else {
+        n = evaluate_mode(ctx, term, 1, nullptr, 0, upper, LOC_UPPER);
+        rc = n < 0 ? (int)n : WAHGPU_OK;
+    }
+    if (rc) { wahgpu_bv_free(*lower); *lower = nullptr; }
+    return rc;
+}
+
+// index::estimate(expr) (src/index.h:196): an upper bound of the hit count —
+// relic: the exact count (src/irelic.cpp:1843-1854); bin: the 1 bits of the
+// bins wholly inside and of the edge bins (src/ibin.cpp:6832-6889).  From
+// the host-side per-bitmap counts; no device work.
+extern "C" int64_t wahgpu_estimate_count(wahgpu_ctx* ctx, const wahgpu_term* term) {
+    if (!ctx || !term || !term->idx) return wg_fail(ctx, WAHGPU_EINVAL, "bad argument");
+    const wahgpu_index* x = term->idx;
+    DevTerm d;
+    const int rc = locate(ctx, x, term, d, LOC_UPPER);
+    if (rc) return rc;
+    return (int64_t)(x->cum_ones[d.h1] - x->cum_ones[d.h0]);
+}
+
+static int64_t evaluate_mode(wahgpu_ctx* ctx, const wahgpu_term* terms, uint32_t nterms, uint32_t* rids,
+                             uint64_t cap, wahgpu_bv** hits, int mode) {
     if (!ctx || !terms || nterms == 0 || (cap && !rids)) return wg_fail(ctx, WAHGPU_EINVAL, "bad argument");
     const uint32_t qo[2] = {0, nterms};
     wahgpu_batch* B = nullptr;
-    int rc = wahgpu_batch_create(ctx, terms, qo, 1, rids ? cap : 0, hits ? 1 : 0, &B);
+    int rc = batch_create(ctx, terms, qo, 1, rids ? cap : 0, hits ? 1 : 0, mode, &B);
     if (rc) return rc;
     rc = wahgpu_batch_run(B);
     uint64_t cnt = 0;

@@ -47,6 +47,7 @@ struct wahgpu_batch {
     size_t scan_tmp_bytes = 0;
     std::vector<unsigned long long> h_counts, h_start;
     uint64_t bytes = 0;               // algorithmic bytes one run reads
+    uint64_t min_bytes = 0;           // the bytes sumBins itself must read (covered set or complement)
     bool h_valid = false;
 };
 

@@ -37,6 +37,36 @@
 //        through fastbit_iapi_build_index("<binning nbins=N equal_weight/>")
 //        and its triple (bin ctor, ibin.cpp:358; write, ibin.cpp:5530-5834);
 //        reply: status (0 ok)
+//  11 nruns_a(u64) runs_a[nruns_a](u64) nruns_b(u64) runs_b[nruns_b](u64)
+//        -> two appendFill-built bitvectors (alternating 0/1 runs, 0 first,
+//        bitvector.h:800) and, for op & | ^ - in both forms (a OP b, then
+//        a OP= b on a private copy of a), the compress()ed result;
+//        reply: len a[len], len b[len], then 8 x (status cnt len words[len])
+//  12 nthreads reps flags ncols, per column: vtype(1 uint32, 2 int32,
+//        3 float32) nrows vals[nrows](4 B) nkeys(u64) keys(f64) noffs(u64)
+//        offs(i64) nbms(u64) bms(u32); then nq, per query: nterms, per term:
+//        col lo(f64) hi(f64) for lo <= x < hi
+//        -> the in-memory C API on indexes given as triples: every column
+//        registered (fastbit_iapi_register_array, src/iapi.cpp:1644) with
+//        its triple attached (fastbit_iapi_attach_full_index, 2018); a query
+//        is osr(x >= lo) AND osr(x < hi) per term, AND across terms
+//        (fastbit_selection_osr / combine, 2062, 1285), evaluated
+//        (fastbit_selection_evaluate, 1383) and, with flags bit 0, its row
+//        ids read (fastbit_selection_get_coordinates, 1517); each selection
+//        is freed after use, so no cached answer is reused.  One untimed
+//        pass on one thread gives the answers; then `reps` timed passes on
+//        nthreads threads (queries round robin).
+//        reply: status seconds(f64, timed passes, max over threads), then
+//        per query: count(u64) seconds(f64, the untimed one-thread pass)
+//        [nrids rids[nrids] with row ids]
+//  13 nthreads reps nrows vals[nrows] nq (lo hi)(f64 x2)[nq] -> times
+//        ibis::relic over the uint32 column (construct(array_t),
+//        irelic.cpp:879): per query evaluate(qContinuousRange(lo <= x < hi),
+//        hits) (irelic.cpp:1827) and the firstIndexSet row-id walk
+//        (bitvector.h:421-542).  One untimed pass on one thread warms the
+//        lazily counted members; then `reps` timed passes on nthreads threads
+//        (queries round robin, each thread its own hit vectors).
+//        reply: seconds(f64, max over threads), then per query count(u64)
 //   8 nthreads reps nops (op na a[na] nb b[nb])[nops] -> times the reference's
 //        operators: each of nthreads threads builds its own operand copies,
 //        then runs its share of the ops (round robin) reps times, each as
@@ -124,6 +154,72 @@ static void* time_thread(void* p) {
             delete R;
         }
     }
+    j->secs = now_s() - t0;
+    return 0;
+}
+
+// request 12: one query of the in-memory C API on the registered columns
+struct Term12 { uint32_t col; double lo, hi; };
+struct Job12 {
+    const std::vector<std::vector<Term12> >* qs;
+    uint32_t tid, nth, reps, rids;
+    pthread_barrier_t* bar;
+    double secs;
+};
+static int64_t eval12(const std::vector<Term12>& q, uint32_t rids, std::vector<uint32_t>* out) {
+    FastBitSelectionHandle h = 0;
+    for (size_t k = 0; k < q.size(); ++k) {
+        char nm[16];
+        snprintf(nm, sizeof nm, "c%u", q[k].col);
+        FastBitSelectionHandle a = fastbit_selection_osr(nm, FastBitCompareGreaterEqual, q[k].lo);
+        FastBitSelectionHandle b = fastbit_selection_osr(nm, FastBitCompareLess, q[k].hi);
+        FastBitSelectionHandle t = fastbit_selection_combine(a, FastBitCombineAnd, b);
+        h = h ? fastbit_selection_combine(h, FastBitCombineAnd, t) : t;
+    }
+    int64_t cnt = fastbit_selection_evaluate(h);
+    if (cnt > 0 && rids) {
+        std::vector<uint64_t> co(cnt);
+        const int64_t got = fastbit_selection_get_coordinates(h, &co[0], cnt, 0);
+        if (out) for (int64_t i = 0; i < got; ++i) out->push_back((uint32_t)co[i]);
+    }
+    fastbit_selection_free(h);
+    return cnt;
+}
+static void* job12(void* p) {
+    Job12* j = (Job12*)p;
+    pthread_barrier_wait(j->bar);
+    const double t0 = now_s();
+    for (uint32_t r = 0; r < j->reps; ++r)
+        for (size_t q = j->tid; q < j->qs->size(); q += j->nth) eval12((*j->qs)[q], j->rids, 0);
+    j->secs = now_s() - t0;
+    return 0;
+}
+
+// request 13: relic::evaluate and the row-id walk per query
+struct Job13 {
+    const ibis::relic* rel;
+    const std::vector<double>* lo;
+    const std::vector<double>* hi;
+    uint32_t tid, nth, reps;
+    pthread_barrier_t* bar;
+    double secs;
+    uint64_t sink;
+};
+static uint64_t eval13(const ibis::relic& rel, double lo, double hi, std::vector<uint32_t>& rids) {
+    ibis::qContinuousRange expr(lo, ibis::qExpr::OP_LE, "x", ibis::qExpr::OP_LT, hi);
+    ibis::bitvector hits;
+    const long c = rel.evaluate(expr, hits);
+    rids.clear();
+    rids_of(hits, rids);
+    return c < 0 ? 0 : (uint64_t)c;
+}
+static void* job13(void* p) {
+    Job13* j = (Job13*)p;
+    std::vector<uint32_t> rids;
+    pthread_barrier_wait(j->bar);
+    const double t0 = now_s();
+    for (uint32_t r = 0; r < j->reps; ++r)
+        for (size_t q = j->tid; q < j->lo->size(); q += j->nth) j->sink += eval13(*j->rel, (*j->lo)[q], (*j->hi)[q], rids);
     j->secs = now_s() - t0;
     return 0;
 }
@@ -257,6 +353,138 @@ int main(int argc, char** argv) {
             }
             delete [] keys; delete [] offs; delete [] bms;
             fastbit_iapi_free_all();
+        } else if (kind == 11) {
+            ibis::bitvector A, B;
+            for (int k = 0; k < 2; ++k) {
+                ibis::bitvector& X = k ? B : A;
+                const uint64_t n = rd64();
+                for (uint64_t i = 0; i < n; ++i) X.appendFill((int)(i & 1), (uint32_t)rd64());
+            }
+            std::vector<uint32_t> wa, wb;
+            for (int k = 0; k < 2; ++k) {
+                ibis::array_t<uint32_t> w;
+                (k ? B : A).write(w);
+                std::vector<uint32_t>& v = k ? wb : wa;
+                v.assign(w.begin(), w.end());
+                wrv(v);
+            }
+            for (int op = 0; op < 4; ++op) {
+                for (int inplace = 0; inplace < 2; ++inplace) {
+                    ibis::bitvector* R = 0;
+                    int st = 0;
+                    try {
+                        if (inplace) {
+                            // a private copy of a (its own storage), then a OP= b
+                            R = from_serial(wa);
+                            switch (op) { case 0: *R &= B; break; case 1: *R |= B; break;
+                                          case 2: *R ^= B; break; default: *R -= B; }
+                        } else {
+                            switch (op) { case 0: R = A & B; break; case 1: R = A | B; break;
+                                          case 2: R = A ^ B; break; default: R = A - B; }
+                        }
+                        R->compress();
+                    } catch (...) { st = 1; }
+                    reply_bv(st, R);
+                    delete R;
+                }
+            }
+        } else if (kind == 12) {
+            const uint32_t nth = rd32(), reps = rd32(), flags = rd32(), ncols = rd32();
+            std::vector<std::vector<char> > vals(ncols);
+            std::vector<std::vector<double> > keys(ncols);
+            std::vector<std::vector<int64_t> > offs(ncols);
+            std::vector<std::vector<uint32_t> > bms(ncols);
+            int st = 0;
+            for (uint32_t c = 0; c < ncols; ++c) {
+                const uint32_t vt = rd32(), nrows = rd32();
+                vals[c].resize((size_t)nrows * 4 + 4);
+                if (nrows && fread(&vals[c][0], 4, nrows, fin) != nrows) exit(3);
+                const uint64_t nk = rd64();
+                keys[c].resize(nk ? nk : 1);
+                if (nk && fread(&keys[c][0], 8, nk, fin) != nk) exit(3);
+                const uint64_t no = rd64();
+                offs[c].resize(no ? no : 1);
+                if (no && fread(&offs[c][0], 8, no, fin) != no) exit(3);
+                const uint64_t nb = rd64();
+                bms[c].resize(nb ? nb : 1);
+                if (nb && fread(&bms[c][0], 4, nb, fin) != nb) exit(3);
+                char nm[16];
+                snprintf(nm, sizeof nm, "c%u", c);
+                const FastBitDataType dt = vt == 1 ? FastBitDataTypeUInt : vt == 2 ? FastBitDataTypeInt : FastBitDataTypeFloat;
+                if (fastbit_iapi_register_array(nm, dt, &vals[c][0], nrows) < 0) st = 1;
+                else if (fastbit_iapi_attach_full_index(nm, &keys[c][0], nk, &offs[c][0], no, &bms[c][0], nb) < 0) st = 2;
+            }
+            const uint32_t nq = rd32();
+            std::vector<std::vector<Term12> > qs(nq);
+            for (uint32_t q = 0; q < nq; ++q) {
+                const uint32_t nt = rd32();
+                for (uint32_t k = 0; k < nt; ++k) {
+                    Term12 t;
+                    t.col = rd32(); t.lo = rdf64(); t.hi = rdf64();
+                    qs[q].push_back(t);
+                }
+            }
+            const uint32_t rids = flags & 1u;
+            std::vector<uint64_t> counts(nq, 0);
+            std::vector<double> lat(nq, 0.0);
+            std::vector<std::vector<uint32_t> > ids(nq);
+            for (uint32_t q = 0; q < nq && st == 0; ++q) {
+                const double t0 = now_s();
+                const int64_t c = eval12(qs[q], rids, &ids[q]);
+                lat[q] = now_s() - t0;
+                if (c < 0) st = 3;
+                counts[q] = c < 0 ? 0 : (uint64_t)c;
+            }
+            double mx = 0;
+            if (st == 0 && reps > 0 && nth > 0) {
+                std::vector<Job12> jobs(nth);
+                std::vector<pthread_t> th(nth);
+                pthread_barrier_t bar;
+                pthread_barrier_init(&bar, 0, nth);
+                for (uint32_t t = 0; t < nth; ++t) {
+                    jobs[t].qs = &qs; jobs[t].tid = t; jobs[t].nth = nth; jobs[t].reps = reps;
+                    jobs[t].rids = rids; jobs[t].bar = &bar; jobs[t].secs = 0;
+                    pthread_create(&th[t], 0, job12, &jobs[t]);
+                }
+                for (uint32_t t = 0; t < nth; ++t) { pthread_join(th[t], 0); if (jobs[t].secs > mx) mx = jobs[t].secs; }
+                pthread_barrier_destroy(&bar);
+            }
+            wr32((uint32_t)st);
+            fwrite(&mx, 8, 1, fout);
+            for (uint32_t q = 0; q < nq; ++q) {
+                fwrite(&counts[q], 8, 1, fout);
+                fwrite(&lat[q], 8, 1, fout);
+                if (rids) wrv(ids[q]);
+            }
+            fastbit_iapi_free_all();
+        } else if (kind == 13) {
+            const uint32_t nth = rd32(), reps = rd32(), nrows = rd32();
+            ibis::array_t<uint32_t> vals(nrows);
+            for (uint32_t i = 0; i < nrows; ++i) vals[i] = rd32();
+            const uint32_t nq = rd32();
+            std::vector<double> lo(nq), hi(nq);
+            for (uint32_t q = 0; q < nq; ++q) { lo[q] = rdf64(); hi[q] = rdf64(); }
+            ibis::relic rel(0);
+            rel.construct(vals);
+            std::vector<uint64_t> counts(nq);
+            std::vector<uint32_t> rids;
+            for (uint32_t q = 0; q < nq; ++q) counts[q] = eval13(rel, lo[q], hi[q], rids);
+            double mx = 0;
+            if (nth > 0 && reps > 0) {
+                std::vector<Job13> jobs(nth);
+                std::vector<pthread_t> th(nth);
+                pthread_barrier_t bar;
+                pthread_barrier_init(&bar, 0, nth);
+                for (uint32_t t = 0; t < nth; ++t) {
+                    jobs[t].rel = &rel; jobs[t].lo = &lo; jobs[t].hi = &hi; jobs[t].tid = t; jobs[t].nth = nth;
+                    jobs[t].reps = reps; jobs[t].bar = &bar; jobs[t].secs = 0; jobs[t].sink = 0;
+                    pthread_create(&th[t], 0, job13, &jobs[t]);
+                }
+                for (uint32_t t = 0; t < nth; ++t) { pthread_join(th[t], 0); if (jobs[t].secs > mx) mx = jobs[t].secs; }
+                pthread_barrier_destroy(&bar);
+            }
+            fwrite(&mx, 8, 1, fout);
+            for (uint32_t q = 0; q < nq; ++q) fwrite(&counts[q], 8, 1, fout);
         } else if (kind == 10) {
             const uint32_t ik = rd32(), plen = rd32();
             std::vector<char> path(plen + 1, 0);

@@ -28,6 +28,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
@@ -72,6 +73,7 @@ private:
 class bitvector {
 public:
     typedef uint32_t word_t;
+    class indexSet;
 
     explicit bitvector(context& c = context::standard()) : ctx_(&c) { set(0, 0); }
     /* bitvector(const array_t<word_t>&): a serialized array (words, then the
@@ -80,6 +82,17 @@ public:
         upload(serialized.data(), serialized.size());
     }
     bitvector(const word_t* serialized, size_t n, context& c = context::standard()) : ctx_(&c) { upload(serialized, n); }
+    /* bitvector(const array_t<word_t>&) (src/bitvector.cpp:54): any
+     * contiguous array of serialized words with begin() and size() (FastBit's
+     * array_t, ...).  The reference shares the array's storage
+     * (array_t.h:104-107); here the words are copied to the device once, so
+     * the array may be released or changed afterwards. */
+    template <class Array, class = decltype(static_cast<const word_t*>(&*std::declval<const Array&>().begin())),
+              class = decltype(std::declval<const Array&>().size()),
+              class = typename std::enable_if<!std::is_same<Array, std::vector<word_t>>::value>::type>
+    explicit bitvector(const Array& arr, context& c = context::standard()) : ctx_(&c) {
+        upload(arr.size() ? &*arr.begin() : nullptr, arr.size());
+    }
     bitvector(const bitvector& o) : ctx_(o.ctx_) {
         std::vector<word_t> w;
         o.write(w);
@@ -125,13 +138,23 @@ public:
         release();
         upload(w.data(), w.size());
     }
-    /* adjustSize(nv, nt) (src/bitvector.cpp:4086-4108) when it grows the
-     * vector: bits up to position nv become 1, the rest up to nt become 0,
-     * through appendFill as in the reference.  Shrinking is not supported. */
+    /* adjustSize(nv, nt) (src/bitvector.cpp:4086-4108): growing, bits up to
+     * position nv become 1 and the rest up to nt 0, through appendFill as in
+     * the reference; shrinking keeps the first nt bits (erase(nt, size()),
+     * src/bitvector.cpp:1012-1036: the whole words before bit nt, then the
+     * covering word's leading part appended).  Construction-time, on the
+     * host. */
     void adjustSize(uint32_t nv, uint32_t nt) {
         const uint64_t sz = size();
         if (nt == sz) return;
-        if (nt < sz) throw error(WAHGPU_EINVAL, "adjustSize cannot shrink a vector here");
+        if (nt < sz) {
+            std::vector<word_t> w;
+            write(w);
+            truncate(w, nt);
+            release();
+            upload(w.data(), w.size());
+            return;
+        }
         if (nv > nt) nv = nt;
         if (nv > sz) {
             appendFill(1, (uint32_t)(nv - sz));
@@ -145,9 +168,22 @@ public:
         std::unique_ptr<bitvector> r(*this & mask);
         return r->cnt();
     }
+    /* setBit(i, val) (src/bitvector.cpp:621).  Past the end the bits are
+     * appended on the host; inside the vector the bit is OR'ed in (val 1)
+     * or cleared with - (val 0) on the device, with a one-bit operand of the
+     * same size.  The bits equal the reference's; the words are in
+     * compress() form. */
     void setBit(uint32_t i, int val) {
         const uint64_t n = size();
-        if (i < n) throw error(WAHGPU_EINVAL, "setBit inside the vector is not supported; append in row order");
+        if (i < n) {
+            std::vector<word_t> w{0u};
+            host_append(w, 0, i);
+            host_append(w, 1, 1);
+            host_append(w, 0, (uint32_t)(n - i - 1));
+            bitvector one(w, *ctx_);
+            if (val) *this |= one; else *this -= one;
+            return;
+        }
         std::vector<word_t> w;
         write(w);
         host_append(w, 0, (uint32_t)(i - n));
@@ -184,10 +220,41 @@ public:
     bitvector* operator^(const bitvector& b) const { return binary(WAHGPU_XOR, b); }
     bitvector* operator-(const bitvector& b) const { return binary(WAHGPU_MINUS, b); }
 
+    /* firstIndexSet() (src/bitvector.h:1253): the first set of 1-bit
+     * positions, walking a host copy of the words (see indexSet). */
+    inline indexSet firstIndexSet() const;
+
     wahgpu_bv* handle() const { return h_; }
     static bitvector adopt(wahgpu_bv* h, context& c) {
         bitvector b(c, h);
         return b;
+    }
+    /* The first nt bits of serialized words w (the leading part of
+     * erase(nt, size()), src/bitvector.cpp:1012-1036). */
+    static void truncate(std::vector<word_t>& w, uint32_t nt) {
+        uint32_t anb = w.back(), aval = 0;
+        w.pop_back();
+        if (anb) { aval = w.back(); w.pop_back(); }
+        std::vector<word_t> r{0u};
+        uint64_t pos = 0;
+        for (size_t k = 0; k < w.size() && pos < nt; ++k) {
+            const word_t x = w[k];
+            const uint64_t g = x > 0x7FFFFFFFu ? (x & 0x3FFFFFFFu) : 1u;
+            if (pos + 31 * g <= nt) {          // a whole word, kept verbatim
+                r.back() = x;
+                r.push_back(0u);
+                pos += 31 * g;
+            } else if (x > 0x7FFFFFFFu) {      // the covering fill's leading part
+                host_append(r, x >= 0xC0000000u ? 1 : 0, (uint32_t)(nt - pos));
+                pos = nt;
+            } else {                           // the covering literal's leading bits
+                const uint32_t k2 = (uint32_t)(nt - pos);
+                for (uint32_t b = 0; b < k2; ++b) host_append(r, (x >> (30u - b)) & 1u, 1);
+                pos = nt;
+            }
+        }
+        for (uint32_t b = 0; pos < nt && b < anb; ++b, ++pos) host_append(r, (aval >> (anb - 1u - b)) & 1u, 1);
+        w.swap(r);
     }
 
 private:
@@ -247,6 +314,89 @@ private:
     wahgpu_bv* h_ = nullptr;
 };
 
+/* ibis::bitvector::indexSet (src/bitvector.h:421-522; operator++,
+ * src/bitvector.cpp:4524-4590): the 1-bit positions one WAH word at a time.
+ * For a 1-fill (or an all-ones literal) isRange() is true and indices()
+ * holds [first, past-the-end); otherwise indices() holds the nIndices()
+ * positions of the word's 1 bits; 0-fills and zero literals are skipped and
+ * the active word comes last.  nIndices() == 0 marks the end.  The walk runs
+ * over a host copy of the serialized words taken by firstIndexSet();
+ * bitvector::rows() gives all positions at once from the GPU. */
+class bitvector::indexSet {
+public:
+    indexSet() {}
+    /* Over serialized words w (the write(array_t&) layout). */
+    explicit indexSet(std::shared_ptr<const std::vector<word_t>> w) : w_(std::move(w)) {
+        const std::vector<word_t>& v = *w_;
+        anb_ = v.empty() ? 0u : v.back();
+        if (anb_ >= 31u) anb_ = 0u;
+        aval_ = anb_ && v.size() >= 2 ? v[v.size() - 2] : 0u;
+        end_ = v.empty() ? 0u : v.size() - (anb_ ? 2u : 1u);
+        it_ = -1;
+        ind_[0] = 0xFFFFFFFFu;
+        nind_ = 0;
+        ++*this;
+    }
+    bool isRange() const { return nind_ >= 31u; }
+    const word_t* indices() const { return ind_; }
+    word_t nIndices() const { return nind_; }
+    indexSet& operator++() {
+        const int64_t end = (int64_t)end_;
+        if (it_ > end) { nind_ = 0; return *this; }
+        word_t index0 = ((ind_[0] + (nind_ > 31u ? nind_ : 31u)) / 31u) * 31u;
+        ++it_;
+        nind_ = 0;
+        const std::vector<word_t>& v = *w_;
+        while (it_ < end) {
+            const word_t x = v[(size_t)it_];
+            if (x >= 0xC0000000u) {               // 1-fill
+                nind_ = (x & 0x3FFFFFFFu) * 31u;
+                ind_[1] = index0 + nind_;
+                ind_[0] = index0;
+                return *this;
+            } else if (x >= 0x80000000u) {        // 0-fill
+                index0 += (x & 0x3FFFFFFFu) * 31u;
+                ++it_;
+            } else if (x > 0) {                   // non-zero literal
+                if (x < 0x7FFFFFFFu) {
+                    word_t i = 0, j = x << 1;
+                    for (; j > 0; ++i, j <<= 1)
+                        if (j > 0x7FFFFFFFu) ind_[nind_++] = index0 + i;
+                } else {
+                    nind_ = 31u;
+                    ind_[0] = index0;
+                    ind_[1] = index0 + 31u;
+                }
+                return *this;
+            } else {                              // zero literal
+                index0 += 31u;
+                ++it_;
+            }
+        }
+        if (anb_ > 0 && aval_ > 0) {
+            word_t i = 0, j = aval_ << (32u - anb_);
+            for (; j > 0; ++i, j <<= 1)
+                if (j > 0x7FFFFFFFu) ind_[nind_++] = index0 + i;
+        }
+        it_ = end + 1;
+        return *this;
+    }
+
+private:
+    std::shared_ptr<const std::vector<word_t>> w_;
+    int64_t it_ = 0;
+    size_t end_ = 0;
+    word_t anb_ = 0, aval_ = 0;
+    word_t nind_ = 0;
+    word_t ind_[32] = {0};
+};
+
+inline bitvector::indexSet bitvector::firstIndexSet() const {
+    auto w = std::make_shared<std::vector<word_t>>();
+    write(*w);
+    return indexSet(w);
+}
+
 /* ibis::qContinuousRange: lower lop x rop upper, compared in double. */
 struct qContinuousRange {
     enum COMPARE { OP_UNDEFINED = 0, OP_LT = 1, OP_LE = 2 };
@@ -276,10 +426,23 @@ public:
         hits = bitvector::adopt(h, *ctx_);
         return (long)n;
     }
-    /* estimate(expr) (src/index.h:196) — here exact. */
+    /* estimate(expr) (src/index.h:196): an upper bound of the hit count —
+     * relic: exact; bin: the 1 bits of the bins wholly inside and of the
+     * edge bins (src/ibin.cpp:6832-6889). */
     uint32_t estimate(const qContinuousRange& e) const {
         wahgpu_term t = term(e);
-        return (uint32_t)ctx_->check(wahgpu_evaluate(ctx_->get(), &t, 1, nullptr, 0, nullptr));
+        return (uint32_t)ctx_->check(wahgpu_estimate_count(ctx_->get(), &t));
+    }
+    /* estimate(expr, lower, upper) (src/index.h:191): lower = rows certainly
+     * hit, upper = a superset of the hits, empty when lower is exact (relic,
+     * src/irelic.h:58-62; bin, src/ibin.cpp:6722-6829). */
+    void estimate(const qContinuousRange& e, bitvector& lower, bitvector& upper) const {
+        wahgpu_term t = term(e);
+        wahgpu_bv* lo = nullptr;
+        wahgpu_bv* up = nullptr;
+        ctx_->check(wahgpu_estimate(ctx_->get(), &t, &lo, &up));
+        lower = bitvector::adopt(lo, *ctx_);
+        upper = bitvector::adopt(up, *ctx_);
     }
     wahgpu_term term(const qContinuousRange& e) const {
         wahgpu_term t;

@@ -101,6 +101,14 @@ int main(int argc, char** argv) {
         wr(out, (uint64_t)c);
         wr(out, ra.estimate(qContinuousRange(10, qContinuousRange::OP_LE, 20, qContinuousRange::OP_LT)));
         wrv(out, hits.rows());
+        // bin::estimate(expr, lower, upper) and estimate(expr)
+        const qContinuousRange eb(-0.5, qContinuousRange::OP_LE, 0.25, qContinuousRange::OP_LT);
+        bitvector lower, upper;
+        rb.estimate(eb, lower, upper);
+        wrv(out, lower.rows());
+        wr(out, upper.size());
+        wrv(out, upper.rows());
+        wr(out, rb.estimate(eb));
     }
     cudaFree(da);
     cudaFree(db);
@@ -119,6 +127,30 @@ int main(int argc, char** argv) {
             refused = e.code() == WAHGPU_EFORMAT ? 1 : 2;
         }
         wr(out, (uint64_t)refused);
+    }
+    // 5. a bitvector from an array-like of serialized words, setBit inside
+    //    the vector (set then clear), a shrinking adjustSize, and the
+    //    indexSet walk of the result
+    {
+        struct words {  // shaped like FastBit's array_t<uint32_t>
+            std::vector<uint32_t> v;
+            const uint32_t* begin() const { return v.data(); }
+            size_t size() const { return v.size(); }
+        } arr{rdv(in)};
+        const uint32_t set_at = rd(in), clear_at = rd(in), keep = rd(in);
+        bitvector b(arr);
+        b.setBit(set_at, 1);
+        b.setBit(clear_at, 0);
+        wrv(out, b.rows());
+        b.adjustSize(0, keep);
+        wr(out, b.size());
+        std::vector<uint32_t> pos;
+        for (bitvector::indexSet is = b.firstIndexSet(); is.nIndices() > 0; ++is) {
+            const uint32_t* ii = is.indices();
+            if (is.isRange()) for (uint32_t j = ii[0]; j < ii[1]; ++j) pos.push_back(j);
+            else for (uint32_t j = 0; j < is.nIndices(); ++j) pos.push_back(ii[j]);
+        }
+        wrv(out, pos);
     }
     return 0;
 }

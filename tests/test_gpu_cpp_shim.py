@@ -12,6 +12,7 @@ import pytest
 from conftest import load_golden, unpack
 from test_gpu_build import canonical_words
 import oracle
+from oracle import wahgen as G
 
 pytestmark = pytest.mark.gpu
 
@@ -85,6 +86,14 @@ def test_cpp_shim(gpu_ctx):
     data += struct.pack("<I", len(clauses))
     for c in clauses:
         data += _u32v([ord(ch) for ch in c])
+    # section 5: array-like constructor, setBit inside, shrinking adjustSize
+    arr = oracle.build_runs(G.geometric_runs(31, 20000, 0.2))
+    arr_bits = np.zeros(20000, bool)
+    arr_bits[oracle.rids(arr)] = True
+    set_at = int(np.flatnonzero(~arr_bits)[100])
+    clear_at = int(np.flatnonzero(arr_bits)[50])
+    keep = 12345
+    data += _u32v(arr) + struct.pack("<III", set_at, clear_at, keep)
     with tempfile.TemporaryDirectory() as td:
         exe = _build(td)
         fi, fo = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
@@ -118,9 +127,26 @@ def test_cpp_shim(gpu_ctx):
     m = (fa >= 10) & (fa < 20)
     assert R.u64() == m.sum() and R.u64() == m.sum()
     assert np.array_equal(R.vec(), np.flatnonzero(m))
+    # bin estimate: lower holds only hits, upper (or lower when upper is
+    # empty) holds every hit, and the count bound covers it
+    hits = set(np.flatnonzero((fb >= -0.5) & (fb < 0.25)).tolist())
+    lower = R.vec()
+    usize = R.u64()
+    upper = R.vec()
+    bound = R.u64()
+    assert set(lower.tolist()) <= hits
+    sup = set(upper.tolist()) if usize else set(lower.tolist())
+    assert hits <= sup and bound == len(sup)
     # relic read from the reference-written file; a bin file refused as relic
     rv = load_golden("idxfile_inputs.npz")["relic_vals"].astype(np.float64)
     m = (rv >= 10) & (rv < 30)
     assert R.u64() == m.sum()
     assert np.array_equal(R.vec(), np.flatnonzero(m))
     assert R.u64() == 1
+    # array-like constructor, setBit inside the vector, shrinking adjustSize
+    bits = arr_bits.copy()
+    bits[set_at] = True
+    bits[clear_at] = False
+    assert np.array_equal(R.vec(), np.flatnonzero(bits))
+    assert R.u64() == keep
+    assert np.array_equal(R.vec(), np.flatnonzero(bits[:keep]))

@@ -236,8 +236,8 @@ def main():
                     help="ROWS:QUERIES — only the binned range case at that size, tile-major count batch run "
                          "warmup+steps times (for ncu)")
     ap.add_argument("--workloads", default=None,
-                    help="comma list of range workloads to add to the line: range,batched,served "
-                         "(default: all three on one GPU, none under torchrun)")
+                    help="comma list of range workloads to add to the line: relic,range,batched,served "
+                         "(default: all four on one GPU, none under torchrun; 'none' for none)")
     ap.add_argument("--only", default=None,
                     help="OP:DENSITY, e.g. '&:0.5' — one operator on one pair, no e2e / CPU legs (for ncu)")
     args = ap.parse_args()
@@ -460,10 +460,14 @@ def main():
                    "kind": "port", "sample": "1 pass of the 20 operator calls (C oracle)"}
 
     extra = {}
-    which = (args.workloads.split(",") if args.workloads else (["range", "batched", "served"] if world == 1 else []))
-    which = [w for w in which if w]
+    which = (args.workloads.split(",") if args.workloads is not None
+             else (["relic", "range", "batched", "served"] if world == 1 else []))
+    which = [w for w in which if w and w != "none"]
+    if "relic" in which and rank == 0:
+        extra["relic"] = relic_workload(args, ctx, stream, peak)
+    which = [w for w in which if w != "relic"]
     if which and rank == 0:
-        extra = range_workloads(args, ctx, stream, peak, which)
+        extra.update(range_workloads(args, ctx, stream, peak, which))
 
     if world > 1:
         dist.barrier()
@@ -575,6 +579,7 @@ def _batched_vs_single(L, tune, ctx, stream, queries, nsingle, peak):
     counts = B.counts()
     del g
     nbytes = B.nbytes()
+    mbytes = B.min_bytes()
     ctx.set_tuning(L.TUNE_RANGE_ORDER, 1)
     ctx.set_tuning(L.TUNE_RANGE_CTAS, 0)
     singles = [L.Batch(ctx, [q], 0) for q in queries[:nsingle]]
@@ -587,6 +592,7 @@ def _batched_vs_single(L, tune, ctx, stream, queries, nsingle, peak):
         b.close()
     B.close()
     gbs = nbytes / (ms / 1e3) / 1e9
+    gbs_min = mbytes / (ms / 1e3) / 1e9
     return {
         "queries": len(queries), "queries_per_s": len(queries) / (ms / 1e3), "ms_per_batch": ms,
         "one_query_per_launch_queries_per_s": nsingle / (ms1 / 1e3), "one_query_per_launch_sample": nsingle,
@@ -595,12 +601,182 @@ def _batched_vs_single(L, tune, ctx, stream, queries, nsingle, peak):
                   "candidates_ms": {f"{_ORDER_NAMES[k[0]]}/ctas={k[1] or 'max'}": round(v, 2)
                                     for k, v in table.items()}},
         "algorithmic_bytes_per_batch": nbytes, "achieved_GBps": gbs, "frac_of_hbm_peak": gbs / peak,
+        "sumbins_bytes_per_batch": mbytes, "sumbins_GBps": gbs_min, "sumbins_frac_of_hbm_peak": gbs_min / peak,
+        "bytes_note": "algorithmic = what this kernel reads (cumulative rows, other bitmaps, edge bitmaps and "
+                      "rows, 8 per count); sumbins = what the reference's sumBins must read (the covered bitmaps "
+                      "or their complement, edge bitmaps and rows, 8 per count)",
         "avg_hits": float(np.mean(counts)),
         "_counts": counts,
         "cuda_graph": True,
         "timing": "CUDA events on the batch stream: 2 replays of the captured fused launch; singles launched "
                   "directly",
     }
+
+
+def _ev_time_each(stream, fn, reps, flush):
+    """Device time (ms) of each of `reps` runs of fn, L2 flushed before each."""
+    import torch
+    ts = []
+    for _ in range(reps):
+        flush()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return ts
+
+
+def relic_workload(args, ctx, stream, peak):
+    """The relic workload: ibis::relic over a 1,000,000-row uint32 column
+    with values uniform in [0,100), 100 ranges lo <= x < hi (lo, hi uniform
+    in [0,100], lo < hi); hit count and ascending row ids of every query.
+    The index is the reference's own (relic::construct, through the
+    reference driver) when the reference build is present, else built on
+    the GPU; the GPU's counts equal the reference's relic::evaluate and its
+    row ids a scan of the column."""
+    import ctypes
+    import torch
+    import libfastlib_b200 as L
+    from oracle import reference as R
+    n = 1_000_000
+    rng = np.random.Generator(np.random.PCG64(42))
+    vals = rng.integers(0, 100, size=n).astype(np.uint32)
+    qrng = np.random.Generator(np.random.PCG64(7))
+    qs = []
+    while len(qs) < 100:
+        lo, hi = (int(v) for v in qrng.integers(0, 101, size=2))
+        if lo < hi:
+            qs.append((float(lo), float(hi)))
+    have_ref = R.available()
+    if have_ref:
+        keys, offs, bms = R.relic_triple(vals)
+        idx = L.Index(ctx, L.RELIC, n, keys, offs, bms, values=vals)
+        source = "the reference's relic::construct (reference driver), attached as its (keys, offsets, bitmaps) triple"
+    else:
+        idx = L.Index.build(ctx, L.RELIC, vals)
+        source = "built on the GPU (reference build absent)"
+    queries = [[idx.term(lo, hi)] for lo, hi in qs]
+    C = L.Batch(ctx, queries, 0)
+    C.run()
+    counts = [int(c) for c in C.counts()]
+    C.close()
+    total = sum(counts)
+    B = L.Batch(ctx, queries, rid_cap=total)
+    for _ in range(args.warmup):
+        B.run()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        B.run()
+    g.replay()
+    torch.cuda.synchronize()
+    flushbuf = torch.zeros(64 << 20, dtype=torch.int32, device=f"cuda:{ctx.device}")  # 256 MB > L2
+    reps = max(5, min(args.steps, 50))
+    ts = _ev_time_each(stream, g.replay, reps, lambda: flushbuf.add_(1))
+    ms = float(np.median(ts))
+    del g
+    assert [int(c) for c in B.counts()] == counts, "relic batch counts changed between runs"
+    for q in (0, 1, len(qs) // 2, len(qs) - 1):
+        lo, hi = qs[q]
+        want = np.flatnonzero((vals >= lo) & (vals < hi)).astype(np.uint32)
+        assert np.array_equal(B.rids(q, counts[q]), want), f"relic row ids of query {q} differ from a scan"
+    parity = {"counts_equal_reference": None, "row_ids_equal_scan_queries": 4}
+    cpu = None
+    if have_ref:
+        nth = os.cpu_count() or 1
+        # about 5 s of one-thread host work, sized by a one-pass probe; the
+        # reference's counts must equal the GPU's
+        s1, ref_counts = R.relic_timed(vals, qs, nthreads=1, reps=1)
+        assert ref_counts == counts, "relic counts differ from the reference's relic::evaluate"
+        parity["counts_equal_reference"] = True
+        reps1 = max(1, int(5.0 / max(s1, 1e-3)))
+        s1, _ = R.relic_timed(vals, qs, nthreads=1, reps=reps1)
+        repsp = max(1, reps1 * nth // 2)
+        sp, _ = R.relic_timed(vals, qs, nthreads=nth, reps=repsp)
+        cpu = {"value": len(qs) * repsp / sp, "unit": "queries/s", "cores": nth, "kind": "reference",
+               "sample": f"{repsp} passes of the 100 queries on {nth} threads (relic::evaluate + firstIndexSet "
+                         "row-id walk, the reference built from source)",
+               "one_thread_queries_per_s": len(qs) * reps1 / s1,
+               "one_thread_ms_per_query": 1e3 * s1 / (len(qs) * reps1)}
+    # one query per launch
+    singles = [L.Batch(ctx, [q], rid_cap=max(c, 1)) for q, c in zip(queries, counts)]
+    for b in singles[:4]:
+        b.run()
+    ms1 = float(np.median(_ev_time_each(stream, lambda: [b.run() for b in singles], 3, lambda: flushbuf.add_(1))))
+    for b in singles:
+        b.close()
+    # end to end through the C ABI: the batch run, then its counts and every
+    # query's row ids read into pinned host memory
+    pinned = torch.empty(max(total, 1), dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+    cnt_host = torch.empty(len(qs), dtype=torch.int64).pin_memory().numpy().view(np.uint64)
+    lib = ctx.lib
+    starts = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    U32P = ctypes.POINTER(ctypes.c_uint32)
+
+    def e2e():
+        B.run()
+        ctx.check(lib.wahgpu_batch_counts(B.h, cnt_host.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+        for q in range(len(qs)):
+            ctx.check(lib.wahgpu_batch_rids(B.h, q, pinned[starts[q]:].ctypes.data_as(U32P), int(counts[q])))
+
+    e2e()
+    assert [int(c) for c in cnt_host] == counts
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e_reps = 5
+    for _ in range(e_reps):
+        e2e()
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / e_reps
+    mb = B.min_bytes() + 4 * total
+    gbs = mb / (ms / 1e3) / 1e9
+    out = {
+        "workload": "relic: ibis::relic over 1,000,000 uint32 rows uniform in [0,100), 100 ranges lo <= x < hi "
+                    "(seeded); hit counts and ascending row ids of every query, one fused launch (CUDA graph)",
+        "index_source": source,
+        "queries": len(qs), "row_ids": total,
+        "queries_per_s": len(qs) / (ms / 1e3), "ms_per_batch": ms,
+        "one_query_per_launch_queries_per_s": len(qs) / (ms1 / 1e3),
+        "e2e": {"value": len(qs) / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 4 * total + 8 * len(qs),
+                "timing": "wall clock, device synchronized: batch run, counts and all row ids read into pinned "
+                          "host memory through the C ABI (the index stays resident; terms are passed by value)"},
+        "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                     "bytes": "bitmaps sumBins reads (covered set or complement) + 8 per count + 4 per row id"},
+        "l2": "a 256 MB buffer is overwritten before each timed batch (the index, ~4 MB, would stay in L2)",
+        "parity": parity,
+        "cpu_baseline": cpu,
+    }
+    B.close()
+    idx.close()
+    return out
+
+
+def _reference_leg(columns, queries, gpu_counts, label, scale=1.0):
+    """The reference's in-memory C API on the GPU-built indexes' triples
+    (the same bitmaps on both sides): its counts for the sample must equal
+    the GPU's; timed on every host core (one pass after an untimed
+    one-thread pass, whose per-query times give the one-thread latency).
+    `scale` multiplies times when the sample covers one row partition of
+    the workload (the reference evaluates a partitioned table one partition
+    after another)."""
+    from oracle import reference as R
+    if not R.available():
+        return {"unavailable": "reference build (oracle/_ref) absent"}
+    nth = os.cpu_count() or 1
+    secs, counts, _ = R.iapi_queries(columns, queries, nthreads=nth, reps=1)
+    lat = np.array(R.latencies()) * scale
+    if gpu_counts is not None:
+        assert [int(c) for c in counts] == [int(c) for c in gpu_counts], f"{label}: counts differ from the reference's"
+    return {"value": len(queries) / (secs * scale), "unit": "queries/s", "cores": nth, "kind": "reference",
+            "sample": label,
+            "one_thread_p50_ms": float(np.percentile(lat, 50) * 1e3),
+            "one_thread_p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "one_thread_queries_per_s": float(len(lat) / lat.sum()) if lat.sum() > 0 else None,
+            "path": "fastbit_iapi_register_array + fastbit_iapi_attach_full_index, then per query "
+                    "fastbit_selection_osr/combine/evaluate (the reference built from source)"}
 
 
 def range_workloads(args, ctx, stream, peak, which):
@@ -618,7 +794,14 @@ def range_workloads(args, ctx, stream, peak, which):
         keys, nobs = idx.keys(), idx.nbitmaps()
         qs = W.binned_range_queries(5, keys, nobs, 1000, 500)
         r = _batched_vs_single(L, tune, ctx, stream, [[idx.term(lo, hi)] for lo, hi in qs], 1000, peak)
-        r.pop("_counts")
+        counts = r.pop("_counts")
+        sample = list(range(0, 1000, 21))
+        vals = col.cpu().numpy()
+        r["cpu_baseline"] = _reference_leg(
+            [(vals, idx.deconstruct())], [[(0, *qs[q])] for q in sample], [counts[q] for q in sample],
+            f"{len(sample)} of the 1000 queries on the same 100M-row index")
+        r["parity"] = {"reference_counts_equal_on_sample": r["cpu_baseline"].get("kind") == "reference"}
+        del vals
         r.update({"workload": "binned range: bin index (1000 equal-weight bins, built on the GPU) over 100M "
                               "float32 rows (70% Normal(0,1), 30% Zipf(1.2) over 1e5 ranks); 1000 queries "
                               "lo <= x < hi spanning 1..500 bins, both ends inside edge bins (row checks); "
@@ -629,24 +812,40 @@ def range_workloads(args, ctx, stream, peak, which):
         del col
     if "batched" in which:
         n = 50_000_000
-        cols, metas = [], []
+        cols, metas, host_cols = [], [], []
         t0 = time.perf_counter()
         for c in range(3):
-            cols.append(L.Index.build(ctx, L.RELIC, W.uniform_int_column(40 + c, n, 1000)))
+            v = W.uniform_int_column(40 + c, n, 1000)
+            cols.append(L.Index.build(ctx, L.RELIC, v))
             metas.append({"kind": "relic", "card": 1000})
+            host_cols.append(v.cpu().numpy())
         for c in range(3):
-            cols.append(L.Index.build(ctx, L.RELIC, W.zipf_column(50 + c, n, 1.1, 1_000_000).to(torch.int32)))
+            v = W.zipf_column(50 + c, n, 1.1, 1_000_000).to(torch.int32)
+            cols.append(L.Index.build(ctx, L.RELIC, v))
             metas.append({"kind": "relic", "card": 1_000_000})
+            host_cols.append(v.cpu().numpy())
         for c in range(2):
-            ix = L.Index.build(ctx, L.BIN, W.normal_column(60 + c, n), nbins=512)
+            v = W.normal_column(60 + c, n)
+            ix = L.Index.build(ctx, L.BIN, v, nbins=512)
             cols.append(ix)
             metas.append({"kind": "bin", "keys": ix.keys(), "nobs": ix.nbitmaps(), "max_span": 256})
+            host_cols.append(v.cpu().numpy())
+        del v
         build_s = time.perf_counter() - t0
         qs = W.conjunctive_queries(4, metas, 4096, max_terms=4)
         queries = [[cols[c].term(lo, hi) for c, lo, hi in q] for q in qs]
         r = _batched_vs_single(L, tune, ctx, stream, queries, 512, peak)
         counts = r.pop("_counts")
         r["with_row_ids"] = _with_row_ids(L, tune, ctx, stream, queries[:256], counts[:256])
+        sample = list(range(0, 4096, 85))
+        used = sorted({c for q in sample for c, _, _ in qs[q]})
+        pos = {c: k for k, c in enumerate(used)}
+        r["cpu_baseline"] = _reference_leg(
+            [(host_cols[c], cols[c].deconstruct()) for c in used],
+            [[(pos[c], lo, hi) for c, lo, hi in qs[q]] for q in sample], [counts[q] for q in sample],
+            f"{len(sample)} of the 4096 queries on the same 8 x 50M-row indexes")
+        r["parity"] = {"reference_counts_equal_on_sample": r["cpu_baseline"].get("kind") == "reference"}
+        del host_cols
         r.update({"workload": "batched conjunctive: 8 columns x 50M rows (3 uint32 U{0..999} relic, 3 uint32 "
                               "Zipf(1.1) over 1e6 relic, 2 float32 Normal bin 512), 4096 WHERE clauses of 1-4 "
                               "column ranges of uneven span; one persistent fused launch vs one query per launch",

@@ -15,8 +15,10 @@
 //   4. per unit, the WAH words it emits — the zero groups before it as one
 //      fill (or a literal 0 for a single group), then its literal, runs of
 //      all-1 groups as one fill — counted, scanned and written.
-// The words are in compress() form; the bits of every bitmap are exactly the
-// reference's.
+// The words are in compress() form, then heavy bitmaps are decompressed as
+// the reference's optionalUnpack does by default (k_unpack_bitmaps), so a
+// relic index's words equal relic::construct's; the bits of every bitmap are
+// exactly the reference's.
 #define WAH_RANGE_TYPES_ONLY
 #include "../../include/wahgpu.h"
 #include "wah_api_internal.h"
@@ -141,6 +143,49 @@ __global__ void k_write_words(const uint32_t* __restrict__ u_seg, const uint32_t
 }
 
 // bin of every row: the last bin whose smallest value is <= the row's value
+// index::optionalUnpack (src/index.cpp:8730-8856) with no index option and
+// no parameter set — what relic::construct and bin::binning do by default:
+// a bitmap whose bytes() (m_vec words * 4 + sizeof(ibis::bitvector), 40 on
+// LP64) exceed max(nrows / 9, sizeof(ibis::bitvector) + 12) is decompressed,
+// every fill becoming its literals.  One warp per bitmap copies its words
+// from the old pool to the new one, or expands them (fills of more than 32
+// groups by the whole warp).
+constexpr uint64_t REF_BITVECTOR_BYTES = 40;
+__global__ void k_unpack_bitmaps(const uint32_t* __restrict__ src, const BitmapMeta* __restrict__ old_bm,
+                                 const BitmapMeta* __restrict__ new_bm, uint32_t nobs, uint32_t* __restrict__ dst) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (b >= nobs) return;
+    const BitmapMeta mo = old_bm[b], mn = new_bm[b];
+    const uint32_t* w = src + mo.wstart;
+    uint32_t* d = dst + mn.wstart;
+    if (mn.n == mo.n) {  // kept as it is
+        for (uint32_t i = lane; i < mo.n; i += 32) d[i] = __ldg(w + i);
+        return;
+    }
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < mo.n; base += 32) {
+        const uint32_t i = base + lane;
+        const bool in = i < mo.n;
+        const uint32_t wd = in ? __ldg(w + i) : 0u;
+        const uint32_t c = in ? wgroups(wd) : 0u;
+        uint32_t x = c;
+#pragma unroll
+        for (int k = 1; k < 32; k <<= 1) { uint32_t t = __shfl_up_sync(0xffffffffu, x, k); if (lane >= (uint32_t)k) x += t; }
+        const uint32_t p = carry + x - c;
+        if (in && c <= 32u) for (uint32_t g = 0; g < c; ++g) d[p + g] = wpattern(wd);
+        uint32_t f = __ballot_sync(0xffffffffu, in && c > 32u);
+        while (f) {
+            const uint32_t s = __ffs(f) - 1u;
+            f &= f - 1u;
+            const uint32_t fp = __shfl_sync(0xffffffffu, p, s), fc = __shfl_sync(0xffffffffu, c, s);
+            const uint32_t pat = __shfl_sync(0xffffffffu, wpattern(wd), s);
+            for (uint32_t g = lane; g < fc; g += 32u) d[fp + g] = pat;
+        }
+        carry += __shfl_sync(0xffffffffu, x, 31);
+    }
+}
+
 template <typename K>
 __global__ void k_bin_of(const K* __restrict__ vals, uint32_t n, const K* __restrict__ bmin, uint32_t nb,
                          uint32_t* __restrict__ bin) {
@@ -322,6 +367,39 @@ int build_typed(wahgpu_ctx* ctx, int kind, int vtype, const K* dvals, uint32_t n
     std::vector<BitmapMeta> hb(nobs);
     BTRY(cudaMemcpyAsync(hb.data(), x->d_bm, (size_t)nobs * sizeof(BitmapMeta), cudaMemcpyDeviceToHost, st));
     BTRY(cudaStreamSynchronize(st));
+    // optionalUnpack's default rule: heavy bitmaps decompressed
+    {
+        const uint64_t bar = std::max<uint64_t>(n / 9, REF_BITVECTOR_BYTES + 12);
+        std::vector<BitmapMeta> nb = hb;
+        uint64_t pos = 0;
+        bool any = false;
+        for (uint32_t j = 0; j < nobs; ++j) {
+            const bool heavy = (uint64_t)hb[j].n * 4 + REF_BITVECTOR_BYTES > bar && hb[j].n != G;
+            nb[j].wstart = pos;
+            nb[j].n = heavy ? G : hb[j].n;
+            pos += nb[j].n;
+            any |= heavy;
+        }
+        if (any) {
+            uint32_t* nw = static_cast<uint32_t*>(wg_alloc(ctx, std::max<uint64_t>(pos, 1) * 4));
+            BitmapMeta* nbm = static_cast<BitmapMeta*>(wg_alloc(ctx, std::max<size_t>(nobs, 1) * sizeof(BitmapMeta)));
+            if (!nw || !nbm) {
+                wg_free(ctx, nw); wg_free(ctx, nbm);
+                wahgpu_index_free(x);
+                return wg_fail(ctx, WAHGPU_ENOMEM, "index build: device allocation failed (unpacking heavy bitmaps)");
+            }
+            BTRY(cudaMemcpyAsync(nbm, nb.data(), (size_t)nobs * sizeof(BitmapMeta), cudaMemcpyHostToDevice, st));
+            k_unpack_bitmaps<<<nblocks((uint64_t)nobs * 32), BT, 0, st>>>(x->d_words, x->d_bm, nbm, nobs, nw);
+            ctx->launches++;
+            BTRY(cudaGetLastError());
+            BTRY(cudaStreamSynchronize(st));  // nb (host) staged above must outlive the copy
+            wg_free(ctx, x->d_words);
+            wg_free(ctx, x->d_bm);
+            x->d_words = nw;
+            x->d_bm = nbm;
+            hb = nb;
+        }
+    }
     x->bwords.resize(nobs);
     for (uint32_t j = 0; j < nobs; ++j) x->bwords[j] = hb[j].n;
     int rc = wg_index_attach(x);

@@ -43,6 +43,27 @@ def canonical_words(rows, nrows):
     return np.array(out, dtype=np.uint32)
 
 
+def unpacked_words(words, nrows):
+    """index::optionalUnpack's default rule (src/index.cpp:8838-8853) on a
+    serialized bitvector of nrows rows: when m_vec's bytes plus
+    sizeof(ibis::bitvector) (40) exceed max(nrows / 9, 52), every fill
+    becomes its literals."""
+    w = np.asarray(words, np.uint32)
+    tail = w[-2:] if 0 < w[-1] < 31 else w[-1:]
+    body = w[: len(w) - len(tail)]
+    G = nrows // 31
+    if len(body) * 4 + 40 <= max(nrows // 9, 52) or len(body) == G:
+        return w
+    out = []
+    for x in body:
+        x = int(x)
+        if x > ALL:
+            out.extend([ALL if x >= 0xC0000000 else 0] * (x & 0x3FFFFFFF))
+        else:
+            out.append(x)
+    return np.concatenate([np.asarray(out, np.uint32), tail])
+
+
 @pytest.mark.parametrize("nrows", [1, 30, 31, 62, 1000, 100003])
 def test_relic_build_bitmaps(gpu_ctx, nrows):
     import libfastlib_b200 as L
@@ -60,7 +81,7 @@ def test_relic_build_bitmaps(gpu_ctx, nrows):
         rows = np.flatnonzero(vals == v).astype(np.uint32)
         bv = idx.bitmap(j)
         assert np.array_equal(bv.rids(), rows), v
-        assert np.array_equal(bv.write(), canonical_words(rows, nrows)), v
+        assert np.array_equal(bv.write(), unpacked_words(canonical_words(rows, nrows), nrows)), v
         assert bv.cnt() == len(rows)
 
 
@@ -112,3 +133,23 @@ def test_built_indexes_answer_like_reference(gpu_ctx):
     for q, (lo, hi) in enumerate(queries):
         c, rids, _ = L.evaluate(gpu_ctx, [bidx.term(lo, hi)])
         assert c == ref[q][0] and np.array_equal(rids, ref[q][1]), q
+
+
+@pytest.mark.parametrize("card,nrows", [(100, 1_000_000), (7, 99_999), (1000, 200_000), (3, 310_001)])
+def test_relic_build_equals_relic_construct(gpu_ctx, card, nrows):
+    """The device-built relic index is word for word the reference's
+    relic::construct (src/irelic.cpp:879-925: mapValues, then
+    optionalUnpack's default decompression of heavy bitmaps): the same
+    keys, offsets and serialized bitmaps as relic::write(keys, offs, bms)."""
+    import libfastlib_b200 as L
+    from oracle import reference as R
+    if not R.available():
+        pytest.skip("reference build (oracle/_ref) absent")
+    rng = np.random.default_rng(card)
+    vals = rng.integers(0, card, size=nrows).astype(np.uint32)
+    keys, offs, bms = R.relic_triple(vals)
+    idx = L.Index.build(gpu_ctx, L.RELIC, vals)
+    k, o, b = idx.deconstruct()
+    assert np.array_equal(k, keys)
+    assert np.array_equal(o, offs)
+    assert np.array_equal(b, bms)

@@ -198,6 +198,16 @@ int wg_index_attach(wahgpu_index* x) {
         x->cum_words[j + 1] = x->cum_words[j] + x->bwords[j];
         x->cum_ones[j + 1] = x->cum_ones[j] + x->bones[j];
     }
+    if (x->kind == WAHGPU_BIN) {
+        x->nonempty.clear();
+        x->bins_sorted = true;
+        for (uint32_t j = 0; j < nobs; ++j) {
+            const double mn = x->keys[j], mx = x->keys[nobs + j];
+            if (x->bones[j] == 0 || !(mn <= mx)) continue;
+            if (!x->nonempty.empty() && !(x->keys[nobs + x->nonempty.back()] < mn)) x->bins_sorted = false;
+            x->nonempty.push_back(j);
+        }
+    }
     x->dev.words = x->d_words; x->dev.bm = x->d_bm; x->dev.tiles = x->d_tiles;
     x->dev.tl_off = x->d_tl_off; x->dev.tl_bm = x->d_tl_bm;
     x->dev.cum = x->d_cum; x->dev.cum_stride = x->cum_stride; x->dev.cum_k = x->cum_k;
@@ -282,6 +292,32 @@ static int locate(wahgpu_ctx* ctx, const wahgpu_index* x, const wahgpu_term* t, 
         if (t->rop == 1) b = (uint32_t)(std::lower_bound(k.begin(), k.end(), t->hi) - k.begin());
         else if (t->rop == 2) b = (uint32_t)(std::upper_bound(k.begin(), k.end(), t->hi) - k.begin());
         if (b > a) { h0 = a; h1 = b; }
+    } else if (x->bins_sorted) {
+        // bins ordered and disjoint: every test below is monotone in the bin
+        // order, so binary searches over the bins holding rows find the
+        // bins wholly inside and the (at most two) straddling ones
+        const auto& ne = x->nonempty;
+        const uint32_t nb = x->nobs, m = (uint32_t)ne.size();
+        auto mn = [&](uint32_t i) { return x->keys[ne[i]]; };
+        auto mx = [&](uint32_t i) { return x->keys[nb + ne[i]]; };
+        auto low = [&](double v) { return t->lop == 0 || (t->lop == 1 ? t->lo < v : t->lo <= v); };
+        auto high = [&](double v) { return t->rop == 0 || (t->rop == 1 ? v < t->hi : v <= t->hi); };
+        auto first = [&](auto pred) {  // first i with pred(i), pred monotone false..true
+            uint32_t lo = 0, hi = m;
+            while (lo < hi) { const uint32_t md = (lo + hi) / 2; if (pred(md)) hi = md; else lo = md + 1; }
+            return lo;
+        };
+        const uint32_t P = first([&](uint32_t i) { return low(mx(i)); });        // some value passes the lower side
+        const uint32_t Q = first([&](uint32_t i) { return !high(mn(i)); });      // [P, Q): some value passes both
+        const uint32_t I0 = first([&](uint32_t i) { return low(mn(i)); });       // every value passes the lower side
+        const uint32_t I1 = first([&](uint32_t i) { return !high(mx(i)); });     // [.., I1): every value passes the upper
+        const uint32_t a = std::max(P, I0), b = std::min(Q, I1);
+        if (b > a) { h0 = ne[a]; h1 = ne[b - 1] + 1; }
+        for (uint32_t i = P; i < Q; ++i) {
+            if (i >= a && i < b) { i = b - 1; continue; }
+            if (nc >= 2) return wg_fail(ctx, WAHGPU_EINVAL, "more than two bins straddle the range");
+            out.cand[nc++] = ne[i];
+        }
     } else {
         std::vector<uint8_t> cls(x->nobs);  // 0 none, 1 all, 2 some
         for (uint32_t j = 0; j < x->nobs; ++j) {

@@ -15,6 +15,10 @@ struct wahgpu_index {
     std::vector<uint64_t> bwords; // m_vec words per bitmap (for the complement choice)
     std::vector<uint32_t> bones;  // 1 bits per bitmap
     std::vector<uint64_t> cum_words, cum_ones;  // prefix sums of bwords / bones
+    // bin: the bins holding rows, in bitmap order, and whether their
+    // [minval, maxval] are ordered and disjoint (then locate searches them)
+    std::vector<uint32_t> nonempty;
+    bool bins_sorted = false;
     uint32_t* d_words = nullptr;
     wah::BitmapMeta* d_bm = nullptr;
     uint32_t* d_tiles = nullptr;

@@ -273,6 +273,15 @@ int64_t wahgpu_evaluate(wahgpu_ctx* ctx, const wahgpu_term* terms, uint32_t nter
  * back to back in device memory, rid_cap == 0 counts only. */
 int wahgpu_batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, const uint32_t* query_offsets,
                         uint32_t nq, uint64_t rid_cap, int dense_first, wahgpu_batch** out);
+/* Like wahgpu_batch_create with row ids, but each query keeps at most
+ * rid_caps[q] of its row ids (the first ones, ascending — a LIMIT), in a
+ * region of its own, so one query with many hits cannot crowd out the
+ * others (no counterpart in the reference, whose getHitRows returns all
+ * rows, src/countQuery.cpp:387-410).  Counts are always complete;
+ * wahgpu_batch_rids returns min(count, rid_caps[q]) ids.  Runs query by
+ * query. */
+int wahgpu_batch_create_capped(wahgpu_ctx* ctx, const wahgpu_term* terms, const uint32_t* query_offsets,
+                               uint32_t nq, const uint64_t* rid_caps, wahgpu_batch** out);
 int wahgpu_batch_run(wahgpu_batch* batch);
 int wahgpu_batch_counts(wahgpu_batch* batch, uint64_t* counts);
 int64_t wahgpu_batch_rids(wahgpu_batch* batch, uint32_t q, uint32_t* out, uint64_t cap);
@@ -304,7 +313,8 @@ int wahgpu_server_create(wahgpu_ctx* ctx, uint32_t nslots, uint32_t max_batch, u
                          wahgpu_server** out);
 /* Queues one query (its terms are copied); returns a request id > 0, or
  * WAHGPU_EBUSY when the query's scratch alone exceeds the budget.  rid_cap
- * > 0 asks for up to rid_cap row ids. */
+ * > 0 asks for its first rid_cap row ids (ascending, like a LIMIT); its
+ * count is always complete. */
 int64_t wahgpu_server_submit(wahgpu_server* s, const wahgpu_term* terms, uint32_t nterms, uint64_t rid_cap);
 /* Waits for a request: hit count, row ids (if asked for), latency in
  * seconds from submit to answer; returns the number of row ids written. */
@@ -312,10 +322,13 @@ int64_t wahgpu_server_wait(wahgpu_server* s, int64_t id, uint64_t* count, uint32
                            double* latency_s);
 /* Open-loop replay: query q = terms[qoff[q], qoff[q+1]) arrives arrival_s[q]
  * seconds after the call starts; waits for all; counts and latencies
- * (scheduled arrival to answer) per query; returns the wall time in
- * microseconds. */
+ * (scheduled arrival to answer) per query; with rid_cap > 0 every query also
+ * returns its first rid_cap row ids, written to rids + q * rid_cap (when
+ * rids is non-NULL) with their number in nrids[q].  Returns the wall time
+ * in microseconds. */
 int64_t wahgpu_server_replay(wahgpu_server* s, const wahgpu_term* terms, const uint32_t* qoff, uint32_t nq,
-                             const double* arrival_s, uint64_t* counts, double* latency_s);
+                             const double* arrival_s, uint64_t rid_cap, uint64_t* counts, double* latency_s,
+                             uint32_t* rids, uint64_t* nrids);
 int wahgpu_server_stats(wahgpu_server* s, uint64_t* batches, uint64_t* served);
 int wahgpu_server_free(wahgpu_server* s);
 

@@ -136,14 +136,18 @@ def load_library(path: Optional[str] = None) -> ctypes.CDLL:
         "wahgpu_batch_device_rids": (P, [P]),
         "wahgpu_batch_free": (ctypes.c_int, [P]),
         "wahgpu_batch_bytes": (ctypes.c_int64, [P]),
+        "wahgpu_batch_create_capped": (ctypes.c_int, [P, ctypes.POINTER(_Term), ctypes.POINTER(ctypes.c_uint32),
+                                                      ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64),
+                                                      ctypes.POINTER(P)]),
         "wahgpu_batch_min_bytes": (ctypes.c_int64, [P]),
         "wahgpu_server_create": (ctypes.c_int, [P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(P)]),
         "wahgpu_server_submit": (ctypes.c_int64, [P, ctypes.POINTER(_Term), ctypes.c_uint32, ctypes.c_uint64]),
         "wahgpu_server_wait": (ctypes.c_int64, [P, ctypes.c_int64, ctypes.POINTER(ctypes.c_uint64), U32P,
                                                  ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)]),
         "wahgpu_server_replay": (ctypes.c_int64, [P, ctypes.POINTER(_Term), U32P, ctypes.c_uint32,
-                                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64),
-                                                   ctypes.POINTER(ctypes.c_double)]),
+                                                   ctypes.POINTER(ctypes.c_double), ctypes.c_uint64,
+                                                   ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_double),
+                                                   U32P, ctypes.POINTER(ctypes.c_uint64)]),
         "wahgpu_server_stats": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
         "wahgpu_server_free": (ctypes.c_int, [P]),
     }
@@ -512,7 +516,10 @@ class Batch:
     """Queries prepared once and run as one kernel launch (capturable in a
     CUDA graph).  queries: list of lists of terms."""
 
-    def __init__(self, ctx: Context, queries, rid_cap: int = 0):
+    def __init__(self, ctx: Context, queries, rid_cap: int = 0, caps=None):
+        """rid_cap: room for the row ids of all queries, back to back; caps:
+        instead, at most caps[q] row ids of query q (the first ones), each
+        query in a region of its own."""
         self.ctx = ctx
         flat = [t for q in queries for t in q]
         offs = np.zeros(len(queries) + 1, dtype=np.uint32)
@@ -520,8 +527,14 @@ class Batch:
         self._terms = (_Term * len(flat))(*flat)
         self._offs = offs
         h = ctypes.c_void_p()
-        ctx.check(ctx.lib.wahgpu_batch_create(ctx.h, self._terms, offs.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
-                                              len(queries), rid_cap, 0, ctypes.byref(h)))
+        op = offs.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+        if caps is not None:
+            c = np.ascontiguousarray(caps, dtype=np.uint64)
+            ctx.check(ctx.lib.wahgpu_batch_create_capped(ctx.h, self._terms, op, len(queries),
+                                                         c.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                                                         ctypes.byref(h)))
+        else:
+            ctx.check(ctx.lib.wahgpu_batch_create(ctx.h, self._terms, op, len(queries), rid_cap, 0, ctypes.byref(h)))
         self.h = h
         self.nq = len(queries)
 
@@ -584,8 +597,10 @@ class Server:
             rid_cap, ctypes.byref(lat))))
         return int(c.value), (out[:n].copy() if rid_cap else None), float(lat.value)
 
-    def replay(self, queries, arrival_s):
-        """Open-loop replay; returns (counts, latencies seconds, wall seconds)."""
+    def replay(self, queries, arrival_s, rid_cap: int = 0):
+        """Open-loop replay; returns (counts, latencies seconds, wall seconds,
+        row ids per query or None) — with rid_cap > 0 each query's first
+        rid_cap row ids."""
         flat = [t for q in queries for t in q]
         offs = np.zeros(len(queries) + 1, dtype=np.uint32)
         offs[1:] = np.cumsum([len(q) for q in queries])
@@ -593,11 +608,17 @@ class Server:
         arrival = np.ascontiguousarray(arrival_s, dtype=np.float64)
         counts = np.zeros(len(queries), dtype=np.uint64)
         lat = np.zeros(len(queries), dtype=np.float64)
+        rids = np.zeros(max(len(queries) * rid_cap, 1), dtype=np.uint32)
+        nrids = np.zeros(len(queries), dtype=np.uint64)
+        U64P = ctypes.POINTER(ctypes.c_uint64)
         us = self.ctx.check(int(self.ctx.lib.wahgpu_server_replay(
             self.h, arr, offs.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), len(queries),
-            arrival.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
-            counts.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), lat.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))))
-        return counts, lat, us / 1e6
+            arrival.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), rid_cap,
+            counts.ctypes.data_as(U64P), lat.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+            rids.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)) if rid_cap else None,
+            nrids.ctypes.data_as(U64P))))
+        ids = [rids[q * rid_cap: q * rid_cap + int(nrids[q])] for q in range(len(queries))] if rid_cap else None
+        return counts, lat, us / 1e6, ids
 
     def stats(self):
         b, s = ctypes.c_uint64(), ctypes.c_uint64()

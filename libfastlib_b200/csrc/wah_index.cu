@@ -390,15 +390,27 @@ static uint64_t term_estimate(const wahgpu_index* x, const DevTerm& d) {
 
 // ------------------------------------------------------------------ batches
 static int batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, const uint32_t* query_offsets,
-                        uint32_t nq, uint64_t rid_cap, int dense_first, int mode, wahgpu_batch** out);
+                        uint32_t nq, uint64_t rid_cap, int dense_first, int mode, const uint64_t* caps,
+                        wahgpu_batch** out);
 
 extern "C" int wahgpu_batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, const uint32_t* query_offsets,
                                    uint32_t nq, uint64_t rid_cap, int dense_first, wahgpu_batch** out) {
-    return batch_create(ctx, terms, query_offsets, nq, rid_cap, dense_first, LOC_HITS, out);
+    return batch_create(ctx, terms, query_offsets, nq, rid_cap, dense_first, LOC_HITS, nullptr, out);
+}
+
+// Row ids with a limit per query (the first rid_caps[q] of query q, in row
+// order, like a LIMIT); every query's ids land in a region of its own.
+extern "C" int wahgpu_batch_create_capped(wahgpu_ctx* ctx, const wahgpu_term* terms, const uint32_t* query_offsets,
+                                          uint32_t nq, const uint64_t* rid_caps, wahgpu_batch** out) {
+    if (!rid_caps) return wg_fail(ctx, WAHGPU_EINVAL, "rid_caps is NULL");
+    uint64_t tot = 0;
+    for (uint32_t q = 0; q < nq; ++q) tot += rid_caps[q];
+    return batch_create(ctx, terms, query_offsets, nq, tot, 0, LOC_HITS, rid_caps, out);
 }
 
 static int batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, const uint32_t* query_offsets,
-                        uint32_t nq, uint64_t rid_cap, int dense_first, int mode, wahgpu_batch** out) {
+                        uint32_t nq, uint64_t rid_cap, int dense_first, int mode, const uint64_t* caps,
+                        wahgpu_batch** out) {
     if (!ctx || !out || !terms || !query_offsets || nq == 0) return wg_fail(ctx, WAHGPU_EINVAL, "bad argument");
     *out = nullptr;
     const uint32_t nt = query_offsets[nq];
@@ -439,6 +451,8 @@ static int batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, const uint32_
         if (query_offsets[q + 1] <= query_offsets[q] || query_offsets[q + 1] > nt)
             return wg_fail(ctx, WAHGPU_EINVAL, "query %u has no term", q);
         dq[q].t0 = query_offsets[q]; dq[q].t1 = query_offsets[q + 1];
+        dq[q].rid_base = q ? dq[q - 1].rid_base + (caps ? caps[q - 1] : 0) : 0;
+        dq[q].rid_lim = caps ? caps[q] : 0;
         std::stable_sort(dt.begin() + dq[q].t0, dt.begin() + dq[q].t1, [&](const DevTerm& a, const DevTerm& b) {
             return term_estimate(idx[a.index], a) < term_estimate(idx[b.index], b);
         });
@@ -457,6 +471,12 @@ static int batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, const uint32_
     B->d_start = static_cast<unsigned long long*>(wg_alloc(ctx, nq * 8));
     B->d_status = static_cast<DevMeta*>(wg_alloc(ctx, sizeof(DevMeta)));
     B->rid_cap = rid_cap;
+    B->capped = caps != nullptr;
+    if (caps) {
+        B->h_lim.assign(caps, caps + nq);
+        B->h_base.resize(nq);
+        for (uint32_t q = 0; q < nq; ++q) B->h_base[q] = dq[q].rid_base;
+    }
     if (rid_cap) B->d_rids = static_cast<uint32_t*>(wg_alloc(ctx, rid_cap * 4));
     if (dense_first) B->d_dense = static_cast<uint32_t*>(wg_alloc(ctx, ((size_t)x0->groups + 1) * 4));
     if (!B->d_idx || !B->d_terms || !B->d_queries || !B->d_counts || !B->d_start || !B->d_status ||
@@ -492,9 +512,10 @@ extern "C" int wahgpu_batch_run(wahgpu_batch* B) {
     // order 2 runs two tile-by-tile passes around a scan of the items' hits,
     // order 1 (and a single query) goes query by query with the look-back
     const bool ids = B->d_rids || B->d_dense;
-    const bool two_pass = ctx->range_order == 2 && ids && B->nq > 1;
+    const bool two_pass = ctx->range_order == 2 && ids && B->nq > 1 && !B->capped;
     a.tile_major = ((ctx->range_order != 0 && !ids) || two_pass) ? 1u : 0u;
     a.pass = 0; a.item_cnt = nullptr; a.item_off = nullptr;
+    a.capped = B->capped && B->d_rids ? 1u : 0u;
     if (two_pass) {
         if (!B->d_items) {
             B->d_items = static_cast<unsigned long long*>(wg_alloc(ctx, (size_t)nitems * 16));
@@ -558,7 +579,8 @@ extern "C" int64_t wahgpu_batch_rids(wahgpu_batch* B, uint32_t q, uint32_t* out,
     wahgpu_ctx* ctx = B->ctx;
     int rc = batch_fetch(B);
     if (rc) return rc;
-    const uint64_t n = B->h_counts[q], s = B->h_start[q];
+    const uint64_t n = B->capped ? std::min<uint64_t>(B->h_counts[q], B->h_lim[q]) : B->h_counts[q];
+    const uint64_t s = B->capped ? B->h_base[q] : B->h_start[q];
     if (!B->d_rids || s + n > B->rid_cap) return wg_fail(ctx, WAHGPU_ESIZE, "row ids exceed the batch's capacity");
     if (cap < n) return wg_fail(ctx, WAHGPU_ESIZE, "need room for %llu row ids", (unsigned long long)n);
     if (n) {
@@ -647,7 +669,7 @@ static int64_t evaluate_mode(wahgpu_ctx* ctx, const wahgpu_term* terms, uint32_t
     if (!ctx || !terms || nterms == 0 || (cap && !rids)) return wg_fail(ctx, WAHGPU_EINVAL, "bad argument");
     const uint32_t qo[2] = {0, nterms};
     wahgpu_batch* B = nullptr;
-    int rc = batch_create(ctx, terms, qo, 1, rids ? cap : 0, hits ? 1 : 0, mode, &B);
+    int rc = batch_create(ctx, terms, qo, 1, rids ? cap : 0, hits ? 1 : 0, mode, nullptr, &B);
     if (rc) return rc;
     rc = wahgpu_batch_run(B);
     uint64_t cnt = 0;

@@ -52,6 +52,8 @@ struct wahgpu_batch {
     std::vector<unsigned long long> h_counts, h_start;
     uint64_t bytes = 0;               // algorithmic bytes one run reads
     uint64_t min_bytes = 0;           // the bytes sumBins itself must read (covered set or complement)
+    bool capped = false;              // row ids limited per query, each query in a region of its own
+    std::vector<uint64_t> h_lim, h_base;
     bool h_valid = false;
 };
 

@@ -80,6 +80,8 @@ struct DevTerm {
 
 struct DevQuery {
     uint32_t t0, t1;      // terms [t0, t1)
+    uint64_t rid_base;    // capped batches: the query's row-id region
+    uint64_t rid_lim;     // capped batches: at most this many row ids (the first ones)
 };
 
 struct RangeArgs {
@@ -104,6 +106,21 @@ struct RangeArgs {
     uint32_t pass;            // 0 one pass, 1 counts, 2 row ids
     unsigned long long* item_cnt;
     const unsigned long long* item_off;
+    // 1: every query writes at most rid_lim row ids into its own region at
+    // rid_base (query-major order; offsets within the query by a segmented
+    // look-back)
+    uint32_t capped;
+};
+
+// 64-bit sums segmented at the first item of each query: {sum lo, sum hi,
+// -, head}; (f1, s1) + (f2, s2) = (f1 | f2, f2 ? s2 : s1 + s2) is
+// associative, so the look-back may combine in any grouping.
+struct SegSum64Comb {
+    __device__ __forceinline__ uint4 operator()(uint4 a, uint4 b) const {
+        if (b.w) return b;
+        const uint64_t s = ((uint64_t)a.y << 32 | a.x) + ((uint64_t)b.y << 32 | b.x);
+        return make_uint4((uint32_t)s, (uint32_t)(s >> 32), 0u, a.w);
+    }
 };
 
 struct RangeShared {
@@ -414,6 +431,24 @@ __global__ void __launch_bounds__(RTHREADS, 6) k_range(RangeArgs A) {
         const uint64_t ex = block_exscan64(cnt, S.scan, total);
         if (A.pass == 2u) {
             if (tid == 0) S.base = A.item_off[qi];
+        } else if (warp == 0 && A.capped) {
+            // the row ids before this tile within its own query
+            const uint4 mine = make_uint4((uint32_t)total, (uint32_t)(total >> 32), 0u, k == 0 ? 1u : 0u);
+            uint4 pre = make_uint4(0u, 0u, 0u, 0u);
+            bool ok = true;
+            if (item == 0) {
+                if (lane == 0) publish(&A.recs[0], epoch, REC_INCL, mine);
+            } else {
+                if (lane == 0) publish(&A.recs[item], epoch, REC_AGG, mine);
+                pre = warp_lookback(A.recs, item, epoch, make_uint4(0u, 0u, 0u, 0u), SegSum64Comb(), &ok);
+                if (lane == 0) publish(&A.recs[item], epoch, REC_INCL, SegSum64Comb()(pre, mine));
+            }
+            if (lane == 0) {
+                if (!ok) atomicExch(&A.status->status, DEV_ERR_TIMEOUT);
+                S.base = k == 0 ? 0ull : ((uint64_t)pre.y << 32 | pre.x);
+                if (total) atomicAdd(&A.counts[q], (unsigned long long)total);
+                if (k == 0) A.rid_start[q] = Q.rid_base;
+            }
         } else if (warp == 0) {
             uint64_t prefix; uint32_t pa, pb;
             const bool ok = lookback64(A.recs, item, epoch, total, 0, 0, prefix, pa, pb);
@@ -427,14 +462,18 @@ __global__ void __launch_bounds__(RTHREADS, 6) k_range(RangeArgs A) {
         __syncthreads();
         if (A.rids) {
             uint64_t off = S.base + ex;
-            for (int j = 0; j < RGPT; ++j) {
+            // capped: offsets are within the query; ids past its limit are
+            // dropped and the rest land in its region
+            const uint64_t lim = A.capped ? Q.rid_lim : A.rid_cap;
+            const uint64_t rbase0 = A.capped ? Q.rid_base : 0ull;
+            for (int j = 0; j < RGPT && off < lim; ++j) {
                 const uint32_t l = l0 + j;
                 if (l >= ng) break;
                 uint32_t bits = S.acc[l];
                 const uint32_t rbase = (g0 + l) * 31u;
                 while (bits) {
                     const uint32_t hb = 31u - __clz(bits);
-                    if (off < A.rid_cap) A.rids[off] = rbase + (30u - hb);
+                    if (off < lim && rbase0 + off < A.rid_cap) A.rids[rbase0 + off] = rbase + (30u - hb);
                     ++off;
                     bits &= ~(1u << hb);
                 }

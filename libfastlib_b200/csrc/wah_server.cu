@@ -89,7 +89,8 @@ void finish_slot(wahgpu_server* S, Slot& sl) {
         if (!rc) {
             r->count = counts[i];
             if (r->rid_cap) {
-                r->rids.resize(std::max<uint64_t>(counts[i], 1));
+                // the first rid_cap row ids of the query (its own region)
+                r->rids.resize(std::max<uint64_t>(std::min<uint64_t>(counts[i], r->rid_cap), 1));
                 const int64_t n = wahgpu_batch_rids(sl.batch, (uint32_t)i, r->rids.data(), r->rids.size());
                 if (n < 0) r->status = (int)n; else r->rids.resize((size_t)n);
             }
@@ -112,17 +113,23 @@ void finish_slot(wahgpu_server* S, Slot& sl) {
 void launch_slot(wahgpu_server* S, Slot& sl, std::vector<Request*>&& take, size_t scratch) {
     std::vector<wahgpu_term> terms;
     std::vector<uint32_t> qoff{0};
+    std::vector<uint64_t> caps;
     uint64_t rid_cap = 0;
     for (Request* r : take) {
         terms.insert(terms.end(), r->terms.begin(), r->terms.end());
         qoff.push_back((uint32_t)terms.size());
+        caps.push_back(r->rid_cap);
         rid_cap += r->rid_cap;
     }
     // count-only batches go tile by tile so their queries share each tile's
     // bitmap words in L2; batches with row ids go query by query
     wahgpu_ctx_set_tuning(sl.ctx, WAHGPU_TUNE_RANGE_ORDER, rid_cap ? 0 : 1);
     wahgpu_batch* B = nullptr;
-    int rc = wahgpu_batch_create(sl.ctx, terms.data(), qoff.data(), (uint32_t)take.size(), rid_cap, 0, &B);
+    // row ids: each request its own region of rid_cap ids (a LIMIT), so a
+    // query with many hits cannot crowd out the others of its batch
+    int rc = rid_cap ? wahgpu_batch_create_capped(sl.ctx, terms.data(), qoff.data(), (uint32_t)take.size(),
+                                                  caps.data(), &B)
+                     : wahgpu_batch_create(sl.ctx, terms.data(), qoff.data(), (uint32_t)take.size(), 0, 0, &B);
     if (!rc) rc = wahgpu_batch_run(B);
     if (!rc && cudaEventRecord(sl.ev, sl.ctx->stream) != cudaSuccess) rc = WAHGPU_ECUDA;
     if (rc) {
@@ -281,7 +288,8 @@ extern "C" int64_t wahgpu_server_wait(wahgpu_server* S, int64_t id, uint64_t* co
 // worker batches; waits for all and writes counts and latencies (arrival to
 // answer).  Returns the wall time of the whole replay in microseconds.
 extern "C" int64_t wahgpu_server_replay(wahgpu_server* S, const wahgpu_term* terms, const uint32_t* qoff, uint32_t nq,
-                                        const double* arrival_s, uint64_t* counts, double* latency_s) {
+                                        const double* arrival_s, uint64_t rid_cap, uint64_t* counts, double* latency_s,
+                                        uint32_t* rids, uint64_t* nrids) {
     if (!S || !terms || !qoff || !arrival_s || nq == 0) return WAHGPU_EINVAL;
     std::vector<int64_t> ids(nq, 0);
     std::atomic<int> err{0};
@@ -295,7 +303,8 @@ extern "C" int64_t wahgpu_server_replay(wahgpu_server* S, const wahgpu_term* ter
             }
             Request* r = new Request();
             r->terms.assign(terms + qoff[q], terms + qoff[q + 1]);
-            r->scratch = request_scratch(terms + qoff[q], 0);
+            r->rid_cap = rid_cap;
+            r->scratch = request_scratch(terms + qoff[q], rid_cap);
             r->t_arrive = due;  // latency counts from the scheduled arrival
             {
                 std::lock_guard<std::mutex> g(S->mu);
@@ -310,10 +319,12 @@ extern "C" int64_t wahgpu_server_replay(wahgpu_server* S, const wahgpu_term* ter
     for (uint32_t q = 0; q < nq; ++q) {
         uint64_t c = 0;
         double l = 0;
-        const int64_t rc = wahgpu_server_wait(S, ids[q], &c, nullptr, 0, &l);
+        const int64_t rc = wahgpu_server_wait(S, ids[q], &c, rids ? rids + (size_t)q * rid_cap : nullptr,
+                                              rids ? rid_cap : 0, &l);
         if (rc < 0) err = (int)rc;
         if (counts) counts[q] = c;
         if (latency_s) latency_s[q] = l;
+        if (nrids) nrids[q] = rc > 0 ? (uint64_t)rc : 0;
     }
     if (err) return err;
     return std::chrono::duration_cast<std::chrono::microseconds>(Clock::now() - t0).count();

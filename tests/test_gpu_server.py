@@ -49,9 +49,16 @@ def test_server_results_equal_alone(gpu_ctx):
         # open loop: Poisson arrivals while earlier batches run
         rng = np.random.default_rng(7)
         arrival = np.cumsum(rng.exponential(1 / 20_000, len(queries)))
-        counts, lat, wall = S.replay(queries, arrival)
+        counts, lat, wall, _ = S.replay(queries, arrival)
         assert [int(c) for c in counts] == [a[0] for a in alone]
         assert np.all(lat > 0) and wall > 0
+        # with the first 500 row ids of every query (each query its own
+        # region, so queries with many hits leave the others theirs)
+        counts, lat, wall, ids = S.replay(queries, arrival, rid_cap=500)
+        assert [int(c) for c in counts] == [a[0] for a in alone]
+        for i, q in enumerate(queries):
+            want = alone[i][1] if alone[i][1] is not None else L.evaluate(gpu_ctx, q)[1]
+            assert np.array_equal(ids[i], want[:500]), i
     finally:
         S.close()
 
@@ -68,3 +75,24 @@ def test_server_refuses_oversized_request(gpu_ctx):
         assert c == 50_000
     finally:
         S.close()
+
+
+def test_capped_batch_row_ids(gpu_ctx):
+    """wahgpu_batch_create_capped: every query keeps its first caps[q] row
+    ids in a region of its own; counts stay complete."""
+    import libfastlib_b200 as L
+    from libfastlib_b200 import workloads as W
+    n = 1_000_003
+    cols = _columns(gpu_ctx, n)
+    qs = W.conjunctive_queries(9, [m for _, m in cols], 64, max_terms=3)
+    queries = [[cols[c][0].term(lo, hi) for c, lo, hi in q] for q in qs]
+    caps = [0 if i % 5 == 0 else (1 + 97 * i) for i in range(len(queries))]
+    B = L.Batch(gpu_ctx, queries, caps=caps)
+    B.run()
+    counts = B.counts()
+    for i, q in enumerate(queries):
+        c, rids, _ = L.evaluate(gpu_ctx, q)
+        assert int(counts[i]) == c, i
+        got = B.rids(i, min(c, caps[i]))
+        assert np.array_equal(got, rids[:caps[i]]), i
+    B.close()

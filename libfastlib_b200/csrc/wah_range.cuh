@@ -137,6 +137,12 @@ static_assert(sizeof(DevTerm) % 4 == 0 && TERM_WORDS <= 32, "a warp stages a ter
 static_assert(sizeof(DevIndex) % 4 == 0 && INDEX_WORDS <= 32, "a warp stages an index");
 
 #ifndef WAH_RANGE_TYPES_ONLY
+// Shared-memory place of tile group l in the accumulators: bits 2-4 XOR'ed
+// with bits 5-7, so groups 32 apart (a sparse bitmap's set bits often are)
+// fall in different banks while every aligned quad of groups stays one
+// 16-byte vector in order.  rsw4: the same for quad index l (groups 4l..).
+__device__ __forceinline__ uint32_t rsw(uint32_t l) { return l ^ (((l >> 5) & 7u) << 2); }
+__device__ __forceinline__ uint32_t rsw4(uint32_t l) { return l ^ ((l >> 3) & 7u); }
 __device__ __forceinline__ bool pass_cmp(double v, uint32_t lop, double lo, uint32_t rop, double hi) {
     const bool a = lop == 0 ? true : (lop == 1 ? lo < v : lo <= v);
     const bool b = rop == 0 ? true : (rop == 1 ? v < hi : v <= hi);
@@ -197,8 +203,8 @@ __device__ __forceinline__ void warp_or_bitmap(RangeShared& S, const DevIndex& I
                 const uint32_t pat = wpattern(wd);
                 for (uint32_t g = a; g < e; ++g) {
                     if (!check) {
-                        if (pat == ALLONES) S.tmp[g - g0] = ALLONES;
-                        else atomicOr(&S.tmp[g - g0], pat);
+                        if (pat == ALLONES) S.tmp[rsw(g - g0)] = ALLONES;
+                        else atomicOr(&S.tmp[rsw(g - g0)], pat);
                     } else {
                         uint32_t bits = pat, set = 0;
                         while (bits) {
@@ -208,7 +214,7 @@ __device__ __forceinline__ void warp_or_bitmap(RangeShared& S, const DevIndex& I
                                 set |= 1u << hb;
                             bits &= ~(1u << hb);
                         }
-                        if (set) atomicOr(&S.tmp[g - g0], set);
+                        if (set) atomicOr(&S.tmp[rsw(g - g0)], set);
                     }
                 }
             }
@@ -230,7 +236,7 @@ __device__ __forceinline__ void warp_or_bitmap(RangeShared& S, const DevIndex& I
             }
             pat = set;
         }
-        if (pat) atomicOr(&S.tmp[Gb - g0], pat);
+        if (pat) atomicOr(&S.tmp[rsw(Gb - g0)], pat);
     }
 }
 
@@ -331,7 +337,7 @@ __global__ void __launch_bounds__(RTHREADS, 6) k_range(RangeArgs A) {
                         const uint4 b = two ? __ldg(lo + l) : v;
                         v = make_uint4(a.x & ~b.x, a.y & ~b.y, a.z & ~b.z, a.w & ~b.w);
                     }
-                    t4[l] = v;
+                    t4[rsw4(l)] = v;
                 }
             } else {
 #pragma unroll
@@ -383,7 +389,7 @@ __global__ void __launch_bounds__(RTHREADS, 6) k_range(RangeArgs A) {
                 __syncthreads();
                 for (uint32_t l = tid; l < ng; l += RTHREADS) {
                     const uint32_t msk = (g0 + l == G && anb > 0) ? lastmask : ALLONES;
-                    S.tmp[l] ^= msk;
+                    S.tmp[rsw(l)] ^= msk;
                 }
                 __syncthreads();
                 // edge bitmaps: rows checked against the raw values
@@ -403,12 +409,12 @@ __global__ void __launch_bounds__(RTHREADS, 6) k_range(RangeArgs A) {
         for (int j = 0; j < RGPT; ++j) {
             const uint32_t l = l0 + j;
             if (l < ng) {
-                uint32_t v = S.acc[l];
+                uint32_t v = S.acc[rsw(l)];
                 if (g0 + l == G && anb > 0) v &= lastmask;
-                S.acc[l] = v;
+                S.acc[rsw(l)] = v;
                 cnt += __popc(v);
             } else if (l < RT) {
-                S.acc[l] = 0u;
+                S.acc[rsw(l)] = 0u;
             }
         }
         if (A.tile_major && A.pass == 1u) {
@@ -469,7 +475,7 @@ __global__ void __launch_bounds__(RTHREADS, 6) k_range(RangeArgs A) {
             for (int j = 0; j < RGPT && off < lim; ++j) {
                 const uint32_t l = l0 + j;
                 if (l >= ng) break;
-                uint32_t bits = S.acc[l];
+                uint32_t bits = S.acc[rsw(l)];
                 const uint32_t rbase = (g0 + l) * 31u;
                 while (bits) {
                     const uint32_t hb = 31u - __clz(bits);
@@ -480,7 +486,7 @@ __global__ void __launch_bounds__(RTHREADS, 6) k_range(RangeArgs A) {
             }
         }
         if (A.dense && q == 0) {
-            for (uint32_t l = tid; l < ng; l += RTHREADS) A.dense[g0 + l] = S.acc[l];
+            for (uint32_t l = tid; l < ng; l += RTHREADS) A.dense[g0 + l] = S.acc[rsw(l)];
         }
         __syncthreads();
     }

@@ -84,6 +84,15 @@ int64_t wahgpu_ctx_launches(wahgpu_ctx* ctx);
                                      placed by a count pass and a scan */
 #define WAHGPU_TUNE_RANGE_CTAS 3  /* resident CTAs per SM of the persistent range launch: 0 (all that fit) .. 32 */
 #define WAHGPU_TUNE_CUM_STRIDE 5  /* bitmaps per cumulative row of indexes built or attached later: 0 auto, 1 none, >= 2 that stride */
+/* Failure-path test hooks (no counterpart in the reference; never needed in
+ * normal use).  WAHGPU_TEST_WITHHOLD_TILE = t: in the next operator call on
+ * the single-pass group-space engine, tile t never publishes its look-back
+ * record, so the tile after it waits until its bounded wait gives up and
+ * the call reports WAHGPU_ETIMEOUT (the hook then clears itself).
+ * WAHGPU_TEST_FAIL_ALLOC = n: the n-th device allocation from now fails as
+ * if the device were out of memory (WAHGPU_ENOMEM), once. */
+#define WAHGPU_TEST_WITHHOLD_TILE 100
+#define WAHGPU_TEST_FAIL_ALLOC 101
 int wahgpu_ctx_set_tuning(wahgpu_ctx* ctx, int key, int64_t value);
 int64_t wahgpu_ctx_get_tuning(wahgpu_ctx* ctx, int key);
 

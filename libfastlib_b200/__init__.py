@@ -54,6 +54,8 @@ TUNE_RANGE_ORDER = 2
 TUNE_RANGE_CTAS = 3
 TUNE_DENSE_ENGINE = 4  # 0 auto (= 4), 1 pipelined group space, 2 word space, 3 two-pass group space, 4 single-pass group space
 TUNE_CUM_STRIDE = 5
+TEST_WITHHOLD_TILE = 100  # failure-path test hook: a tile that never publishes its look-back record
+TEST_FAIL_ALLOC = 101     # failure-path test hook: the n-th device allocation from now fails
 DENSE_TILES = (1024, 2048, 4096)
 CMP_NONE, CMP_LT, CMP_LE = 0, 1, 2
 U32, F32, I32 = 0, 1, 2

@@ -49,6 +49,7 @@ void* wg_alloc(wahgpu_ctx* ctx, size_t bytes) {
     size_t c = size_class(bytes);
     {
         std::lock_guard<std::mutex> g(ctx->mu);
+        if (ctx->test_fail_alloc > 0 && --ctx->test_fail_alloc == 0) return nullptr;  // test hook
         auto it = ctx->pool.find(c);
         if (it != ctx->pool.end() && !it->second.empty()) {
             void* p = it->second.back();
@@ -177,6 +178,13 @@ extern "C" int wahgpu_ctx_set_tuning(wahgpu_ctx* ctx, int key, int64_t value) {
     case WAHGPU_TUNE_RANGE_CTAS:
         if (value < 0 || value > 32) return wg_fail(ctx, WAHGPU_EINVAL, "range CTAs per SM must be 0..32");
         ctx->range_ctas = (uint32_t)value;
+        return WAHGPU_OK;
+    case WAHGPU_TEST_WITHHOLD_TILE:
+        ctx->test_withhold = value < 0 ? 0xFFFFFFFFu : (uint32_t)value;
+        return WAHGPU_OK;
+    case WAHGPU_TEST_FAIL_ALLOC:
+        if (value < 0) return wg_fail(ctx, WAHGPU_EINVAL, "allocation count must be >= 0");
+        ctx->test_fail_alloc = value;
         return WAHGPU_OK;
     case WAHGPU_TUNE_CUM_STRIDE:
         if (value < 0 || value > (1 << 30)) return wg_fail(ctx, WAHGPU_EINVAL, "cumulative stride must be 0 (auto), 1 (none) or a stride");
@@ -635,6 +643,8 @@ int wg_launch_fuse(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t
     a.out = res->words; a.obp = res->bpos; a.meta = res->meta; a.cap = res->cap;
     a.recs = recs; a.sync = sync;
     a.aval = aval; a.anb = anb;
+    a.withhold = ctx->test_withhold;
+    ctx->test_withhold = 0xFFFFFFFFu;
     CUDA_TRY(ctx, cudaMemsetAsync(res->meta, 0, sizeof(DevMeta), ctx->stream));
     switch (op) {
     case OP_AND: launch_fuse_op<OP_AND>(ctx, ntiles, ctx->stream, a); break;

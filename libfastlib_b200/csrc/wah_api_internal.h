@@ -30,6 +30,11 @@ struct wahgpu_ctx {
     uint32_t range_order = 1;           // WAHGPU_TUNE_RANGE_ORDER
     uint32_t range_ctas = 0;            // WAHGPU_TUNE_RANGE_CTAS (0: as many as fit)
     uint32_t cum_stride = 0;            // WAHGPU_TUNE_CUM_STRIDE (0 auto, 1 none)
+    // failure-path test hooks (WAHGPU_TEST_*): the tile of the next
+    // single-pass operator launch that never publishes its look-back record
+    // (UINT32_MAX: none), and the allocations left before one fails (0: off)
+    uint32_t test_withhold = 0xFFFFFFFFu;
+    int64_t test_fail_alloc = 0;
 };
 
 struct wahgpu_bv {

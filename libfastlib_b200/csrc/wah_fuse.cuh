@@ -58,6 +58,7 @@ struct FuseArgs {
     uint32_t cap;          // words the result can hold (>= nx + ny)
     TileRec* recs; LaunchSync* sync;
     uint32_t aval, anb;
+    uint32_t withhold;     // test hook: this tile never publishes (UINT32_MAX: none)
 };
 
 struct FuseShared {
@@ -301,12 +302,13 @@ __global__ void __launch_bounds__(FTHREADS, 4) k_gfuse(FuseArgs A) {
     if (warp == 0) {
         uint4 pre = make_uint4(0u, 0u, 0u, 0u);
         bool ok = true;
+        const bool pub = t != A.withhold;
         if (t == 0) {
-            if (lane == 0) publish(&A.recs[0], epoch, REC_INCL, tot);
+            if (lane == 0 && pub) publish(&A.recs[0], epoch, REC_INCL, tot);
         } else {
-            if (lane == 0) publish(&A.recs[t], epoch, REC_AGG, tot);
+            if (lane == 0 && pub) publish(&A.recs[t], epoch, REC_AGG, tot);
             pre = warp_lookback(A.recs, t, epoch, make_uint4(0u, 0u, 0u, 0u), comb, &ok);
-            if (lane == 0) publish(&A.recs[t], epoch, REC_INCL, comb(pre, tot));
+            if (lane == 0 && pub) publish(&A.recs[t], epoch, REC_INCL, comb(pre, tot));
         }
         if (lane == 0) {
             // a wait that gave up leaves the prefix unknown: no words are

@@ -30,10 +30,15 @@ def build(force: bool = False) -> str:
     return LIB
 
 
-def build_reference(ref_root: str = "/root/reference", jobs: int = 8) -> bool:
+def build_reference(ref_root: str = None, jobs: int = 8) -> bool:
     """Compiles the reference library and the oracle driver into oracle/_ref
-    (only where the reference sources exist).  Returns True when refdrv is
-    available afterwards."""
+    (only where the reference sources exist: `ref_root`, else the directory
+    named by the FASTBIT_REFERENCE environment variable, else ../reference
+    beside this repository).  Returns True when refdrv is available
+    afterwards."""
+    if ref_root is None:
+        ref_root = os.environ.get("FASTBIT_REFERENCE") or os.path.join(os.path.dirname(os.path.dirname(HERE)),
+                                                                        "reference")
     if os.path.isdir(os.path.join(ref_root, "src")):
         subprocess.run(["make", "-s", "-f", os.path.join(HERE, "Makefile.ref"), f"REF={ref_root}",
                         f"-j{jobs}", "all"], check=True, cwd=os.path.dirname(HERE),

@@ -87,8 +87,10 @@ int wg_scratch(wahgpu_ctx* ctx, uint32_t ntiles, TileRec** recs, LaunchSync** sy
         CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
         if (ctx->scratch) cudaFree(ctx->scratch);
         ctx->scratch = nullptr;
-        // sync words, TileRec records, then the dense kernel's 16-byte records
-        size_t bytes = sizeof(LaunchSync) * 2 + (size_t)want * (sizeof(TileRec) + sizeof(uint4));
+        // sync words, TileRec records, then the dense kernel's 16-byte
+        // records and the single-pass kernel's (each format in a region of
+        // its own, so a stale record of one is never read by the other)
+        size_t bytes = sizeof(LaunchSync) * 2 + (size_t)want * (sizeof(TileRec) + 2 * sizeof(uint4));
         if (cudaMalloc(&ctx->scratch, bytes) != cudaSuccess) {
             cudaGetLastError();
             ctx->scratch_tiles = 0;
@@ -104,6 +106,10 @@ int wg_scratch(wahgpu_ctx* ctx, uint32_t ntiles, TileRec** recs, LaunchSync** sy
 // The dense kernel's records, after the TileRec array of the scratch block.
 static uint4* wg_dense_recs(wahgpu_ctx* ctx, TileRec* recs) {
     return reinterpret_cast<uint4*>(recs + ctx->scratch_tiles);
+}
+// The single-pass group-space kernel's records, after the dense kernel's.
+static uint4* wg_fuse_recs(wahgpu_ctx* ctx, TileRec* recs) {
+    return wg_dense_recs(ctx, recs) + ctx->scratch_tiles;
 }
 
 // ------------------------------------------------------------------ context
@@ -641,7 +647,7 @@ int wg_launch_fuse(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t
     a.yw = y->words; a.ygt = y->gt; a.ny = y->h.n;
     a.groups = groups; a.ntiles = ntiles;
     a.out = res->words; a.obp = res->bpos; a.meta = res->meta; a.cap = res->cap;
-    a.recs = recs; a.sync = sync;
+    a.recs = wg_fuse_recs(ctx, recs); a.sync = sync;
     a.aval = aval; a.anb = anb;
     a.withhold = ctx->test_withhold;
     ctx->test_withhold = 0xFFFFFFFFu;

@@ -56,7 +56,7 @@ struct FuseArgs {
     uint32_t groups, ntiles;
     uint32_t* out; uint32_t* obp; DevMeta* meta;
     uint32_t cap;          // words the result can hold (>= nx + ny)
-    TileRec* recs; LaunchSync* sync;
+    uint4* recs; LaunchSync* sync;  // one 16-byte look-back record per tile
     uint32_t aval, anb;
     uint32_t withhold;     // test hook: this tile never publishes (UINT32_MAX: none)
 };
@@ -119,6 +119,97 @@ struct FuseComb {
         return make_uint4(a.x + b.x, max(a.y, b.y), a.z + b.z, a.w | b.w);
     }
 };
+
+// Look-back records: one 16-byte record per tile, {heads, last head, ones,
+// epoch * 4 + state}, written and read as one 16-byte access (a record is
+// never seen half written; those of earlier launches carry an older epoch).
+// A tile publishes its aggregate (REC_AGG) and later, in the same record,
+// its inclusive prefix (REC_INCL).
+__device__ __forceinline__ void frec_publish(uint4* recs, uint32_t t, uint32_t epoch, uint32_t state, uint4 v) {
+    st_cg4(recs + t, make_uint4(v.x, v.y, v.z, epoch * 4u + state));
+}
+constexpr int FLB = 4;  // predecessors per lane per look-back round: 128 tiles per round trip
+
+// Warp-wide look-back over 16-byte records: each round the lanes read the
+// records of the 128 tiles before `hi` (lane l the FLB tiles
+// [hi - FLB(l+1), hi - FLB l), all loads in flight together), wait (bounded)
+// for any not yet published, and stop at the nearest inclusive record.
+// Returns the exclusive prefix of tile t in every lane; *ok turns false
+// when a wait gave up.
+__device__ __forceinline__ uint4 fuse_lookback(const uint4* recs, uint32_t t, uint32_t epoch, bool* ok) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const FuseComb comb;
+    uint4 acc = make_uint4(0u, 0u, 0u, 0u);  // tiles already visited (later ones)
+    int64_t hi = t;
+    *ok = true;
+    while (hi > 0) {
+        uint4 v[FLB];
+        uint32_t st[FLB];
+#pragma unroll
+        for (int k = 0; k < FLB; ++k) {  // k = 0: the latest tile of the lane
+            const int64_t i = hi - 1 - (int64_t)FLB * lane - k;
+            v[k] = i >= 0 ? ld_cg4(recs + i) : make_uint4(0u, 0u, 0u, epoch * 4u + REC_INCL);
+        }
+        uint32_t ns = 8;
+        for (uint32_t it = 0;; ++it) {
+            bool all = true;
+#pragma unroll
+            for (int k = 0; k < FLB; ++k) {
+                st[k] = (v[k].w >> 2) == (epoch & 0x3FFFFFFFu) ? (v[k].w & 3u) : 0u;
+                all &= st[k] != 0u;
+            }
+            if (all) break;
+            if (it >= SPIN_LIMIT) {
+                *ok = false;
+#pragma unroll
+                for (int k = 0; k < FLB; ++k)
+                    if (!st[k]) { st[k] = REC_INCL; v[k] = make_uint4(0u, 0u, 0u, 0u); }
+                break;
+            }
+            __nanosleep(ns);
+            if (ns < 256) ns <<= 1;
+#pragma unroll
+            for (int k = 0; k < FLB; ++k)
+                if (!st[k]) {
+                    const int64_t i = hi - 1 - (int64_t)FLB * lane - k;
+                    v[k] = ld_cg4(recs + i);
+                }
+        }
+        // the lane's tiles in order, from its latest inclusive record on
+        uint4 mine = make_uint4(0u, 0u, 0u, 0u);
+        bool incl = false;
+#pragma unroll
+        for (int k = 0; k < FLB; ++k) {
+            if (incl) continue;
+            const uint4 x = make_uint4(v[k].x, v[k].y, v[k].z, 0u);
+            mine = comb(x, mine);
+            incl = st[k] == REC_INCL;
+        }
+        const uint32_t bal = __ballot_sync(0xffffffffu, incl);
+        const uint32_t L = bal ? (uint32_t)(__ffs(bal) - 1) : 31u;  // nearest lane holding an inclusive record
+        if (lane > L) mine = make_uint4(0u, 0u, 0u, 0u);
+        // ordered tree: lane l ends up with lanes [l, ...] combined, higher
+        // lanes being earlier tiles
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            uint4 o;
+            o.x = __shfl_down_sync(0xffffffffu, mine.x, d);
+            o.y = __shfl_down_sync(0xffffffffu, mine.y, d);
+            o.z = __shfl_down_sync(0xffffffffu, mine.z, d);
+            o.w = 0u;
+            if (lane + d < 32u) mine = comb(o, mine);
+        }
+        uint4 win;
+        win.x = __shfl_sync(0xffffffffu, mine.x, 0);
+        win.y = __shfl_sync(0xffffffffu, mine.y, 0);
+        win.z = __shfl_sync(0xffffffffu, mine.z, 0);
+        win.w = 0u;
+        acc = comb(win, acc);
+        if (bal) break;
+        hi -= 32 * FLB;
+    }
+    return acc;
+}
 
 // The word of a uniform run of class c and len groups.
 __device__ __forceinline__ uint32_t fuse_run(uint32_t c, uint32_t len) {
@@ -304,11 +395,11 @@ __global__ void __launch_bounds__(FTHREADS, 4) k_gfuse(FuseArgs A) {
         bool ok = true;
         const bool pub = t != A.withhold;
         if (t == 0) {
-            if (lane == 0 && pub) publish(&A.recs[0], epoch, REC_INCL, tot);
+            if (lane == 0 && pub) frec_publish(A.recs, 0, epoch, REC_INCL, tot);
         } else {
-            if (lane == 0 && pub) publish(&A.recs[t], epoch, REC_AGG, tot);
-            pre = warp_lookback(A.recs, t, epoch, make_uint4(0u, 0u, 0u, 0u), comb, &ok);
-            if (lane == 0 && pub) publish(&A.recs[t], epoch, REC_INCL, comb(pre, tot));
+            if (lane == 0 && pub) frec_publish(A.recs, t, epoch, REC_AGG, tot);
+            pre = fuse_lookback(A.recs, t, epoch, &ok);
+            if (lane == 0 && pub) frec_publish(A.recs, t, epoch, REC_INCL, comb(pre, tot));
         }
         if (lane == 0) {
             // a wait that gave up leaves the prefix unknown: no words are

@@ -623,11 +623,18 @@ static bool fuse_applies(const wahgpu_bv* x, const wahgpu_bv* y, const wahgpu_bv
     auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
     return groups > 0 && al(x->words) && al(y->words) && al(res->words);
 }
-template <int OP>
+template <int OP, int FT>
 static void launch_fuse_op(const wahgpu_ctx* ctx, uint32_t ntiles, cudaStream_t s, const FuseArgs& a) {
     static PerDeviceSetup setup;
-    wg_kernel_setup(setup, ctx->device, k_gfuse<OP>, FTHREADS, 0);
-    k_gfuse<OP><<<ntiles, FTHREADS, 0, s>>>(a);
+    const size_t sm = sizeof(FuseShared<FT>);
+    wg_kernel_setup(setup, ctx->device, k_gfuse<OP, FT>, FCfg<FT>::THREADS, sm);
+    k_gfuse<OP, FT><<<ntiles, FCfg<FT>::THREADS, sm, s>>>(a);
+}
+template <int OP>
+static void launch_fuse_tile(const wahgpu_ctx* ctx, uint32_t ft, uint32_t ntiles, cudaStream_t s, const FuseArgs& a) {
+    if (ft == 1024) launch_fuse_op<OP, 1024>(ctx, ntiles, s, a);
+    else if (ft == 4096) launch_fuse_op<OP, 4096>(ctx, ntiles, s, a);
+    else launch_fuse_op<OP, 2048>(ctx, ntiles, s, a);
 }
 int wg_launch_fuse(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t groups,
                    uint32_t anb, uint32_t aval, wahgpu_bv* res) {
@@ -638,7 +645,8 @@ int wg_launch_fuse(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t
     if (rc) return rc;
     rc = wg_gtile(y);
     if (rc) return rc;
-    const uint32_t ntiles = (groups + FT - 1) / FT;
+    const uint32_t ft = ctx->dense_tile;  // WAHGPU_TUNE_DENSE_TILE: 1024, 2048 (default) or 4096 groups
+    const uint32_t ntiles = (groups + ft - 1) / ft;
     TileRec* recs; LaunchSync* sync;
     rc = wg_scratch(ctx, ntiles, &recs, &sync);
     if (rc) return rc;
@@ -653,10 +661,10 @@ int wg_launch_fuse(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t
     ctx->test_withhold = 0xFFFFFFFFu;
     CUDA_TRY(ctx, cudaMemsetAsync(res->meta, 0, sizeof(DevMeta), ctx->stream));
     switch (op) {
-    case OP_AND: launch_fuse_op<OP_AND>(ctx, ntiles, ctx->stream, a); break;
-    case OP_OR: launch_fuse_op<OP_OR>(ctx, ntiles, ctx->stream, a); break;
-    case OP_XOR: launch_fuse_op<OP_XOR>(ctx, ntiles, ctx->stream, a); break;
-    default: launch_fuse_op<OP_MINUS>(ctx, ntiles, ctx->stream, a); break;
+    case OP_AND: launch_fuse_tile<OP_AND>(ctx, ft, ntiles, ctx->stream, a); break;
+    case OP_OR: launch_fuse_tile<OP_OR>(ctx, ft, ntiles, ctx->stream, a); break;
+    case OP_XOR: launch_fuse_tile<OP_XOR>(ctx, ft, ntiles, ctx->stream, a); break;
+    default: launch_fuse_tile<OP_MINUS>(ctx, ft, ntiles, ctx->stream, a); break;
     }
     ctx->launches++;
     CUDA_TRY(ctx, cudaGetLastError());

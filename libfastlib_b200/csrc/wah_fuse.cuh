@@ -6,9 +6,9 @@
 // the run holds two or more groups, else the literal 0 / 0x7FFFFFFF) and
 // one literal per mixed group.
 //
-// k_gfuse<OP>: one CTA per tile of FT = 2048 groups, one launch, operands
+// k_gfuse<OP, FT>: one CTA per tile of FT groups (2048 by default), one launch, operands
 // read once and result words written once (no intermediate array):
-//  1. word phase (all FTHREADS threads): each thread loads 8 consecutive
+//  1. word phase (all the CTA's threads): each thread loads 8 consecutive
 //     words of each operand from the 16-byte boundary at or below the
 //     tile's first word (two 16-byte loads per operand), measures each
 //     word in groups (clipped to the tile), and one block scan of both
@@ -16,7 +16,7 @@
 //     every word's first group.  Each word then writes its 31-bit pattern
 //     into the tile's group-space array of its operand (a fill of up to 8
 //     groups by its own thread, a longer one by its whole warp).
-//  2. group phase (the first 256 threads, 8 consecutive groups each): the
+//  2. group phase (the first FT / 8 threads, 8 consecutive groups each): the
 //     result patterns R = a OP b, their classes, the run heads (a mixed
 //     group, a class change, or group 0) and the popcount; one block scan
 //     gives each thread its heads' output indices within the tile and the
@@ -28,7 +28,7 @@
 //     written by the lane of the next head, in this tile or a later one;
 //     the last tile writes the final run's word and the metadata.  Words
 //     land in shared memory and leave as 16-byte coalesced stores.
-// Group arrays are stored transposed (group q at (q % 8) * 256 + q / 8) so
+// Group arrays are stored transposed (group q at (q % 8) * FT/8 + q / 8) so
 // both the painting (words ~ groups per lane) and the group phase (8
 // consecutive groups per lane) hit 32 different banks.
 //
@@ -40,15 +40,23 @@
 
 namespace wah {
 
-constexpr int FT = 2048;                 // groups per tile (a multiple of the group-tile index stride DT)
-constexpr int FWARPS = 9;                // 9 warps: 2304 word slots >= FT + 3 (alignment slack)
-constexpr int FTHREADS = FWARPS * 32;
 constexpr int FWPT = 8;                  // word slots per thread and operand
 constexpr int FGPT = 8;                  // groups per thread in the group phase
-constexpr int FGTHREADS = FT / FGPT;     // 256 threads in the group phase
-constexpr int FROWS = FT / FGPT;         // transposed row length
 constexpr int FSHORT = 8;                // fills up to this many groups are painted by their own thread
-static_assert(FT % DT == 0 && FTHREADS * FWPT >= FT + 3 && FGTHREADS % 32 == 0, "tile shape");
+
+// Tile shape: FT groups per tile (1024, 2048 or 4096: WAHGPU_TUNE_DENSE_TILE),
+// enough warps for FT + 3 word slots (the tile's words from the 16-byte
+// boundary below its first), FT / 8 threads in the group phase.
+template <int FT_>
+struct FCfg {
+    static constexpr int FT = FT_;
+    static constexpr int WARPS = (FT_ + 3 + FWPT * 32 - 1) / (FWPT * 32);
+    static constexpr int THREADS = WARPS * 32;
+    static constexpr int GTHREADS = FT_ / FGPT;
+    static constexpr int ROWS = FT_ / FGPT;   // transposed row length
+    static constexpr int MINB = THREADS <= 320 ? 4 : 2;
+    static_assert(FT_ % DT == 0 && THREADS * FWPT >= FT_ + 3 && GTHREADS % 32 == 0, "tile shape");
+};
 
 struct FuseArgs {
     const uint32_t* xw; const uint32_t* xgt; uint32_t nx;
@@ -61,23 +69,26 @@ struct FuseArgs {
     uint32_t withhold;     // test hook: this tile never publishes (UINT32_MAX: none)
 };
 
+template <int FT>
 struct FuseShared {
+    using C = FCfg<FT>;
     uint32_t pat[2][FT];       // group patterns per operand, transposed
     uint32_t out[FT + 4];      // this tile's words, at index o - (obase & ~3)
-    uint4 wagg[FGTHREADS / 32];
-    uint32_t wsum[FWARPS];
+    uint4 wagg[C::GTHREADS / 32];
+    uint32_t wsum[C::WARPS];
     uint4 pre;                 // exclusive prefix of the tile (look-back)
     uint32_t tile, epoch, bad, fill, skip;
 };
 
-__device__ __forceinline__ uint32_t fidx(uint32_t q) { return (q & (FGPT - 1u)) * FROWS + (q / FGPT); }
+template <int FT>
+__device__ __forceinline__ uint32_t fidx(uint32_t q) { return (q & (FGPT - 1u)) * FCfg<FT>::ROWS + (q / FGPT); }
 
 // Word range of one operand over the tile [g0, g1): words [wi0, wi0 + nw),
 // the first starting at group s0 <= g0.  gt: the operand's group-tile index
 // (entry k = index and first group of the word covering group DT*k; the
 // entry past the end = (n, G)).  False for a range the metadata cannot give.
 __device__ __forceinline__ bool fuse_range(const uint32_t* __restrict__ gt, uint32_t n, uint32_t g0, uint32_t g1,
-                                           uint32_t& wi0, uint32_t& s0, uint32_t& nw) {
+                                           uint32_t FT, uint32_t& wi0, uint32_t& s0, uint32_t& nw) {
     const uint32_t e0 = g0 / DT, e1 = (g1 + DT - 1) / DT;
     wi0 = __ldg(gt + 2 * e0); s0 = __ldg(gt + 2 * e0 + 1);
     const uint32_t wi1 = __ldg(gt + 2 * e1), s1 = __ldg(gt + 2 * e1 + 1);
@@ -105,11 +116,11 @@ __device__ __forceinline__ uint4 fuse_ld4(const uint32_t* __restrict__ w, uint32
 // whose tile words are [wi0, wi0 + nw) with the first starting at s0;
 // clipped to the tile and to FT so 16-bit sums cannot overflow.
 __device__ __forceinline__ uint32_t fuse_len(uint32_t w, uint32_t k, uint32_t wi0, uint32_t nw, uint32_t s0,
-                                             uint32_t g0, uint32_t g1) {
+                                             uint32_t g0, uint32_t g1, uint32_t FT) {
     if (k < wi0 || k - wi0 >= nw) return 0u;
     uint32_t c = wgroups(w);
     if (k == wi0) c = min(s0 + c, g1) - g0;
-    return min(c, (uint32_t)FT);
+    return min(c, FT);
 }
 
 // {heads, last head, ones, -}: sum, max, sum.  A last head is packed as
@@ -216,9 +227,11 @@ __device__ __forceinline__ uint32_t fuse_run(uint32_t c, uint32_t len) {
     return len >= 2u ? fill_word(c, len) : (c ? ALLONES : 0u);
 }
 
-template <int OP>
-__global__ void __launch_bounds__(FTHREADS, 4) k_gfuse(FuseArgs A) {
-    __shared__ __align__(16) FuseShared S;
+template <int OP, int FT>
+__global__ void __launch_bounds__(FCfg<FT>::THREADS, FCfg<FT>::MINB) k_gfuse(FuseArgs A) {
+    using C = FCfg<FT>;
+    extern __shared__ __align__(16) unsigned char fsm_raw[];
+    FuseShared<FT>& S = *reinterpret_cast<FuseShared<FT>*>(fsm_raw);
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     if (tid == 0) {
         S.tile = claim_tile(A.sync);
@@ -235,8 +248,8 @@ __global__ void __launch_bounds__(FTHREADS, 4) k_gfuse(FuseArgs A) {
 
     // ---- word phase
     uint32_t xi0, xs0, xn, yi0, ys0, yn;
-    const bool okx = fuse_range(A.xgt, A.nx, g0, g1, xi0, xs0, xn);
-    const bool oky = fuse_range(A.ygt, A.ny, g0, g1, yi0, ys0, yn);
+    const bool okx = fuse_range(A.xgt, A.nx, g0, g1, FT, xi0, xs0, xn);
+    const bool oky = fuse_range(A.ygt, A.ny, g0, g1, FT, yi0, ys0, yn);
     if (!(okx && oky) && tid == 0) {
         S.bad = 1;
         atomicExch(&A.meta->status, DEV_ERR_FORMAT);
@@ -253,7 +266,7 @@ __global__ void __launch_bounds__(FTHREADS, 4) k_gfuse(FuseArgs A) {
     uint32_t run = 0;
 #pragma unroll
     for (int j = 0; j < FWPT; ++j) {
-        run += fuse_len(wx[j], kx + j, xi0, xn, xs0, g0, g1) | (fuse_len(wy[j], ky + j, yi0, yn, ys0, g0, g1) << 16);
+        run += fuse_len(wx[j], kx + j, xi0, xn, xs0, g0, g1, FT) | (fuse_len(wy[j], ky + j, yi0, yn, ys0, g0, g1, FT) << 16);
         st[j] = run;
     }
     uint32_t inc = run;
@@ -280,7 +293,7 @@ __global__ void __launch_bounds__(FTHREADS, 4) k_gfuse(FuseArgs A) {
             if (L <= (uint32_t)FSHORT) {
 #pragma unroll
                 for (uint32_t e = 0; e < (uint32_t)FSHORT; ++e)
-                    if (e < L) S.pat[0][fidx(qx + e)] = p;
+                    if (e < L) S.pat[0][fidx<FT>(qx + e)] = p;
             } else {
                 longx = true;
             }
@@ -291,7 +304,7 @@ __global__ void __launch_bounds__(FTHREADS, 4) k_gfuse(FuseArgs A) {
             if (L <= (uint32_t)FSHORT) {
 #pragma unroll
                 for (uint32_t e = 0; e < (uint32_t)FSHORT; ++e)
-                    if (e < L) S.pat[1][fidx(qy + e)] = p;
+                    if (e < L) S.pat[1][fidx<FT>(qy + e)] = p;
             } else {
                 longy = true;
             }
@@ -315,7 +328,7 @@ __global__ void __launch_bounds__(FTHREADS, 4) k_gfuse(FuseArgs A) {
                     const uint32_t q0 = __shfl_sync(0xffffffffu, q, src);
                     const uint32_t L0 = __shfl_sync(0xffffffffu, L, src);
                     const uint32_t p0 = __shfl_sync(0xffffffffu, wpattern(o ? wy[j] : wx[j]), src);
-                    for (uint32_t e = lane; e < L0; e += 32u) S.pat[o][fidx(q0 + e)] = p0;
+                    for (uint32_t e = lane; e < L0; e += 32u) S.pat[o][fidx<FT>(q0 + e)] = p0;
                 }
             }
         }
@@ -325,13 +338,13 @@ __global__ void __launch_bounds__(FTHREADS, 4) k_gfuse(FuseArgs A) {
     // ---- group phase
     uint32_t r[FGPT];
     uint32_t hm = 0, ones = 0, lasth = 0;
-    const bool grp = tid < (uint32_t)FGTHREADS;
+    const bool grp = tid < (uint32_t)C::GTHREADS;
     if (grp) {
         const uint32_t q0 = tid * FGPT;
         const bool bad = S.bad != 0;
         uint32_t pr;  // the result of the group before q0
         if (tid > 0) {
-            pr = op2<OP>(S.pat[0][fidx(q0 - 1u)], S.pat[1][fidx(q0 - 1u)]);
+            pr = op2<OP>(S.pat[0][fidx<FT>(q0 - 1u)], S.pat[1][fidx<FT>(q0 - 1u)]);
         } else if (g0 > 0 && !bad) {
             const uint32_t xp = __ldg(A.xw + (xs0 < g0 ? xi0 : xi0 - 1u));
             const uint32_t yp = __ldg(A.yw + (ys0 < g0 ? yi0 : yi0 - 1u));
@@ -344,8 +357,8 @@ __global__ void __launch_bounds__(FTHREADS, 4) k_gfuse(FuseArgs A) {
         for (int e = 0; e < FGPT; ++e) {
             const uint32_t q = q0 + e;
             const bool in = q < ng;
-            const uint32_t a = (in && !bad) ? S.pat[0][fidx(q)] : 0u;
-            const uint32_t b = (in && !bad) ? S.pat[1][fidx(q)] : 0u;
+            const uint32_t a = (in && !bad) ? S.pat[0][fidx<FT>(q)] : 0u;
+            const uint32_t b = (in && !bad) ? S.pat[1][fidx<FT>(q)] : 0u;
             r[e] = op2<OP>(a, b);
             const uint32_t c = cls_of(r[e]);
             if (in) {
@@ -388,7 +401,7 @@ __global__ void __launch_bounds__(FTHREADS, 4) k_gfuse(FuseArgs A) {
         ex = comb(ex, e1);
     }
 #pragma unroll
-    for (int w = 0; w < FGTHREADS / 32; ++w) tot = comb(tot, S.wagg[w]);
+    for (int w = 0; w < C::GTHREADS / 32; ++w) tot = comb(tot, S.wagg[w]);
     // look-back for the heads and last head of all earlier tiles
     if (warp == 0) {
         uint4 pre = make_uint4(0u, 0u, 0u, 0u);
@@ -461,7 +474,7 @@ __global__ void __launch_bounds__(FTHREADS, 4) k_gfuse(FuseArgs A) {
     if (cnt && !skip) {
         const uint32_t end = obase + cnt;
         const uint32_t nv = (end - oal + 3u) / 4u;
-        for (uint32_t v = tid; v < nv; v += FTHREADS) {
+        for (uint32_t v = tid; v < nv; v += C::THREADS) {
             const uint32_t gi = oal + 4u * v;
             if (gi >= obase && gi + 3u < end) {
                 *reinterpret_cast<uint4*>(A.out + gi) = *reinterpret_cast<const uint4*>(&S.out[4u * v]);

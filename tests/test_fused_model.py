@@ -17,9 +17,14 @@ from oracle import wahgen as G
 
 ALL, H0, H1, MAXC = 0x7FFFFFFF, 0x80000000, 0xC0000000, 0x3FFFFFFF
 DT = 1024
-FT, FWARPS, FWPT, FGPT = 2048, 9, 8, 8
-FTHREADS, FGTHREADS, FROWS = FWARPS * 32, FT // FGPT, FT // FGPT
+FWPT, FGPT = 8, 8
 C_ZERO, C_ONE, C_MIXED = 0, 1, 2
+
+
+def shape(FT):
+    """FCfg<FT>: warps for FT + 3 word slots, FT / 8 group-phase threads."""
+    warps = (FT + 3 + FWPT * 32 - 1) // (FWPT * 32)
+    return warps * 32, FT // FGPT, FT // FGPT
 
 
 def wgroups(w):
@@ -38,9 +43,9 @@ def op2(op, a, b):
     return [a & b, a | b, a ^ b, a & ~b & ALL][op]
 
 
-def fidx(q):
+def fidx(q, FT):
     assert 0 <= q < FT
-    return (q % FGPT) * FROWS + q // FGPT
+    return (q % FGPT) * (FT // FGPT) + q // FGPT
 
 
 def gtile(w, groups):
@@ -57,7 +62,7 @@ def gtile(w, groups):
     return out
 
 
-def fuse_range(gt, n, g0, g1):
+def fuse_range(gt, n, g0, g1, FT):
     wi0, s0 = gt[g0 // DT]
     wi1, s1 = gt[(g1 + DT - 1) // DT]
     wend = wi1 + 1 if (wi1 < n and s1 < g1) else wi1
@@ -66,7 +71,7 @@ def fuse_range(gt, n, g0, g1):
     return wi0, s0, nw
 
 
-def fuse_len(w, k, wi0, nw, s0, g0, g1):
+def fuse_len(w, k, wi0, nw, s0, g0, g1, FT):
     if k < wi0 or k - wi0 >= nw:
         return 0
     c = wgroups(w)
@@ -79,8 +84,9 @@ def run_word(c, ln):
     return ((H1 if c else H0) | ln) if ln >= 2 else (ALL if c else 0)
 
 
-def model(op, xw, yw, groups):
-    """The words k_gfuse writes, and the popcount of m_vec."""
+def model(op, xw, yw, groups, FT=2048):
+    """The words k_gfuse<OP, FT> writes, and the popcount of m_vec."""
+    FTHREADS, FGTHREADS, FROWS = shape(FT)
     xw = [int(v) for v in xw]
     yw = [int(v) for v in yw]
     nx, ny = len(xw), len(yw)
@@ -93,8 +99,8 @@ def model(op, xw, yw, groups):
         g0 = t * FT
         g1 = min(g0 + FT, groups)
         ng = g1 - g0
-        xi0, xs0, xn = fuse_range(gx, nx, g0, g1)
-        yi0, ys0, yn = fuse_range(gy, ny, g0, g1)
+        xi0, xs0, xn = fuse_range(gx, nx, g0, g1, FT)
+        yi0, ys0, yn = fuse_range(gy, ny, g0, g1, FT)
         pat = [[None] * FT, [None] * FT]
         run = 0
         for tid in range(FTHREADS):
@@ -103,21 +109,21 @@ def model(op, xw, yw, groups):
             for j in range(FWPT):
                 wxv = xw[kx + j] if kx + j < xi0 + xn else 0
                 wyv = yw[ky + j] if ky + j < yi0 + yn else 0
-                packed = fuse_len(wxv, kx + j, xi0, xn, xs0, g0, g1) | (fuse_len(wyv, ky + j, yi0, yn, ys0, g0, g1) << 16)
+                packed = fuse_len(wxv, kx + j, xi0, xn, xs0, g0, g1, FT) | (fuse_len(wyv, ky + j, yi0, yn, ys0, g0, g1, FT) << 16)
                 ex = run
                 run += packed
                 assert (run & 0xFFFF) <= 2 * FT and (run >> 16) <= 2 * FT
                 for o, (w, ln, q) in enumerate(((wxv, packed & 0xFFFF, ex & 0xFFFF), (wyv, packed >> 16, ex >> 16))):
                     if ln and q < ng:
                         for e in range(min(ln, ng - q)):
-                            pat[o][fidx(q + e)] = wpattern(w)
+                            pat[o][fidx(q + e, FT)] = wpattern(w)
         for q in range(ng):
-            assert pat[0][fidx(q)] is not None and pat[1][fidx(q)] is not None, (t, q)
+            assert pat[0][fidx(q, FT)] is not None and pat[1][fidx(q, FT)] is not None, (t, q)
         thr = []
         for tid in range(FGTHREADS):
             q0 = tid * FGPT
             if tid > 0:
-                pr = op2(op, pat[0][fidx(q0 - 1)] or 0, pat[1][fidx(q0 - 1)] or 0)
+                pr = op2(op, pat[0][fidx(q0 - 1, FT)] or 0, pat[1][fidx(q0 - 1, FT)] or 0)
             elif g0 > 0:
                 pr = op2(op, wpattern(xw[xi0 if xs0 < g0 else xi0 - 1]), wpattern(yw[yi0 if ys0 < g0 else yi0 - 1]))
             else:
@@ -127,7 +133,7 @@ def model(op, xw, yw, groups):
             for e in range(FGPT):
                 q = q0 + e
                 inr = q < ng
-                rv = op2(op, pat[0][fidx(q)] if inr else 0, pat[1][fidx(q)] if inr else 0)
+                rv = op2(op, pat[0][fidx(q, FT)] if inr else 0, pat[1][fidx(q, FT)] if inr else 0)
                 r.append(rv)
                 c = cls_of(rv)
                 if inr:
@@ -208,8 +214,9 @@ def _expect(op, a, b):
     return G.canonicalize(g), g
 
 
+@pytest.mark.parametrize("FT", [1024, 2048, 4096])
 @pytest.mark.parametrize("seed", range(6))
-def test_model_equals_oracle(seed):
+def test_model_equals_oracle(seed, FT):
     rng = np.random.default_rng(100 + seed)
     styles = ["dense", "mixed", "short", "sparse", "canon"]
     ng = int(rng.integers(1, 3 * FT + 700)) if seed else 5 * FT
@@ -220,7 +227,7 @@ def test_model_equals_oracle(seed):
     a, b = G.serialize(wa), G.serialize(wb)
     for op in range(4):
         want, groups = _expect(op, a, b)
-        got, ones = model(op, wa, wb, ng)
+        got, ones = model(op, wa, wb, ng, FT)
         assert np.array_equal(got, np.asarray(want, np.uint32)), (seed, op)
         assert ones == sum(bin(v).count("1") for v in groups)
 

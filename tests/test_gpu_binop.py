@@ -99,33 +99,39 @@ def _full_size(gpu_ctx, density):
 
 class _engine:
     """A given engine for canonical-result operators
-    (WAHGPU_TUNE_DENSE_ENGINE): 3 two-pass, 4 single-pass (the default)."""
+    (WAHGPU_TUNE_DENSE_ENGINE: 3 two-pass, 4 single-pass, the default) and
+    tile size (WAHGPU_TUNE_DENSE_TILE)."""
 
-    def __init__(self, ctx, engine):
-        self.ctx, self.engine = ctx, engine
+    def __init__(self, ctx, engine, tile=2048):
+        self.ctx, self.engine, self.tile = ctx, engine, tile
 
     def __enter__(self):
         import libfastlib_b200 as L
-        self.old = self.ctx.get_tuning(L.TUNE_DENSE_ENGINE)
+        self.old = (self.ctx.get_tuning(L.TUNE_DENSE_ENGINE), self.ctx.get_tuning(L.TUNE_DENSE_TILE))
         self.ctx.set_tuning(L.TUNE_DENSE_ENGINE, self.engine)
+        self.ctx.set_tuning(L.TUNE_DENSE_TILE, self.tile)
 
     def __exit__(self, *exc):
         import libfastlib_b200 as L
-        self.ctx.set_tuning(L.TUNE_DENSE_ENGINE, self.old)
+        self.ctx.set_tuning(L.TUNE_DENSE_ENGINE, self.old[0])
+        self.ctx.set_tuning(L.TUNE_DENSE_TILE, self.old[1])
 
 
-@pytest.mark.parametrize("engine", [3, 4])
+ENGINES = [(3, 2048), (4, 1024), (4, 2048), (4, 4096)]
+
+
+@pytest.mark.parametrize("engine,tile", ENGINES)
 @pytest.mark.parametrize("density", [0.1, 0.5])
-def test_full_size_group_space_engines(gpu_ctx, density, engine):
-    """The two-pass and the single-pass group-space engines give the same
-    words at full size."""
-    with _engine(gpu_ctx, engine):
+def test_full_size_group_space_engines(gpu_ctx, density, engine, tile):
+    """The two-pass and the single-pass group-space engines (every tile
+    size of the latter) give the same words at full size."""
+    with _engine(gpu_ctx, engine, tile):
         _full_size(gpu_ctx, density)
 
 
-@pytest.mark.parametrize("engine", [3, 4])
-def test_many_tiles_fuzz_engines(gpu_ctx, engine):
-    with _engine(gpu_ctx, engine):
+@pytest.mark.parametrize("engine,tile", ENGINES)
+def test_many_tiles_fuzz_engines(gpu_ctx, engine, tile):
+    with _engine(gpu_ctx, engine, tile):
         _fuzz(gpu_ctx)
 
 

@@ -288,6 +288,19 @@ def main():
             for i, (A, B) in enumerate(dev):
                 A.binop_into(op, B, res[i][op])
 
+    # engine 0 (auto): the autotuner picks the dense-path engine and tile
+    # size on this step's dense-path calls (the reference's _d2 rule
+    # (|a| + |b|) * 31 > nbits), timed with CUDA events
+    dense_tuning = None
+    if args.dense_engine == 0:
+        from libfastlib_b200 import tune
+        dcalls = [(A, B, op, res[i][op]) for op in OPS for i, (A, B) in enumerate(dev)
+                  if (A.nwords() + B.nwords()) * 31 > NBITS]
+        if dcalls:
+            best, table = tune.tune_dense(ctx, dcalls)
+            dense_tuning = {"chosen": {"engine": best[0], "tile_groups": best[1]},
+                            "candidates_ms_per_step": {f"engine {e} tile {t}": round(v, 4) for (e, t), v in table.items()}}
+
     clk = ClockSampler(local)
     if not args.only:
         clk.start()
@@ -369,16 +382,20 @@ def main():
     peak, peak_kind = peaks()
     achieved = dense_b / (dense_ms / 1e3) / 1e9 if dense_ms > 0 else None
     traffic = None
-    engine_kernels = {0: "k_gop + k_gpack", 3: "k_gop + k_gpack", 1: "k_dense",
-                      2: "k_merge"}[args.dense_engine]
-    traffic_file = {0: "two_pass_traffic.json", 3: "two_pass_traffic.json", 1: "k_dense_traffic.json",
-                    2: "k_merge_traffic.json"}[args.dense_engine]
+    traffic_calls = []
+    engine = dense_tuning["chosen"]["engine"] if dense_tuning else (args.dense_engine or 4)
+    tile = dense_tuning["chosen"]["tile_groups"] if dense_tuning else args.dense_tile
+    engine_kernels = {4: f"k_gfuse (tile {tile})", 3: "k_gop + k_gpack", 1: "k_dense", 2: "k_merge"}[engine]
+    traffic_file = {4: f"k_gfuse_{tile}_traffic.json", 3: "two_pass_traffic.json", 1: "k_dense_traffic.json",
+                    2: "k_merge_traffic.json"}[engine]
     tp = os.path.join(ROOT, "profiles", traffic_file)
     if os.path.exists(tp):
         try:
+            # DRAM bytes per launch from one ncu capture of the named calls;
+            # the mean over the calls captured among this line's dense calls
             per = json.load(open(tp))["bytes_per_launch"]
-            got = [per[k] for k in dense_calls if k in per]
-            traffic = sum(got) / len(got) if got else None
+            traffic_calls = [k for k in dense_calls if k in per]
+            traffic = sum(per[k] for k in traffic_calls) / len(traffic_calls) if traffic_calls else None
         except Exception:
             traffic = None
 
@@ -482,7 +499,8 @@ def main():
                          "kernel": engine_kernels + " (+ the metadata memset), per-call CUDA events over the "
                                    "dense-path calls " + ", ".join(dense_calls),
                          "traffic_source": f"profiles/{traffic_file} (ncu dram__bytes_read.sum + "
-                                           "dram__bytes_write.sum per operator call)"},
+                                           "dram__bytes_write.sum per operator call), calls "
+                                           + (", ".join(traffic_calls) or "none captured")},
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "host_threads": len(ectx),
                     "timing": "wall clock around the calls, device synchronized, max over ranks"},
@@ -490,6 +508,7 @@ def main():
             "clocks": clocks,
             "gpu_launches": launches,
             "detail_call_ms": call_ms,
+            "dense_tuning": dense_tuning,
         }
         line.update(extra)
         print(json.dumps(line))

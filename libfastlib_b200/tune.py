@@ -2,14 +2,14 @@
 them): times each candidate on the caller's own workload with CUDA events
 and leaves the fastest set on the context.
 
-    best, table = tune_batch(ctx, batch)          # range batches
-    best, table = tune_dense_tile(ctx, a, b, op)  # dense-path operators
+    best, table = tune_batch(ctx, batch)                  # range batches
+    best, table = tune_dense(ctx, [(a, b, op, out), ...])  # dense-path operators
 """
 from __future__ import annotations
 
 import itertools
 
-from . import TUNE_DENSE_TILE, TUNE_RANGE_CTAS, TUNE_RANGE_ORDER
+from . import TUNE_DENSE_ENGINE, TUNE_DENSE_TILE, TUNE_RANGE_CTAS, TUNE_RANGE_ORDER
 
 
 def _time(fn, reps: int) -> float:
@@ -51,4 +51,21 @@ def tune_dense_tile(ctx, a, b, op: int, out, tiles=(1024, 2048, 4096), reps: int
         table[t] = _time(lambda: a.binop_into(op, b, out), reps)
     best = min(table, key=table.get)
     ctx.set_tuning(TUNE_DENSE_TILE, best)
+    return best, table
+
+
+def tune_dense(ctx, calls, engines=((4, 1024), (4, 2048), (4, 4096), (3, 2048)), reps: int = 5):
+    """Engine x tile size for the canonical-result (dense-path) operators,
+    timed on the caller's calls [(a, b, op, out), ...] together: the
+    single-pass group-space kernel at 1024 / 2048 / 4096 groups per tile
+    (its look-back chain shortens as tiles grow, its occupancy falls) and
+    the two-pass kernels.  Leaves the fastest set on the context."""
+    table = {}
+    for eng, tile in engines:
+        ctx.set_tuning(TUNE_DENSE_ENGINE, eng)
+        ctx.set_tuning(TUNE_DENSE_TILE, tile)
+        table[(eng, tile)] = _time(lambda: [a.binop_into(op, b, out) for a, b, op, out in calls], reps)
+    best = min(table, key=table.get)
+    ctx.set_tuning(TUNE_DENSE_ENGINE, best[0])
+    ctx.set_tuning(TUNE_DENSE_TILE, best[1])
     return best, table

@@ -112,17 +112,6 @@ __device__ __forceinline__ uint4 fuse_ld4(const uint32_t* __restrict__ w, uint32
     return v;
 }
 
-// Groups of the tile covered by slot word k (global index) of an operand
-// whose tile words are [wi0, wi0 + nw) with the first starting at s0;
-// clipped to the tile and to FT so 16-bit sums cannot overflow.
-__device__ __forceinline__ uint32_t fuse_len(uint32_t w, uint32_t k, uint32_t wi0, uint32_t nw, uint32_t s0,
-                                             uint32_t g0, uint32_t g1, uint32_t FT) {
-    if (k < wi0 || k - wi0 >= nw) return 0u;
-    uint32_t c = wgroups(w);
-    if (k == wi0) c = min(s0 + c, g1) - g0;
-    return min(c, FT);
-}
-
 // {heads, last head, ones, -}: sum, max, sum.  A last head is packed as
 // (group + 1) << 2 | class, so 0 means "none" and later heads compare larger.
 struct FuseComb {
@@ -264,9 +253,16 @@ __global__ void __launch_bounds__(FCfg<FT>::THREADS, FCfg<FT>::MINB) k_gfuse(Fus
     }
     uint32_t st[FWPT];  // inclusive sums of the packed lengths (x low, y high)
     uint32_t run = 0;
+    // slot j holds tile word kx + j - xi0 (valid when in [0, xn)); word 0
+    // may start before the tile and is clipped to it
+    const uint32_t rx = kx - xi0, ry = ky - yi0;
 #pragma unroll
     for (int j = 0; j < FWPT; ++j) {
-        run += fuse_len(wx[j], kx + j, xi0, xn, xs0, g0, g1, FT) | (fuse_len(wy[j], ky + j, yi0, yn, ys0, g0, g1, FT) << 16);
+        uint32_t lx = rx + j < xn ? min(wgroups(wx[j]), (uint32_t)FT) : 0u;
+        uint32_t ly = ry + j < yn ? min(wgroups(wy[j]), (uint32_t)FT) : 0u;
+        if (rx + j == 0u) lx = min(xs0 + wgroups(wx[j]), g1) - g0;
+        if (ry + j == 0u) ly = min(ys0 + wgroups(wy[j]), g1) - g0;
+        run += lx | (ly << 16);
         st[j] = run;
     }
     uint32_t inc = run;
@@ -287,24 +283,28 @@ __global__ void __launch_bounds__(FCfg<FT>::THREADS, FCfg<FT>::MINB) k_gfuse(Fus
         const uint32_t d = st[j] - (j ? st[j - 1] : 0u);
         const uint32_t lx = d & 0xFFFFu, ly = d >> 16;
         const uint32_t qx = ex & 0xFFFFu, qy = ex >> 16;
+        // a literal is one store; a short fill a short loop; a long fill
+        // goes to the whole warp below
         if (lx && qx < ng) {
-            const uint32_t p = wpattern(wx[j]);
             const uint32_t L = min(lx, ng - qx);
-            if (L <= (uint32_t)FSHORT) {
-#pragma unroll
-                for (uint32_t e = 0; e < (uint32_t)FSHORT; ++e)
-                    if (e < L) S.pat[0][fidx<FT>(qx + e)] = p;
+            if (L == 1u) {
+                S.pat[0][fidx<FT>(qx)] = wpattern(wx[j]);
+            } else if (L <= (uint32_t)FSHORT) {
+                const uint32_t p = wpattern(wx[j]);
+#pragma unroll 1
+                for (uint32_t q = qx; q < qx + L; ++q) S.pat[0][fidx<FT>(q)] = p;
             } else {
                 longx = true;
             }
         }
         if (ly && qy < ng) {
-            const uint32_t p = wpattern(wy[j]);
             const uint32_t L = min(ly, ng - qy);
-            if (L <= (uint32_t)FSHORT) {
-#pragma unroll
-                for (uint32_t e = 0; e < (uint32_t)FSHORT; ++e)
-                    if (e < L) S.pat[1][fidx<FT>(qy + e)] = p;
+            if (L == 1u) {
+                S.pat[1][fidx<FT>(qy)] = wpattern(wy[j]);
+            } else if (L <= (uint32_t)FSHORT) {
+                const uint32_t p = wpattern(wy[j]);
+#pragma unroll 1
+                for (uint32_t q = qy; q < qy + L; ++q) S.pat[1][fidx<FT>(q)] = p;
             } else {
                 longy = true;
             }
@@ -438,10 +438,16 @@ __global__ void __launch_bounds__(FCfg<FT>::THREADS, FCfg<FT>::MINB) k_gfuse(Fus
     if (!skip && grp && (hm || (last_tile && tid == 0 && tot.x == 0u))) {
         uint32_t o = obase + ex.x;
         uint32_t prevh = max(pre.y, ex.y);  // the head before my first one
+        // word idx: this tile's words go to shared memory; the last run of
+        // an earlier tile straight to its place (word 0 also to w0; tile 0
+        // sets w0 from its own words after the flush)
         auto emit = [&](uint32_t idx, uint32_t wd) {
-            if (idx >= obase) S.out[idx - oal] = wd;
-            else A.out[idx] = wd;  // the last run of an earlier tile
-            if (idx == 0u) A.meta->w0 = wd;
+            if (idx >= obase) {
+                S.out[idx - oal] = wd;
+            } else {
+                A.out[idx] = wd;
+                if (idx == 0u) A.meta->w0 = wd;
+            }
         };
 #pragma unroll
         for (int e = 0; e < FGPT; ++e) {
@@ -453,7 +459,7 @@ __global__ void __launch_bounds__(FCfg<FT>::THREADS, FCfg<FT>::MINB) k_gfuse(Fus
                     emit(o - 1u, wd);
                 }
                 const uint32_t c = cls_of(r[e]);
-                if (c == C_MIXED) emit(o, r[e]);
+                if (c == C_MIXED) S.out[o - oal] = r[e];
                 if ((o & 31u) == 0u) A.obp[o >> 5] = q;
                 prevh = ((q + 1u) << 2) | c;
                 ++o;
@@ -487,6 +493,7 @@ __global__ void __launch_bounds__(FCfg<FT>::THREADS, FCfg<FT>::MINB) k_gfuse(Fus
     }
     if (tid == 0) {
         if (S.fill) atomicOr(&A.meta->nfill, 1u);
+        if (obase == 0u && cnt && !skip) A.meta->w0 = S.out[0];
         if (last_tile) {
             const uint4 all = comb(pre, tot);
             const uint32_t n = skip ? 0u : all.x;

@@ -39,6 +39,7 @@ constexpr int RTHREADS = 256;
 constexpr int RWARPS = RTHREADS / 32;
 constexpr int RGPT = RT / RTHREADS;  // groups per thread in the epilogue
 constexpr uint32_t RDIRECT = 32;     // spans of at most this many bitmaps skip the tile lists
+constexpr int RCHK = 2;              // raw values in flight per lane in an edge-bin row check
 
 // per-bitmap metadata of an attached index
 struct BitmapMeta {
@@ -148,6 +149,12 @@ __device__ __forceinline__ bool pass_cmp(double v, uint32_t lop, double lo, uint
     const bool b = rop == 0 ? true : (rop == 1 ? v < hi : v <= hi);
     return a && b;
 }
+// a column value from its 4 raw bytes (0 uint32, 1 float32, 2 int32)
+__device__ __forceinline__ double raw_value(uint32_t v, uint32_t vtype) {
+    if (vtype == 1) return (double)__uint_as_float(v);
+    if (vtype == 2) return (double)(int32_t)v;
+    return (double)v;
+}
 __device__ __forceinline__ double col_value(const void* vals, uint32_t vtype, uint32_t row) {
     if (vtype == 1) return (double)__ldg(reinterpret_cast<const float*>(vals) + row);
     if (vtype == 2) return (double)__ldg(reinterpret_cast<const int32_t*>(vals) + row);
@@ -206,13 +213,24 @@ __device__ __forceinline__ void warp_or_bitmap(RangeShared& S, const DevIndex& I
                         if (pat == ALLONES) S.tmp[rsw(g - g0)] = ALLONES;
                         else atomicOr(&S.tmp[rsw(g - g0)], pat);
                     } else {
+                        // the rows of the group's 1 bits, RCHK raw values
+                        // loaded at once (one memory latency per RCHK rows)
                         uint32_t bits = pat, set = 0;
+                        const uint32_t* raw = reinterpret_cast<const uint32_t*>(I.values);
                         while (bits) {
-                            const uint32_t hb = 31u - __clz(bits);
-                            const uint32_t row = g * 31u + (30u - hb);
-                            if (pass_cmp(col_value(I.values, I.vtype, row), check->lop, check->lo, check->rop, check->hi))
-                                set |= 1u << hb;
-                            bits &= ~(1u << hb);
+                            uint32_t hb[RCHK], v[RCHK];
+#pragma unroll
+                            for (int k = 0; k < RCHK; ++k) {
+                                hb[k] = bits ? 31u - __clz(bits) : 32u;
+                                if (bits) bits &= ~(1u << hb[k]);
+                            }
+#pragma unroll
+                            for (int k = 0; k < RCHK; ++k)  // every column type is 4 bytes a row
+                                v[k] = hb[k] < 32u ? __ldg(raw + g * 31u + (30u - hb[k])) : 0u;
+#pragma unroll
+                            for (int k = 0; k < RCHK; ++k)
+                                if (hb[k] < 32u && pass_cmp(raw_value(v[k], I.vtype), check->lop, check->lo, check->rop, check->hi))
+                                    set |= 1u << hb[k];
                         }
                         if (set) atomicOr(&S.tmp[rsw(g - g0)], set);
                     }

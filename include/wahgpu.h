@@ -103,7 +103,10 @@ int64_t wahgpu_ctx_get_tuning(wahgpu_ctx* ctx, int key);
 int wahgpu_bv_from_serial(wahgpu_ctx* ctx, const uint32_t* words, uint64_t nwords,
                           wahgpu_bv** out);
 /* Same from a serialized array already in device memory (read on the
- * device; the trailer words are read back to the host). */
+ * device; the trailer words are read back to the host).  The words are read
+ * in order on the context's stream, which waits for no other stream: work
+ * still writing them on another stream must be ordered before the call
+ * (an event recorded there and waited on by wahgpu_ctx_stream's stream). */
 int wahgpu_bv_from_device_serial(wahgpu_ctx* ctx, const uint32_t* dev_words, uint64_t nwords,
                                  wahgpu_bv** out);
 /* An empty bitvector with room for `cap_words` whole words, for use as the
@@ -205,7 +208,8 @@ int wahgpu_index_set_values(wahgpu_index* idx, int vtype, const void* values, ui
  * never split between bins, and each bin's keys are the smallest and
  * largest value it holds; the raw values are kept for edge-bin row checks.
  * Every bitmap holds exactly the rows the reference's would; its words are
- * in compress() form. */
+ * in compress() form.  `dev_values` is read on the context's stream, as for
+ * wahgpu_bv_from_device_serial: order its producers before the call. */
 int wahgpu_index_build(wahgpu_ctx* ctx, int kind, int vtype, const void* dev_values, uint64_t nrows,
                        uint32_t nbins, wahgpu_index** out);
 /* Index files.  wahgpu_index_read replaces relic::read(const char*) and

@@ -185,6 +185,16 @@ class Context:
     def sync(self) -> None:
         self.check(self.lib.wahgpu_ctx_sync(self.h))
 
+    def after_torch(self, t) -> None:
+        """Orders the context's stream after the work torch has queued on
+        its current stream, so a CUDA tensor handed to the library is read
+        only once the kernels producing it are done (the context's own
+        stream is non-blocking: it does not wait for torch's by itself)."""
+        import torch
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.current_stream(t.device))
+        torch.cuda.ExternalStream(int(self.lib.wahgpu_ctx_stream(self.h) or 0), device=t.device).wait_event(ev)
+
     @property
     def launches(self) -> int:
         return int(self.lib.wahgpu_ctx_launches(self.h))
@@ -217,6 +227,7 @@ class Context:
         (host array, or a CUDA tensor of 32-bit words read on the device)."""
         if getattr(serial, "is_cuda", False):
             t = serial.contiguous()
+            self.after_torch(t)
             h = ctypes.c_void_p()
             self.check(self.lib.wahgpu_bv_from_device_serial(self.h, ctypes.c_void_p(t.data_ptr()), t.numel(),
                                                             ctypes.byref(h)))
@@ -364,6 +375,7 @@ class Index:
         if not t.is_cuda:
             t = t.to(f"cuda:{ctx.device}")
         t = t.contiguous()
+        ctx.after_torch(t)
         h = ctypes.c_void_p()
         ctx.check(ctx.lib.wahgpu_index_build(ctx.h, kind, vt, ctypes.c_void_p(t.data_ptr()), t.numel(), nbins,
                                              ctypes.byref(h)))

@@ -229,9 +229,9 @@ def main():
                     help="host threads (one context each) sharing the end-to-end leg's calls")
     ap.add_argument("--dense-tile", type=int, default=2048, choices=[1024, 2048, 4096],
                     help="groups per tile of the dense-path kernel")
-    ap.add_argument("--dense-engine", type=int, default=0, choices=[0, 1, 2, 3],
+    ap.add_argument("--dense-engine", type=int, default=0, choices=[0, 1, 2, 3, 4, 5],
                     help="canonical-result operators: 0 auto, 1 pipelined group-space kernel, 2 word-space merge, "
-                         "3 two-pass group-space kernels")
+                         "3 two-pass group-space kernels, 4 single pass over CTA tiles, 5 single pass over warp tiles")
     ap.add_argument("--only-range", default=None,
                     help="ROWS:QUERIES — only the binned range case at that size, tile-major count batch run "
                          "warmup+steps times (for ncu)")
@@ -383,11 +383,12 @@ def main():
     achieved = dense_b / (dense_ms / 1e3) / 1e9 if dense_ms > 0 else None
     traffic = None
     traffic_calls = []
-    engine = dense_tuning["chosen"]["engine"] if dense_tuning else (args.dense_engine or 4)
+    engine = dense_tuning["chosen"]["engine"] if dense_tuning else (args.dense_engine or 5)
     tile = dense_tuning["chosen"]["tile_groups"] if dense_tuning else args.dense_tile
-    engine_kernels = {4: f"k_gfuse (tile {tile})", 3: "k_gop + k_gpack", 1: "k_dense", 2: "k_merge"}[engine]
-    traffic_file = {4: f"k_gfuse_{tile}_traffic.json", 3: "two_pass_traffic.json", 1: "k_dense_traffic.json",
-                    2: "k_merge_traffic.json"}[engine]
+    engine_kernels = {5: "k_gone", 4: f"k_gfuse (tile {tile})", 3: "k_gop + k_gpack", 1: "k_dense",
+                      2: "k_merge"}[engine]
+    traffic_file = {5: "k_gone_traffic.json", 4: f"k_gfuse_{tile}_traffic.json", 3: "two_pass_traffic.json",
+                    1: "k_dense_traffic.json", 2: "k_merge_traffic.json"}[engine]
     tp = os.path.join(ROOT, "profiles", traffic_file)
     if os.path.exists(tp):
         try:

@@ -6,6 +6,7 @@
 #include "wah_kernels.cuh"
 #include "wah_gop.cuh"
 #include "wah_fuse.cuh"
+#include "wah_gone.cuh"
 #include "wah_api_internal.h"
 
 #include <cuda_runtime.h>
@@ -174,7 +175,7 @@ extern "C" int wahgpu_ctx_set_tuning(wahgpu_ctx* ctx, int key, int64_t value) {
         ctx->dense_tile = (uint32_t)value;
         return WAHGPU_OK;
     case WAHGPU_TUNE_DENSE_ENGINE:
-        if (value < 0 || value > 4) return wg_fail(ctx, WAHGPU_EINVAL, "dense engine must be 0, 1, 2, 3 or 4");
+        if (value < 0 || value > 5) return wg_fail(ctx, WAHGPU_EINVAL, "dense engine must be 0 .. 5");
         ctx->dense_engine = (uint32_t)value;
         return WAHGPU_OK;
     case WAHGPU_TUNE_RANGE_ORDER:
@@ -674,6 +675,62 @@ int wg_launch_fuse(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t
     return WAHGPU_OK;
 }
 
+// Single-pass warp-tile engine (wah_gone.cuh): one launch per call, one
+// warp per 1024-group tile, operands read once, words written once from
+// registers.
+int wg_launch_gone(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t groups,
+                   uint32_t anb, uint32_t aval, wahgpu_bv* res) {
+    int rc = bv_reserve(res, (uint64_t)x->h.n + y->h.n);
+    if (rc) return rc;
+    if (groups == 0) return wg_launch_gop(ctx, op, x, y, groups, anb, aval, res);
+    rc = wg_gtile(x);
+    if (rc) return rc;
+    rc = wg_gtile(y);
+    if (rc) return rc;
+    const uint32_t ntiles = (groups + GT - 1) / GT;
+    TileRec* recs; LaunchSync* sync;
+    rc = wg_scratch(ctx, ntiles, &recs, &sync);
+    if (rc) return rc;
+    FuseArgs a;
+    a.xw = x->words; a.xgt = x->gt; a.nx = x->h.n;
+    a.yw = y->words; a.ygt = y->gt; a.ny = y->h.n;
+    a.groups = groups; a.ntiles = ntiles;
+    a.out = res->words; a.obp = res->bpos; a.meta = res->meta; a.cap = res->cap;
+    a.recs = wg_fuse_recs(ctx, recs); a.sync = sync;
+    a.aval = aval; a.anb = anb;
+    a.withhold = ctx->test_withhold;
+    ctx->test_withhold = 0xFFFFFFFFu;
+    CUDA_TRY(ctx, cudaMemsetAsync(res->meta, 0, sizeof(DevMeta), ctx->stream));
+    const uint32_t grid = (ntiles + GWARPS - 1) / GWARPS;
+    const size_t sm = GWARPS * sizeof(GopWarp);
+    static PerDeviceSetup setup[4];
+    cudaStream_t s = ctx->stream;
+    switch (op) {
+    case OP_AND:
+        wg_kernel_setup(setup[0], ctx->device, k_gone<OP_AND>, GTHREADS, sm);
+        k_gone<OP_AND><<<grid, GTHREADS, sm, s>>>(a);
+        break;
+    case OP_OR:
+        wg_kernel_setup(setup[1], ctx->device, k_gone<OP_OR>, GTHREADS, sm);
+        k_gone<OP_OR><<<grid, GTHREADS, sm, s>>>(a);
+        break;
+    case OP_XOR:
+        wg_kernel_setup(setup[2], ctx->device, k_gone<OP_XOR>, GTHREADS, sm);
+        k_gone<OP_XOR><<<grid, GTHREADS, sm, s>>>(a);
+        break;
+    default:
+        wg_kernel_setup(setup[3], ctx->device, k_gone<OP_MINUS>, GTHREADS, sm);
+        k_gone<OP_MINUS><<<grid, GTHREADS, sm, s>>>(a);
+        break;
+    }
+    ctx->launches++;
+    CUDA_TRY(ctx, cudaGetLastError());
+    res->h_valid = false;
+    res->gt_valid = false;
+    res->compressed_form = true;
+    return WAHGPU_OK;
+}
+
 // A one-word device bitvector holding the collapsed form of an all-zero
 // operand (do_cnt(), src/bitvector.cpp:601-604).
 static int collapsed_copy(wahgpu_ctx* ctx, const wahgpu_bv* src, wahgpu_bv** out) {
@@ -718,7 +775,10 @@ static bool dense_two_pass(const wahgpu_ctx* ctx) {
     return ctx->dense_engine == 3;
 }
 static bool dense_fused(const wahgpu_ctx* ctx) {
-    return ctx->dense_engine == 0 || ctx->dense_engine == 4;
+    return ctx->dense_engine == 4;
+}
+static bool dense_warp_tiles(const wahgpu_ctx* ctx) {
+    return ctx->dense_engine == 0 || ctx->dense_engine == 5;
 }
 
 // adjustSize(0, nt) of a copy of b (src/bitvector.cpp:4086-4108): the copy
@@ -862,6 +922,8 @@ extern "C" int wahgpu_bv_binop_into(wahgpu_ctx* ctx, int op, int inplace, wahgpu
         // (no step states) when the tuning asks for it
         if (dense_in_word_space(ctx, ca, cb, G))
             rc = wg_launch_merge(ctx, op, false, false, false, ca, cb, G, anb, aval, res);
+        else if (dense_warp_tiles(ctx))
+            rc = wg_launch_gone(ctx, op, ca, cb, G, anb, aval, res);
         else if (dense_fused(ctx))
             rc = wg_launch_fuse(ctx, op, ca, cb, G, anb, aval, res);
         else if (dense_two_pass(ctx))

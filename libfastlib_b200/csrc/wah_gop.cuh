@@ -127,36 +127,40 @@ __device__ __forceinline__ uint4 gop_chunk(const uint32_t* ws, const uint16_t* m
                       wpattern(ws[i2 ? i2 - 1u : 0u]), wpattern(ws[i3 ? i3 - 1u : 0u]));
 }
 
-template <int OP>
-__global__ void __launch_bounds__(GTHREADS) k_gop(GopArgs A) {
-    extern __shared__ __align__(16) unsigned char gsm[];
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const uint32_t t = blockIdx.x * GWARPS + warp;
-    if (t >= A.ntiles) return;
-    GopWarp& W = reinterpret_cast<GopWarp*>(gsm)[warp];
-    const uint32_t G = A.groups;
-    const uint32_t g0 = t * (uint32_t)GT, g1 = min(g0 + (uint32_t)GT, G);
+// Result patterns of one warp's tile [g0, g1) of x OP y: both operands'
+// words over the tile are staged in shared memory at once with cp.async and
+// expanded to one 31-bit pattern per group (a word-start marker per word
+// and a warp max-scan find the word of every group, so a fill costs one
+// marker whatever its length; an operand with one word per group is read
+// directly).  Calls f(j, r) for the chunks j = 0..7 in order, r holding the
+// results of groups 128 j + 4 lane + e of the tile (e = 0..3; groups past
+// g1 hold whatever the zero-padded words give and must be ignored).  prev
+// is set to the result of group g0 - 1 (0 for g0 = 0).  Returns false for a
+// word range the metadata scan would have rejected (the patterns are then
+// meaningless).
+template <int OP, class F>
+__device__ __forceinline__ bool gop_tile(const uint32_t* __restrict__ xw, const uint32_t* __restrict__ xgt,
+                                         uint32_t nx, const uint32_t* __restrict__ yw,
+                                         const uint32_t* __restrict__ ygt, uint32_t ny, GopWarp& W, uint32_t g0,
+                                         uint32_t g1, uint32_t& prev, F&& f) {
+    const uint32_t lane = threadIdx.x & 31u;
     const uint32_t ng = g1 - g0;
     uint32_t xi0, xs0, xn, yi0, ys0, yn;
-    const bool ok = gop_range(A.xgt, A.nx, g0, g1, xi0, xs0, xn) & gop_range(A.ygt, A.ny, g0, g1, yi0, ys0, yn);
-    if (!ok && lane == 0) atomicExch(&A.meta->status, DEV_ERR_FORMAT);
+    const bool ok = gop_range(xgt, nx, g0, g1, xi0, xs0, xn) & gop_range(ygt, ny, g0, g1, yi0, ys0, yn);
     // both operands' words in flight at once
-    for (uint32_t i = lane; i < xn; i += 32) cp_async4(&W.ws[0][i], A.xw + xi0 + i);
-    for (uint32_t i = lane; i < yn; i += 32) cp_async4(&W.ws[1][i], A.yw + yi0 + i);
+    for (uint32_t i = lane; i < xn; i += 32) cp_async4(&W.ws[0][i], xw + xi0 + i);
+    for (uint32_t i = lane; i < yn; i += 32) cp_async4(&W.ws[1][i], yw + yi0 + i);
     const bool xpure = xs0 == g0 && xn == ng, ypure = ys0 == g0 && yn == ng;
     // the result before the tile (the words covering g0 - 1)
-    uint32_t prev = 0;
+    prev = 0;
     if (g0 > 0 && ok) {
-        const uint32_t xp = __ldg(A.xw + (xs0 < g0 ? xi0 : xi0 - 1u));
-        const uint32_t yp = __ldg(A.yw + (ys0 < g0 ? yi0 : yi0 - 1u));
+        const uint32_t xp = __ldg(xw + (xs0 < g0 ? xi0 : xi0 - 1u));
+        const uint32_t yp = __ldg(yw + (ys0 < g0 ? yi0 : yi0 - 1u));
         prev = op2<OP>(wpattern(xp), wpattern(yp));
     }
     cp_async_wait_all();
     __syncwarp();
-    uint32_t* R = A.R + g0;
-    uint32_t heads = 0, first = GNONE, popc = 0;
     uint32_t xc = 0, yc = 0;
-    uint32_t before = prev;  // the result of the group before the current chunk
     // an impure operand is placed first (its markers then its patterns);
     // two impure operands share the marker array one after the other, so
     // the second one's patterns are read in a second sweep
@@ -197,7 +201,25 @@ __global__ void __launch_bounds__(GTHREADS) k_gop(GopArgs A) {
         else a = gop_chunk(W.ws[0], W.mk, j, xc);
         if (ypure) b = pattern4(reinterpret_cast<const uint4*>(W.ws[1])[32 * j + lane]);
         else b = gop_chunk(W.ws[1], W.mk, j, yc);
-        const uint4 r = make_uint4(op2<OP>(a.x, b.x), op2<OP>(a.y, b.y), op2<OP>(a.z, b.z), op2<OP>(a.w, b.w));
+        f(j, make_uint4(op2<OP>(a.x, b.x), op2<OP>(a.y, b.y), op2<OP>(a.z, b.z), op2<OP>(a.w, b.w)));
+    }
+    return ok;
+}
+
+template <int OP>
+__global__ void __launch_bounds__(GTHREADS) k_gop(GopArgs A) {
+    extern __shared__ __align__(16) unsigned char gsm[];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t t = blockIdx.x * GWARPS + warp;
+    if (t >= A.ntiles) return;
+    GopWarp& W = reinterpret_cast<GopWarp*>(gsm)[warp];
+    const uint32_t G = A.groups;
+    const uint32_t g0 = t * (uint32_t)GT, g1 = min(g0 + (uint32_t)GT, G);
+    const uint32_t ng = g1 - g0;
+    uint32_t* R = A.R + g0;
+    uint32_t heads = 0, first = GNONE, popc = 0;
+    uint32_t before;  // the result of the group before the current chunk
+    const bool ok = gop_tile<OP>(A.xw, A.xgt, A.nx, A.yw, A.ygt, A.ny, W, g0, g1, before, [&](int j, uint4 r) {
         reinterpret_cast<uint4*>(R)[32 * j + lane] = r;
         uint32_t pb = __shfl_up_sync(0xffffffffu, r.w, 1);
         if (lane == 0) pb = before;
@@ -214,7 +236,8 @@ __global__ void __launch_bounds__(GTHREADS) k_gop(GopArgs A) {
             }
             pc = c;
         }
-    }
+    });
+    if (!ok && lane == 0) atomicExch(&A.meta->status, DEV_ERR_FORMAT);
     heads = __reduce_add_sync(0xffffffffu, heads);
     popc = __reduce_add_sync(0xffffffffu, popc);
     first = __reduce_min_sync(0xffffffffu, first);

@@ -54,12 +54,13 @@ def tune_dense_tile(ctx, a, b, op: int, out, tiles=(1024, 2048, 4096), reps: int
     return best, table
 
 
-def tune_dense(ctx, calls, engines=((4, 1024), (4, 2048), (4, 4096), (3, 2048)), reps: int = 5):
+def tune_dense(ctx, calls, engines=((5, 2048), (4, 1024), (4, 2048), (4, 4096), (3, 2048)), reps: int = 5):
     """Engine x tile size for the canonical-result (dense-path) operators,
     timed on the caller's calls [(a, b, op, out), ...] together: the
-    single-pass group-space kernel at 1024 / 2048 / 4096 groups per tile
-    (its look-back chain shortens as tiles grow, its occupancy falls) and
-    the two-pass kernels.  Leaves the fastest set on the context."""
+    single-pass kernel over warp tiles (5), the single-pass kernel over CTA
+    tiles of 1024 / 2048 / 4096 groups (4: its look-back chain shortens as
+    tiles grow, its occupancy falls) and the two-pass kernels (3).  Leaves
+    the fastest set on the context."""
     table = {}
     for eng, tile in engines:
         ctx.set_tuning(TUNE_DENSE_ENGINE, eng)

@@ -8,7 +8,8 @@ group phase's heads and popcount with the group before each thread, the
 the next head writes a uniform run's word (deferred across tiles) and the
 last tile the final run.  Every shared-memory and global index is asserted
 in range, so a change to that arithmetic can be tried here before it runs
-on a GPU."""
+on a GPU.  A second model follows the write phase of the warp-tile engine
+(wah_gone.cuh: k_gone) lane by lane and chunk by chunk."""
 import numpy as np
 import pytest
 
@@ -243,3 +244,96 @@ def test_model_geometric_runs():
             want, _ = _expect(op, a, b)
             got, _ = model(op, ba, bb, groups)
             assert np.array_equal(got, np.asarray(want, np.uint32)), (d, op)
+
+
+def model_warp_tiles(op, groups_a, groups_b, GT=1024):
+    """The words k_gone<OP> (libfastlib_b200/csrc/wah_gone.cuh) writes, from
+    the operands' group patterns (its expansion is the two-pass engine's,
+    checked on the GPU): per tile of GT groups the lane heads of chunks of
+    128 groups (lane l holding groups 4 l .. 4 l + 3), the look-back prefix
+    {heads, last head}, then the write phase in lane and chunk order with
+    every index asserted in range."""
+    G_ = len(groups_a)
+    r = [op2(op, int(a), int(b)) for a, b in zip(groups_a, groups_b)]
+    ntiles = (G_ + GT - 1) // GT
+    tiles = []
+    for t in range(ntiles):
+        g0, g1 = t * GT, min(t * GT + GT, G_)
+        heads, lasth = 0, 0
+        for q in range(g0, g1):
+            c = cls_of(r[q])
+            if q == 0 or c == C_MIXED or c != cls_of(r[q - 1]):
+                heads += 1
+                lasth = ((q + 1) << 2) | c
+        tiles.append((heads, lasth))
+    n = sum(h for h, _ in tiles)
+    out = [None] * n
+    pre_h, pre_l = 0, 0
+    for t in range(ntiles):
+        g0 = t * GT
+        heads, lasth = tiles[t]
+        acc, carry = pre_h, pre_l
+        for j in range(GT // 128):
+            lane_m = []
+            for lane in range(32):
+                q0 = g0 + 128 * j + 4 * lane
+                m = 0
+                for e in range(4):
+                    q = q0 + e
+                    if q < min(g0 + GT, G_):
+                        c = cls_of(r[q])
+                        pc = cls_of(r[q - 1]) if q > 0 else None
+                        if q == 0 or c == C_MIXED or c != pc:
+                            m |= 1 << e
+                lane_m.append(m)
+            mine = []
+            for lane, m in enumerate(lane_m):
+                v = 0
+                for e in range(4):
+                    if (m >> e) & 1:
+                        q = g0 + 128 * j + 4 * lane + e
+                        v = ((q + 1) << 2) | cls_of(r[q])
+                mine.append(v)
+            sums = np.cumsum([bin(m).count("1") for m in lane_m]).tolist()
+            for lane, m in enumerate(lane_m):
+                prevh = max([carry] + mine[:lane])
+                o = acc + sums[lane] - bin(m).count("1")
+                for e in range(4):
+                    if not (m >> e) & 1:
+                        continue
+                    q = g0 + 128 * j + 4 * lane + e
+                    if prevh and (prevh & 3) != C_MIXED:
+                        assert 1 <= o <= n
+                        out[o - 1] = run_word(prevh & 3, q - ((prevh >> 2) - 1))
+                    c = cls_of(r[q])
+                    if c == C_MIXED:
+                        assert 0 <= o < n
+                        out[o] = r[q]
+                    prevh = ((q + 1) << 2) | c
+                    o += 1
+            acc += sums[-1]
+            carry = max([carry] + mine)
+        if t == ntiles - 1 and carry and (carry & 3) != C_MIXED:
+            assert 1 <= acc <= n
+            out[acc - 1] = run_word(carry & 3, G_ - ((carry >> 2) - 1))
+        pre_h, pre_l = pre_h + heads, max(pre_l, lasth)
+    assert all(v is not None for v in out)
+    return np.array(out, dtype=np.uint32)
+
+
+@pytest.mark.parametrize("seed", range(5))
+def test_warp_tile_model_equals_oracle(seed):
+    rng = np.random.default_rng(300 + seed)
+    styles = ["dense", "mixed", "short", "sparse", "canon"]
+    ng = int(rng.integers(1, 3 * 1024 + 700)) if seed else 4 * 1024
+    wa = G.random_words(rng, ng, styles[seed % 5])
+    wb = G.random_words(rng, ng, styles[(seed + 1) % 5])
+    if seed == 3:
+        wa = [G.fill(1, ng)]  # one run over every tile
+    a, b = G.serialize(wa), G.serialize(wb)
+    _, ga = _expect(0, a, a)
+    _, gb = _expect(0, b, b)
+    for op in range(4):
+        want, _ = _expect(op, a, b)
+        got = model_warp_tiles(op, ga, gb)
+        assert np.array_equal(got, np.asarray(want, np.uint32)), (seed, op)

@@ -99,8 +99,9 @@ def _full_size(gpu_ctx, density):
 
 class _engine:
     """A given engine for canonical-result operators
-    (WAHGPU_TUNE_DENSE_ENGINE: 3 two-pass, 4 single-pass, the default) and
-    tile size (WAHGPU_TUNE_DENSE_TILE)."""
+    (WAHGPU_TUNE_DENSE_ENGINE: 3 two-pass, 4 single-pass CTA tiles, 5
+    single-pass warp tiles, the default) and tile size
+    (WAHGPU_TUNE_DENSE_TILE, used by engine 4)."""
 
     def __init__(self, ctx, engine, tile=2048):
         self.ctx, self.engine, self.tile = ctx, engine, tile
@@ -117,14 +118,14 @@ class _engine:
         self.ctx.set_tuning(L.TUNE_DENSE_TILE, self.old[1])
 
 
-ENGINES = [(3, 2048), (4, 1024), (4, 2048), (4, 4096)]
+ENGINES = [(3, 2048), (4, 1024), (4, 2048), (4, 4096), (5, 2048)]
 
 
 @pytest.mark.parametrize("engine,tile", ENGINES)
 @pytest.mark.parametrize("density", [0.1, 0.5])
 def test_full_size_group_space_engines(gpu_ctx, density, engine, tile):
     """The two-pass and the single-pass group-space engines (every tile
-    size of the latter) give the same words at full size."""
+    size of the CTA-tile one) give the same words at full size."""
     with _engine(gpu_ctx, engine, tile):
         _full_size(gpu_ctx, density)
 
@@ -249,9 +250,10 @@ def test_dense_path_fuzz(gpu_ctx, tile):
                     assert c == rc and np.array_equal(w, ref), (trial, op, ip)
 
 
-@pytest.mark.parametrize("engine", [1, 3])
+@pytest.mark.parametrize("engine", [1, 3, 4, 5])
 def test_group_space_engines_fuzz(gpu_ctx, engine):
-    """Both group-space engines (1 pipelined, 3 two-pass): dense operands
+    """The group-space engines (1 pipelined, 3 two-pass, 4 and 5 single
+    pass): dense operands
     with fills longer than a tile, pure and impure tiles, count-1
     fill words among literals, partial last tiles."""
     import libfastlib_b200 as L

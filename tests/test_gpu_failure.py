@@ -24,12 +24,13 @@ def _pair():
     return a, b
 
 
-def test_withheld_record_times_out(gpu_ctx):
+@pytest.mark.parametrize("engine", [4, 5])
+def test_withheld_record_times_out(gpu_ctx, engine):
     import libfastlib_b200 as L
     a, b = _pair()
     A, B = gpu_ctx.bitvector(a), gpu_ctx.bitvector(b)
     old = gpu_ctx.get_tuning(L.TUNE_DENSE_ENGINE)
-    gpu_ctx.set_tuning(L.TUNE_DENSE_ENGINE, 4)
+    gpu_ctx.set_tuning(L.TUNE_DENSE_ENGINE, engine)
     try:
         gpu_ctx.set_tuning(L.TEST_WITHHOLD_TILE, 1)
         with pytest.raises(L.WahError) as e:

@@ -676,8 +676,7 @@ int wg_launch_fuse(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t
 }
 
 // Single-pass warp-tile engine (wah_gone.cuh): one launch per call, one
-// warp per 1024-group tile, operands read once, words written once from
-// registers.
+// warp per 1024-group tile, operands read once, words written once.
 int wg_launch_gone(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t groups,
                    uint32_t anb, uint32_t aval, wahgpu_bv* res) {
     int rc = bv_reserve(res, (uint64_t)x->h.n + y->h.n);
@@ -702,7 +701,7 @@ int wg_launch_gone(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t
     ctx->test_withhold = 0xFFFFFFFFu;
     CUDA_TRY(ctx, cudaMemsetAsync(res->meta, 0, sizeof(DevMeta), ctx->stream));
     const uint32_t grid = (ntiles + GWARPS - 1) / GWARPS;
-    const size_t sm = GWARPS * sizeof(GopWarp);
+    const size_t sm = GWARPS * sizeof(GoneWarp);
     static PerDeviceSetup setup[4];
     cudaStream_t s = ctx->stream;
     switch (op) {

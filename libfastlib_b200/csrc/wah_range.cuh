@@ -361,46 +361,45 @@ __global__ void __launch_bounds__(RTHREADS, 6) k_range(RangeArgs A) {
 #pragma unroll
                 for (uint32_t l = tid; l < RT / 4; l += RTHREADS) t4[l] = make_uint4(0u, 0u, 0u, 0u);
             }
-            // the bitmaps to OR: with cumulative rows the edge spans
-            // [h0, e0) u [e1, h1) and a plain span of at most RDIRECT
-            // bitmaps are walked directly (one that misses the tile costs
-            // its tile-index lookup); wider spans and complements take the
-            // entries of the tile's list that hold a 1 bit in it
+            // the bitmaps to OR, as two ranges: with cumulative rows the
+            // edge spans [h0, e0) and [e1, h1), else the span [h0, h1) or
+            // the complement [0, h0) and [h1, nobs).  Ranges of at most
+            // RDIRECT bitmaps in all are walked directly (one that misses
+            // the tile costs its tile-index lookup); wider ones take the
+            // entries of the tile's list of bitmaps holding a 1 bit in it
+            // that fall in the ranges (lower bounds by 16-lane searches)
             const bool flip = T.flip != 0u;
-            const bool direct = T.c1 || (!flip && T.h1 - T.h0 <= RDIRECT);
-            if (!direct && warp == 0) {
+            uint32_t ra0, ra1, rb0, rb1;  // bitmap ids [ra0, ra1) u [rb0, rb1)
+            if (T.c1) { ra0 = T.h0; ra1 = T.e0; rb0 = T.e1; rb1 = T.h1; }
+            else if (flip) { ra0 = 0u; ra1 = T.h0; rb0 = T.h1; rb1 = I.nobs; }
+            else { ra0 = T.h0; ra1 = T.h1; rb0 = rb1 = T.h1; }
+            const bool direct = !flip && (ra1 - ra0) + (rb1 - rb0) <= RDIRECT;
+            if (!direct && warp < 2) {
                 const uint32_t o0 = __ldg(I.tl_off + k), o1 = __ldg(I.tl_off + k + 1);
                 const uint32_t gbase = lane & 16u;
-                const uint32_t r = group16_lower_bound(I.tl_bm + o0, o1 - o0, gbase ? T.h1 : T.h0, gbase, lane & 15u);
-                if (lane == 0) { S.hdr[2] = o0; S.hdr[3] = o0 + r; }
-                if (lane == 16) { S.hdr[4] = o0 + r; S.hdr[5] = o1; }
+                const uint32_t v = warp == 0 ? (gbase ? ra1 : ra0) : (gbase ? rb1 : rb0);
+                const uint32_t r = group16_lower_bound(I.tl_bm + o0, o1 - o0, v, gbase, lane & 15u);
+                if ((lane & 15u) == 0) S.hdr[2 + 2 * warp + (gbase >> 4)] = o0 + r;
             }
             __syncthreads();
             // one job list per term: the edge bitmaps' row checks first
             // (the longest jobs), then the bitmaps to OR; a complement is
             // flipped before the checked rows join it
             const uint32_t nc = flip ? 0u : T.ncand;
-            uint32_t nsel, ne0 = 0, o0 = 0, e0 = 0, e1 = 0;
-            if (direct) {
-                ne0 = T.c1 ? T.e0 - T.h0 : T.h1 - T.h0;
-                nsel = T.c1 ? ne0 + (T.h1 - T.e1) : ne0;
-            } else {
-                // entries of the tile list: [o0, e0) u [e1, o1) (complement),
-                // or [e0, e1) (the plain span)
-                o0 = S.hdr[2]; e0 = S.hdr[3]; e1 = S.hdr[4];
-                const uint32_t o1 = S.hdr[5];
-                nsel = flip ? (e0 - o0) + (o1 - e1) : (e1 - e0);
+            uint32_t sa = ra0, sb = rb0, na = ra1 - ra0, nb = rb1 - rb0;  // the two ranges' starts and sizes
+            if (!direct) {  // as entries of the tile list
+                sa = S.hdr[2]; na = S.hdr[3] - sa;
+                sb = S.hdr[4]; nb = S.hdr[5] - sb;
             }
+            const uint32_t nsel = na + nb;
             for (uint32_t j = warp; j < nc + nsel; j += RWARPS) {
                 if (j < nc) {
                     warp_or_bitmap(S, I, T.cand[j], k, g0, g1, G, anb, &T);
                     continue;
                 }
                 const uint32_t jj = j - nc;
-                uint32_t b;
-                if (direct) b = jj < ne0 ? T.h0 + jj : T.e1 + (jj - ne0);
-                else if (flip) b = __ldg(I.tl_bm + (jj < e0 - o0 ? o0 + jj : e1 + (jj - (e0 - o0))));
-                else b = __ldg(I.tl_bm + e0 + jj);
+                const uint32_t e = jj < na ? sa + jj : sb + (jj - na);
+                const uint32_t b = direct ? e : __ldg(I.tl_bm + e);
                 warp_or_bitmap(S, I, b, k, g0, g1, G, anb, nullptr);
             }
             if (flip) {

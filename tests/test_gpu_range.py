@@ -250,7 +250,9 @@ def test_cumulative_rows_any_stride(gpu_ctx):
                     hi = sv[-1] + 1           # to above the largest
                 spans.append((float(lo), float(hi) + (0.5 if i % 2 else 0.0)))
             want = [np.flatnonzero((f >= lo) & (f < hi)) for lo, hi in spans]
-            for stride in (1, 2, 3, 8, 0):
+            # 40 and 300: edge spans wider than the direct walk, taken from
+            # the tile lists
+            for stride in (1, 2, 3, 8, 40, 300, 0):
                 gpu_ctx.set_tuning(L.TUNE_CUM_STRIDE, stride)
                 idx = L.Index.build(gpu_ctx, kind, vals, **kw)
                 B = L.Batch(gpu_ctx, [[idx.term(lo, hi)] for lo, hi in spans], rid_cap=sum(len(w) for w in want))

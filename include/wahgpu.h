@@ -85,6 +85,7 @@ int64_t wahgpu_ctx_launches(wahgpu_ctx* ctx);
                                      placed by a count pass and a scan */
 #define WAHGPU_TUNE_RANGE_CTAS 3  /* resident CTAs per SM of the persistent range launch: 0 (all that fit) .. 32 */
 #define WAHGPU_TUNE_CUM_STRIDE 5  /* bitmaps per cumulative row of indexes built or attached later: 0 auto, 1 none, >= 2 that stride */
+#define WAHGPU_TUNE_MERGE_TILE 6  /* block-index entries per tile of the word-space merge: 0 auto (by operand size), 16 | 32 | 64 */
 /* Failure-path test hooks (no counterpart in the reference; never needed in
  * normal use).  WAHGPU_TEST_WITHHOLD_TILE = t: in the next operator call on
  * the single-pass group-space engine, tile t never publishes its look-back

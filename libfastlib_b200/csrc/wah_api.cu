@@ -143,8 +143,6 @@ extern "C" int wahgpu_ctx_create(int device, wahgpu_ctx** out) {
         delete c;
         return wg_fail(nullptr, WAHGPU_ENOMEM, "pinned staging allocation failed");
     }
-    // the merge kernel uses more than the default 48 KB of shared memory only
-    // when TILE_BLOCKS grows; the attribute is set once here
     *out = c;
     return WAHGPU_OK;
 }
@@ -193,6 +191,11 @@ extern "C" int wahgpu_ctx_set_tuning(wahgpu_ctx* ctx, int key, int64_t value) {
         if (value < 0) return wg_fail(ctx, WAHGPU_EINVAL, "allocation count must be >= 0");
         ctx->test_fail_alloc = value;
         return WAHGPU_OK;
+    case WAHGPU_TUNE_MERGE_TILE:
+        if (value != 0 && value != 16 && value != 32 && value != 64)
+            return wg_fail(ctx, WAHGPU_EINVAL, "merge tile must be 0 (auto), 16, 32 or 64 entries, not %lld", (long long)value);
+        ctx->merge_tile = (uint32_t)value;
+        return WAHGPU_OK;
     case WAHGPU_TUNE_CUM_STRIDE:
         if (value < 0 || value > (1 << 30)) return wg_fail(ctx, WAHGPU_EINVAL, "cumulative stride must be 0 (auto), 1 (none) or a stride");
         ctx->cum_stride = (uint32_t)value;
@@ -209,6 +212,7 @@ extern "C" int64_t wahgpu_ctx_get_tuning(wahgpu_ctx* ctx, int key) {
     case WAHGPU_TUNE_RANGE_ORDER: return ctx->range_order;
     case WAHGPU_TUNE_RANGE_CTAS: return ctx->range_ctas;
     case WAHGPU_TUNE_CUM_STRIDE: return ctx->cum_stride;
+    case WAHGPU_TUNE_MERGE_TILE: return ctx->merge_tile;
     default: return wg_fail(ctx, WAHGPU_EINVAL, "unknown tuning key %d", key);
     }
 }
@@ -423,21 +427,43 @@ static uint32_t combine_active(int op, uint32_t a, uint32_t b) {
     }
 }
 
-// Launches one instantiation of the merge kernel; its shared-memory opt-in
-// above 48 KB is made on first use.
-template <int OP, bool FSM, bool UNARY, bool FLIP>
-static void launch_k(dim3 g, size_t sm, cudaStream_t s, const MergeArgs& a) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_merge<OP, FSM, UNARY, FLIP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        attr = true;
-    }
-    k_merge<OP, FSM, UNARY, FLIP><<<g, MERGE_THREADS, sm, s>>>(a);
+// Launches one instantiation of the merge kernel (its shared-memory
+// attribute set once per device).
+template <int OP, bool FSM, bool UNARY, bool FLIP, int TB>
+static void launch_k(const wahgpu_ctx* ctx, dim3 g, cudaStream_t s, const MergeArgs& a) {
+    static PerDeviceSetup setup;
+    const size_t sm = sizeof(TileShared<TB>);
+    wg_kernel_setup(setup, ctx->device, k_merge<OP, FSM, UNARY, FLIP, TB>, MERGE_THREADS, sm);
+    k_merge<OP, FSM, UNARY, FLIP, TB><<<g, MERGE_THREADS, sm, s>>>(a);
 }
-template <int OP>
-static void launch_merge_op(bool fsm, dim3 g, size_t sm, cudaStream_t s, const MergeArgs& a) {
-    if (fsm) launch_k<OP, true, false, false>(g, sm, s, a);
-    else launch_k<OP, false, false, false>(g, sm, s, a);
+template <int TB>
+static void launch_merge_tb(const wahgpu_ctx* ctx, int op, bool fsm, bool unary, bool flip, dim3 g, cudaStream_t s,
+                            const MergeArgs& a) {
+    if (unary) {
+        if (flip) launch_k<0, false, true, true, TB>(ctx, g, s, a);
+        else launch_k<0, false, true, false, TB>(ctx, g, s, a);
+        return;
+    }
+#define WG_MERGE_OP(O)                                                          \
+    if (fsm) launch_k<O, true, false, false, TB>(ctx, g, s, a);                 \
+    else launch_k<O, false, false, false, TB>(ctx, g, s, a);
+    switch (op) {
+    case OP_AND: WG_MERGE_OP(OP_AND) break;
+    case OP_OR: WG_MERGE_OP(OP_OR) break;
+    case OP_XOR: WG_MERGE_OP(OP_XOR) break;
+    default: WG_MERGE_OP(OP_MINUS) break;
+    }
+#undef WG_MERGE_OP
+}
+// Block-index entries per merge tile: the context's setting, else by the
+// operands' size: the largest of 64 / 32 / 16 that still gives about two
+// tiles per SM, so small operands spread over the GPU in short tiles.
+static uint32_t merge_tile_blocks(const wahgpu_ctx* ctx, uint32_t nblocks) {
+    if (ctx->merge_tile) return ctx->merge_tile;
+    const uint64_t want = 2ull * (uint64_t)ctx->sm_count;
+    if ((uint64_t)nblocks >= want * 64u) return 64;
+    if ((uint64_t)nblocks >= want * 32u) return 32;
+    return 16;
 }
 
 // Merge launch: x OP y, or a (complemented) copy of x when y == nullptr.
@@ -449,7 +475,9 @@ int wg_launch_merge(wahgpu_ctx* ctx, int op, bool fsm, bool unary, bool flip,
     const uint32_t need = nx + ny;
     int rc = bv_reserve(res, need);
     if (rc) return rc;
-    uint32_t ntiles = unary ? (nbx + TILE_BLOCKS - 1) / TILE_BLOCKS : (nbx + nby + TILE_BLOCKS - 1) / TILE_BLOCKS;
+    const uint32_t nblk = unary ? nbx : nbx + nby;
+    const uint32_t tb = merge_tile_blocks(ctx, nblk);
+    uint32_t ntiles = (nblk + tb - 1) / tb;
     if (ntiles == 0) ntiles = 1;
     TileRec* recs; LaunchSync* sync;
     rc = wg_scratch(ctx, ntiles, &recs, &sync);
@@ -462,20 +490,10 @@ int wg_launch_merge(wahgpu_ctx* ctx, int op, bool fsm, bool unary, bool flip,
     a.recs = recs; a.sync = sync; a.ntiles = ntiles;
     a.aval = aval; a.anb = anb;
     CUDA_TRY(ctx, cudaMemsetAsync(res->meta, 0, sizeof(DevMeta), ctx->stream));
-    const size_t sm = sizeof(TileShared);
     dim3 g(ntiles);
-    cudaStream_t s = ctx->stream;
-    if (unary) {
-        if (flip) launch_k<0, false, true, true>(g, sm, s, a);
-        else launch_k<0, false, true, false>(g, sm, s, a);
-    } else {
-        switch (op) {
-        case OP_AND: launch_merge_op<OP_AND>(fsm, g, sm, s, a); break;
-        case OP_OR: launch_merge_op<OP_OR>(fsm, g, sm, s, a); break;
-        case OP_XOR: launch_merge_op<OP_XOR>(fsm, g, sm, s, a); break;
-        default: launch_merge_op<OP_MINUS>(fsm, g, sm, s, a); break;
-        }
-    }
+    if (tb == 16) launch_merge_tb<16>(ctx, op, fsm, unary, flip, g, ctx->stream, a);
+    else if (tb == 32) launch_merge_tb<32>(ctx, op, fsm, unary, flip, g, ctx->stream, a);
+    else launch_merge_tb<64>(ctx, op, fsm, unary, flip, g, ctx->stream, a);
     ctx->launches++;
     CUDA_TRY(ctx, cudaGetLastError());
     res->h_valid = false;

@@ -30,14 +30,16 @@ namespace wah {
 #ifndef WAH_MERGE_THREADS
 #define WAH_MERGE_THREADS 256
 #endif
-#ifndef WAH_MERGE_TILE_BLOCKS
-#define WAH_MERGE_TILE_BLOCKS 64
-#endif
 constexpr int MERGE_THREADS = WAH_MERGE_THREADS;
-constexpr int TILE_BLOCKS = WAH_MERGE_TILE_BLOCKS;             // bpos entries per tile
-constexpr int TILE_WORDS = 32 * (TILE_BLOCKS + 2);            // max words held per operand
-// events per thread: a tile holds at most TILE_WORDS words of both operands together
-constexpr int SEG_PER_THREAD = (TILE_WORDS + MERGE_THREADS - 1) / MERGE_THREADS;
+// Tile shape: TB bpos entries per tile (16, 32 or 64: WAHGPU_TUNE_MERGE_TILE;
+// small tiles give small operands more CTAs and each a shorter chain).
+template <int TB>
+struct MCfg {
+    static constexpr int TILE_BLOCKS = TB;
+    static constexpr int TILE_WORDS = 32 * (TB + 2);  // max words held per operand
+    // events per thread: a tile holds at most TILE_WORDS words of both operands together
+    static constexpr int SEG_PER_THREAD = (TILE_WORDS + MERGE_THREADS - 1) / MERGE_THREADS;
+};
 
 struct MergeArgs {
     const uint32_t* xw;   // lhs words
@@ -143,11 +145,12 @@ __device__ __forceinline__ uint32_t warp_merge_split(const uint32_t* a, uint32_t
     return lo;
 }
 
+template <int TB>
 struct TileShared {
-    uint32_t wx[TILE_WORDS];
-    uint32_t ex[TILE_WORDS];  // end position of each held x word
-    uint32_t wy[TILE_WORDS];
-    uint32_t ey[TILE_WORDS];
+    uint32_t wx[MCfg<TB>::TILE_WORDS];
+    uint32_t ex[MCfg<TB>::TILE_WORDS];  // end position of each held x word
+    uint32_t wy[MCfg<TB>::TILE_WORDS];
+    uint32_t ey[MCfg<TB>::TILE_WORDS];
     uint32_t warp_agg[MERGE_THREADS / 32][4];
     uint32_t tile_prefix[4];
     uint32_t hdr[16];  // tile geometry broadcast
@@ -194,8 +197,10 @@ struct SegRec {
     uint32_t pos, val, bits;  // bits: trans(20) | cls<<20 | head<<22 | xfill<<23 | yfill<<24
 };
 
-template <int OP, bool FSM, bool UNARY, bool FLIP>
+template <int OP, bool FSM, bool UNARY, bool FLIP, int TB>
 __global__ void __launch_bounds__(MERGE_THREADS, 2) k_merge(MergeArgs A) {
+    constexpr int TILE_BLOCKS = TB, SEG_PER_THREAD = MCfg<TB>::SEG_PER_THREAD;
+    using TileShared = wah::TileShared<TB>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TileShared& S = *reinterpret_cast<TileShared*>(smem_raw);
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;

@@ -356,3 +356,27 @@ def test_unequal_sizes(gpu_ctx):
                 assert c == rc and np.array_equal(w, ref), (trial, op, ip, len(a), len(b))
                 checked += 1
     assert checked > 300
+
+
+@pytest.mark.parametrize("tile", [16, 32, 64])
+def test_merge_tile_sizes(gpu_ctx, tile):
+    """The word-space merge at every tile size (WAHGPU_TUNE_MERGE_TILE):
+    the many-tile fuzz, the sparse full-size pairs and unary copies."""
+    import libfastlib_b200 as L
+    gpu_ctx.set_tuning(L.TUNE_MERGE_TILE, tile)
+    try:
+        _fuzz(gpu_ctx)
+        for density in (1e-4, 1e-2):
+            _full_size(gpu_ctx, density)
+        rng = np.random.default_rng(90 + tile)
+        for style in ("sparse", "mixed"):
+            src = G.serialize(G.random_words(rng, 60000, style))
+            A = gpu_ctx.bitvector(src)
+            A.compress()
+            ref, cnt = oracle.compress(src)
+            assert np.array_equal(A.write(), ref) and A.cnt() == cnt, style
+            B = gpu_ctx.bitvector(src)
+            B.flip()
+            assert np.array_equal(B.write(), oracle.flip(src)), style
+    finally:
+        gpu_ctx.set_tuning(L.TUNE_MERGE_TILE, 0)

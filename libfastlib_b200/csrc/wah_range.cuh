@@ -23,9 +23,10 @@
 // index in shared memory; a span covering whole blocks of the index's
 // cumulative rows starts as C(k1) & ~C(k0) read as 16-byte vectors, and the
 // remaining bitmaps (the edges of such a span, a short span, or the tile's
-// list of bitmaps holding a 1 bit in it) form one job list with the edge
-// bins' row checks: each warp walks a bitmap's words for the tile 128 at a
-// time (positions by ballot / scan) into a shared-memory accumulator.  The
+// list of bitmaps holding a 1 bit in it) are OR'ed into a shared-memory
+// accumulator: a bitmap with a few words over the tile by one lane (32 such
+// bitmaps per warp at once), a longer one and each edge bin's row check by a
+// whole warp walking its words 128 at a time (positions by ballot / scan).  The
 // term result is AND'ed into the query result; a tile whose AND is empty
 // skips the query's remaining terms.
 #ifndef WAH_RANGE_CUH
@@ -258,6 +259,65 @@ __device__ __forceinline__ void warp_or_bitmap(RangeShared& S, const DevIndex& I
     }
 }
 
+// Bitmaps with at most LSHORT words over the tile are OR'ed by one lane
+// each; longer ones (or one holding a 1-fill longer than LFILL groups of
+// the tile) by the whole warp.
+constexpr uint32_t LSHORT = 4, LFILL = 8;
+
+// One lane per bitmap: lane l ORs bitmap b (valid when `have`) into S.tmp
+// when its words over the tile are few: its metadata, tile-index entries
+// and words are loaded by all lanes at once, so 32 sparse bitmaps cost
+// three memory round trips instead of three each.  The bitmaps left over
+// are OR'ed by the whole warp, one after the other.
+__device__ __forceinline__ void lanes_or_bitmaps(RangeShared& S, const DevIndex& I, bool have, uint32_t b,
+                                                 uint32_t k, uint32_t g0, uint32_t g1, uint32_t G, uint32_t anb) {
+    uint32_t i0 = 0, i1 = 0, s0 = 0, gb = 0, banb = 0, aval = 0;
+    uint64_t wstart = 0;
+    if (have) {
+        const BitmapMeta* m = I.bm + b;
+        const uint32_t* tix = I.tiles + ((size_t)b * (I.ntiles + 1) + k) * 2;
+        wstart = __ldg(&m->wstart);
+        const uint32_t n = __ldg(&m->n);
+        banb = __ldg(&m->anb); aval = __ldg(&m->aval); gb = __ldg(&m->groups);
+        i0 = __ldg(tix); s0 = __ldg(tix + 1);
+        const uint32_t in1 = __ldg(tix + 2), sn1 = __ldg(tix + 3);
+        i1 = min(sn1 < g1 ? in1 + 1u : in1, n);
+    }
+    bool lng = have && i1 > i0 + LSHORT;
+    if (have && !lng) {
+        const uint32_t* w = I.words + wstart;
+        uint32_t wv[LSHORT];
+#pragma unroll
+        for (uint32_t j = 0; j < LSHORT; ++j) wv[j] = i0 + j < i1 ? __ldg(w + i0 + j) : 0u;
+        uint32_t p = s0;
+#pragma unroll
+        for (uint32_t j = 0; j < LSHORT; ++j) {
+            if (i0 + j >= i1) break;
+            const uint32_t wd = wv[j];
+            const uint32_t c = wgroups(wd);
+            if (!is_fill(wd)) {
+                if (wd && p >= g0 && p < g1) atomicOr(&S.tmp[rsw(p - g0)], wd);
+            } else if (wd >= HEADER1) {
+                const uint32_t a = max(p, g0), e = min(p + c, g1);
+                if (e > a + LFILL) lng = true;  // the warp paints it (OR is idempotent)
+                else for (uint32_t g = a; g < e; ++g) S.tmp[rsw(g - g0)] = ALLONES;
+            }
+            p += c;
+        }
+        // the active bits form the group after the whole words
+        if (!lng && banb > 0 && gb >= g0 && gb < g1) {
+            const uint32_t pat = (aval & ((1u << banb) - 1u)) << (31u - banb);
+            if (pat) atomicOr(&S.tmp[rsw(gb - g0)], pat);
+        }
+    }
+    uint32_t lm = __ballot_sync(0xffffffffu, lng);
+    while (lm) {
+        const uint32_t src = __ffs(lm) - 1u;
+        lm &= lm - 1u;
+        warp_or_bitmap(S, I, __shfl_sync(0xffffffffu, b, src), k, g0, g1, G, anb, nullptr);
+    }
+}
+
 // Lower bound of v in the ascending list a[0, n) by a group of 16 lanes
 // (lanes [gbase, gbase+16) of a full warp; every lane of the warp calls it):
 // each round the 16 lanes probe evenly spaced entries of [lo, hi) and the
@@ -392,15 +452,19 @@ __global__ void __launch_bounds__(RTHREADS, 6) k_range(RangeArgs A) {
                 sb = S.hdr[4]; nb = S.hdr[5] - sb;
             }
             const uint32_t nsel = na + nb;
-            for (uint32_t j = warp; j < nc + nsel; j += RWARPS) {
-                if (j < nc) {
-                    warp_or_bitmap(S, I, T.cand[j], k, g0, g1, G, anb, &T);
-                    continue;
+            // row checks one per warp; the bitmaps to OR in batches of up to
+            // 32 per warp (one per lane), spread over the warps
+            for (uint32_t c = warp; c < nc; c += RWARPS) warp_or_bitmap(S, I, T.cand[c], k, g0, g1, G, anb, &T);
+            const uint32_t per = min(32u, (nsel + RWARPS - 1) / RWARPS);
+            for (uint32_t j0 = warp * per; j0 < nsel; j0 += RWARPS * per) {
+                const uint32_t jj = j0 + lane;
+                const bool have = lane < per && jj < nsel;
+                uint32_t b = 0;
+                if (have) {
+                    const uint32_t e = jj < na ? sa + jj : sb + (jj - na);
+                    b = direct ? e : __ldg(I.tl_bm + e);
                 }
-                const uint32_t jj = j - nc;
-                const uint32_t e = jj < na ? sa + jj : sb + (jj - na);
-                const uint32_t b = direct ? e : __ldg(I.tl_bm + e);
-                warp_or_bitmap(S, I, b, k, g0, g1, G, anb, nullptr);
+                lanes_or_bitmaps(S, I, have, b, k, g0, g1, G, anb);
             }
             if (flip) {
                 __syncthreads();

@@ -235,6 +235,8 @@ def main():
     ap.add_argument("--only-range", default=None,
                     help="ROWS:QUERIES — only the binned range case at that size, tile-major count batch run "
                          "warmup+steps times (for ncu)")
+    ap.add_argument("--merge-tile", type=int, default=0, choices=[0, 16, 32, 64],
+                    help="block-index entries per tile of the word-space merge (0: by operand size)")
     ap.add_argument("--workloads", default=None,
                     help="comma list of range workloads to add to the line: relic,range,batched,served "
                          "(default: all four on one GPU, none under torchrun; 'none' for none)")
@@ -273,6 +275,7 @@ def main():
     ctx = L.Context(local)
     ctx.set_tuning(L.TUNE_DENSE_TILE, args.dense_tile)
     ctx.set_tuning(L.TUNE_DENSE_ENGINE, args.dense_engine)
+    ctx.set_tuning(L.TUNE_MERGE_TILE, args.merge_tile)
     # a dedicated stream: the legacy default stream (handle 0) cannot be
     # handed to the library, which treats NULL as "its own stream"
     stream = torch.cuda.Stream()
@@ -411,9 +414,9 @@ def main():
         tb = torch.from_numpy(b).pin_memory()
         pinned.append((ta.numpy(), tb.numpy(), ta, tb))
     ectx = [ctx] + [L.Context(local) for _ in range(args.e2e_threads - 1)]
-    for c in ectx[1:]:
-        c.set_tuning(L.TUNE_DENSE_TILE, args.dense_tile)
-        c.set_tuning(L.TUNE_DENSE_ENGINE, args.dense_engine)
+    for c in ectx[1:]:  # the launch shapes the device-side leg ran with (tuned or given)
+        for key in (L.TUNE_DENSE_TILE, L.TUNE_DENSE_ENGINE, L.TUNE_MERGE_TILE):
+            c.set_tuning(key, ctx.get_tuning(key))
     outbufs = [[torch.empty(len(a) + len(b) + 4, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
                 for a, b in pairs] for _ in ectx]
     calls = [(op, i) for op in OPS for i in range(len(pinned))]

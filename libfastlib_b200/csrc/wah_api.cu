@@ -63,7 +63,12 @@ void* wg_alloc(wahgpu_ctx* ctx, size_t bytes) {
         // release cached blocks and retry once
         cudaStreamSynchronize(ctx->stream);
         std::lock_guard<std::mutex> g(ctx->mu);
-        for (auto& kv : ctx->pool) for (void* q : kv.second) cudaFree(q);
+        for (auto& kv : ctx->pool)
+            for (void* q : kv.second) {
+                cudaFree(q);
+                ctx->sizes.erase(q);
+                ctx->bytes_allocated -= kv.first;
+            }
         ctx->pool.clear();
         cudaGetLastError();
         if (cudaMalloc(&p, c) != cudaSuccess) { cudaGetLastError(); return nullptr; }
@@ -79,6 +84,34 @@ void wg_free(wahgpu_ctx* ctx, void* p) {
     auto it = ctx->sizes.find(p);
     if (it == ctx->sizes.end()) return;
     ctx->pool[it->second].push_back(p);
+}
+
+// Pinned host blocks, pooled by size class like the device blocks: staging
+// for copies that must not wait for the host (a block goes back to the pool
+// only once the copies reading it are known to be done).
+void* wg_host_alloc(wahgpu_ctx* ctx, size_t bytes) {
+    const size_t c = size_class(bytes);
+    {
+        std::lock_guard<std::mutex> g(ctx->mu);
+        auto it = ctx->hpool.find(c);
+        if (it != ctx->hpool.end() && !it->second.empty()) {
+            void* p = it->second.back();
+            it->second.pop_back();
+            return p;
+        }
+    }
+    void* p = nullptr;
+    if (cudaMallocHost(&p, c) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+    std::lock_guard<std::mutex> g(ctx->mu);
+    ctx->hsizes[p] = c;
+    return p;
+}
+void wg_host_free(wahgpu_ctx* ctx, void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    auto it = ctx->hsizes.find(p);
+    if (it == ctx->hsizes.end()) return;
+    ctx->hpool[it->second].push_back(p);
 }
 
 // Scratch for the look-back scans: tile records plus the launch sync words.
@@ -152,6 +185,7 @@ extern "C" int wahgpu_ctx_destroy(wahgpu_ctx* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     for (auto& kv : ctx->sizes) cudaFree(kv.first);
+    for (auto& kv : ctx->hsizes) cudaFreeHost(kv.first);
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->h_meta_stage) cudaFreeHost(ctx->h_meta_stage);
     cudaStreamDestroy(ctx->own_stream);

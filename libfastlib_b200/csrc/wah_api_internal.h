@@ -19,6 +19,8 @@ struct wahgpu_ctx {
     // caching device allocator: size class -> free blocks; block -> class
     std::map<size_t, std::vector<void*>> pool;
     std::map<void*, size_t> sizes;
+    std::map<size_t, std::vector<void*>> hpool;  // pinned host blocks by size class
+    std::map<void*, size_t> hsizes;
     size_t bytes_allocated = 0;
     // look-back scratch: two LaunchSync words then TileRec records
     void* scratch = nullptr;
@@ -72,6 +74,8 @@ int wg_kernel_setup(PerDeviceSetup& s, int device, Kernel k, int threads, size_t
 int wg_fail(wahgpu_ctx* ctx, int code, const char* fmt, ...);
 void* wg_alloc(wahgpu_ctx* ctx, size_t bytes);
 void wg_free(wahgpu_ctx* ctx, void* p);
+void* wg_host_alloc(wahgpu_ctx* ctx, size_t bytes);
+void wg_host_free(wahgpu_ctx* ctx, void* p);
 int wg_scratch(wahgpu_ctx* ctx, uint32_t ntiles, wah::TileRec** recs, wah::LaunchSync** sync);
 int wg_bv_meta(wahgpu_bv* b);
 wahgpu_bv* wg_bv_new(wahgpu_ctx* ctx);

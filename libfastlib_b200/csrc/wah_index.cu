@@ -484,10 +484,20 @@ static int batch_create(wahgpu_ctx* ctx, const wahgpu_term* terms, const uint32_
         wahgpu_batch_free(B);
         return wg_fail(ctx, WAHGPU_ENOMEM, "batch allocation failed");
     }
-    CUDA_TRY(ctx, cudaMemcpyAsync(B->d_idx, di.data(), di.size() * sizeof(DevIndex), cudaMemcpyHostToDevice, ctx->stream));
-    CUDA_TRY(ctx, cudaMemcpyAsync(B->d_terms, dt.data(), nt * sizeof(DevTerm), cudaMemcpyHostToDevice, ctx->stream));
-    CUDA_TRY(ctx, cudaMemcpyAsync(B->d_queries, dq.data(), nq * sizeof(DevQuery), cudaMemcpyHostToDevice, ctx->stream));
-    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));  // host staging above is pageable
+    // the tables leave from pinned staging the batch keeps until it is
+    // freed, so the host does not wait for the copies
+    const size_t bi = di.size() * sizeof(DevIndex), bt = (size_t)nt * sizeof(DevTerm), bq = (size_t)nq * sizeof(DevQuery);
+    B->h_stage = static_cast<unsigned char*>(wg_host_alloc(ctx, bi + bt + bq));
+    if (!B->h_stage) {
+        wahgpu_batch_free(B);
+        return wg_fail(ctx, WAHGPU_ENOMEM, "batch staging allocation failed");
+    }
+    memcpy(B->h_stage, di.data(), bi);
+    memcpy(B->h_stage + bi, dt.data(), bt);
+    memcpy(B->h_stage + bi + bt, dq.data(), bq);
+    CUDA_TRY(ctx, cudaMemcpyAsync(B->d_idx, B->h_stage, bi, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(B->d_terms, B->h_stage + bi, bt, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(B->d_queries, B->h_stage + bi + bt, bq, cudaMemcpyHostToDevice, ctx->stream));
     *out = B;
     return WAHGPU_OK;
 }
@@ -592,6 +602,26 @@ extern "C" int64_t wahgpu_batch_rids(wahgpu_batch* B, uint32_t q, uint32_t* out,
 
 extern "C" const uint32_t* wahgpu_batch_device_rids(wahgpu_batch* B) { return B ? B->d_rids : nullptr; }
 
+// Every query's count and the whole row-id buffer (rid_cap words) in one
+// round trip, for a caller that answers all the queries of a capped batch
+// at once: query q's ids are rids[h_base[q], h_base[q] + min(count, limit)).
+int wg_batch_fetch_all(wahgpu_batch* B, uint32_t* rids) {
+    wahgpu_ctx* ctx = B->ctx;
+    if (B->h_valid) return WAHGPU_OK;
+    B->h_counts.resize(B->nq);
+    B->h_start.resize(B->nq);
+    DevMeta st{};
+    CUDA_TRY(ctx, cudaMemcpyAsync(B->h_counts.data(), B->d_counts, B->nq * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(B->h_start.data(), B->d_start, B->nq * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(&st, B->d_status, sizeof(DevMeta), cudaMemcpyDeviceToHost, ctx->stream));
+    if (rids && B->d_rids && B->rid_cap)
+        CUDA_TRY(ctx, cudaMemcpyAsync(rids, B->d_rids, B->rid_cap * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (st.status == DEV_ERR_TIMEOUT) return wg_fail(ctx, WAHGPU_ETIMEOUT, "a device-side look-back wait gave up");
+    B->h_valid = true;
+    return WAHGPU_OK;
+}
+
 // Algorithmic bytes of one run: per term the words of the bitmaps it ORs
 // (or of their complement), of its edge bitmaps and the raw values of the
 // edge bitmaps' rows; 8 per query for its count.
@@ -610,6 +640,7 @@ extern "C" int wahgpu_batch_free(wahgpu_batch* B) {
     wg_free(ctx, B->d_counts); wg_free(ctx, B->d_start); wg_free(ctx, B->d_status);
     wg_free(ctx, B->d_rids); wg_free(ctx, B->d_dense);
     wg_free(ctx, B->d_items); wg_free(ctx, B->d_scan_tmp);
+    wg_host_free(ctx, B->h_stage);
     delete B;
     return WAHGPU_OK;
 }

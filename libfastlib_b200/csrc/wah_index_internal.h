@@ -55,7 +55,9 @@ struct wahgpu_batch {
     bool capped = false;              // row ids limited per query, each query in a region of its own
     std::vector<uint64_t> h_lim, h_base;
     bool h_valid = false;
+    unsigned char* h_stage = nullptr;  // pinned staging of the uploaded tables
 };
 
 int wg_index_attach(wahgpu_index* x);
+int wg_batch_fetch_all(wahgpu_batch* B, uint32_t* rids);
 #endif

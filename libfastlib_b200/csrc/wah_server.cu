@@ -80,24 +80,27 @@ size_t request_scratch(const wahgpu_term* terms, uint64_t rid_cap) {
 }
 
 void finish_slot(wahgpu_server* S, Slot& sl) {
-    std::vector<uint64_t> counts(sl.reqs.size());
-    int rc = wahgpu_batch_counts(sl.batch, counts.data());
+    wahgpu_batch* B = sl.batch;
+    // counts and every request's row-id region in one round trip, through
+    // pinned staging of the slot's context
+    uint32_t* ids = B->rid_cap ? static_cast<uint32_t*>(wg_host_alloc(sl.ctx, B->rid_cap * 4)) : nullptr;
+    int rc = (B->rid_cap && !ids) ? WAHGPU_ENOMEM : wg_batch_fetch_all(B, ids);
     const auto now = Clock::now();
     for (size_t i = 0; i < sl.reqs.size(); ++i) {
         Request* r = sl.reqs[i];
         r->status = rc;
         if (!rc) {
-            r->count = counts[i];
+            r->count = B->h_counts[i];
             if (r->rid_cap) {
                 // the first rid_cap row ids of the query (its own region)
-                r->rids.resize(std::max<uint64_t>(std::min<uint64_t>(counts[i], r->rid_cap), 1));
-                const int64_t n = wahgpu_batch_rids(sl.batch, (uint32_t)i, r->rids.data(), r->rids.size());
-                if (n < 0) r->status = (int)n; else r->rids.resize((size_t)n);
+                const uint64_t n = std::min<uint64_t>(B->h_counts[i], B->h_lim[i]);
+                r->rids.assign(ids + B->h_base[i], ids + B->h_base[i] + n);
             }
         }
         r->latency = std::chrono::duration<double>(now - r->t_arrive).count();
     }
-    wahgpu_batch_free(sl.batch);
+    wg_host_free(sl.ctx, ids);
+    wahgpu_batch_free(B);
     sl.batch = nullptr;
     std::lock_guard<std::mutex> g(S->mu);
     for (Request* r : sl.reqs) r->done = true;

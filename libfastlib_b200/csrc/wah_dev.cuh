@@ -127,21 +127,21 @@ __device__ __forceinline__ uint32_t wait_record(const TileRec* recs, uint32_t t,
 // Reads the records of up to 32 predecessors of tile t per round trip, stops
 // at the nearest one holding an inclusive prefix, and combines the window in
 // tile order with `comb(earlier, later)`.  Returns the exclusive prefix of
-// tile t in every lane; *ok turns false when a wait gave up.
+// tile t in every lane; *ok turns false in every lane when any wait gave up.
 template <class Comb>
 __device__ __forceinline__ uint4 warp_lookback(const TileRec* recs, uint32_t t, uint32_t epoch,
                                                uint4 identity, Comb comb, bool* ok) {
     const uint32_t lane = threadIdx.x & 31u;
     uint4 acc = identity;  // combination of the tiles already visited (later ones)
     int64_t hi = t;        // tiles [0, hi) not yet visited
-    *ok = true;
+    bool mine_ok = true;
     while (hi > 0) {
         const int64_t p = hi - 1 - lane;
         uint4 v = identity;
         uint32_t st = REC_INCL;  // lanes past tile 0 act as an inclusive identity
         if (p >= 0) {
             st = wait_record(recs, (uint32_t)p, epoch, v);
-            if (st == 0) { *ok = false; st = REC_INCL; v = identity; }
+            if (st == 0) { mine_ok = false; st = REC_INCL; v = identity; }
         }
         const uint32_t incl = __ballot_sync(0xffffffffu, st == REC_INCL);
         const uint32_t L = __ffs(incl) - 1u;  // nearest inclusive record in the window
@@ -166,6 +166,8 @@ __device__ __forceinline__ uint4 warp_lookback(const TileRec* recs, uint32_t t, 
         if (incl) break;
         hi -= 32;
     }
+    // warp-uniform: false in every lane when any lane's wait gave up
+    *ok = __all_sync(0xffffffffu, mine_ok);
     return acc;
 }
 

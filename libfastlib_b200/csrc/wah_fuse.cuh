@@ -134,14 +134,15 @@ constexpr int FLB = 4;  // predecessors per lane per look-back round: 128 tiles 
 // records of the 128 tiles before `hi` (lane l the FLB tiles
 // [hi - FLB(l+1), hi - FLB l), all loads in flight together), wait (bounded)
 // for any not yet published, and stop at the nearest inclusive record.
-// Returns the exclusive prefix of tile t in every lane; *ok turns false
-// when a wait gave up.
+// Returns the exclusive prefix of tile t in every lane; *ok turns false in
+// every lane when a wait of any lane gave up (warp-uniform, so callers may
+// branch on it around warp-wide shuffles).
 __device__ __forceinline__ uint4 fuse_lookback(const uint4* recs, uint32_t t, uint32_t epoch, bool* ok) {
     const uint32_t lane = threadIdx.x & 31u;
     const FuseComb comb;
     uint4 acc = make_uint4(0u, 0u, 0u, 0u);  // tiles already visited (later ones)
     int64_t hi = t;
-    *ok = true;
+    bool mine_ok = true;
     while (hi > 0) {
         uint4 v[FLB];
         uint32_t st[FLB];
@@ -160,7 +161,7 @@ __device__ __forceinline__ uint4 fuse_lookback(const uint4* recs, uint32_t t, ui
             }
             if (all) break;
             if (it >= SPIN_LIMIT) {
-                *ok = false;
+                mine_ok = false;
 #pragma unroll
                 for (int k = 0; k < FLB; ++k)
                     if (!st[k]) { st[k] = REC_INCL; v[k] = make_uint4(0u, 0u, 0u, 0u); }
@@ -208,6 +209,7 @@ __device__ __forceinline__ uint4 fuse_lookback(const uint4* recs, uint32_t t, ui
         if (bal) break;
         hi -= 32 * FLB;
     }
+    *ok = __all_sync(0xffffffffu, mine_ok);
     return acc;
 }
 

@@ -82,7 +82,8 @@ int64_t wahgpu_ctx_launches(wahgpu_ctx* ctx);
                                       5 single-pass group-space kernel over warp tiles */
 #define WAHGPU_TUNE_RANGE_ORDER 2 /* batch work order: 0 query by query; 1 (default) tile by tile for count-only \
                                      batches, else query by query; 2 tile by tile, row ids of several queries \
-                                     placed by a count pass and a scan */
+                                     placed by a count pass and a scan (capped batches: the id pass revisits \
+                                     only the tiles holding ids under each query's limit) */
 #define WAHGPU_TUNE_RANGE_CTAS 3  /* resident CTAs per SM of the persistent range launch: 0 (all that fit) .. 32 */
 #define WAHGPU_TUNE_CUM_STRIDE 5  /* bitmaps per cumulative row of indexes built or attached later: 0 auto, 1 none, >= 2 that stride */
 #define WAHGPU_TUNE_MERGE_TILE 6  /* block-index entries per tile of the word-space merge: 0 auto (by operand size), 16 | 32 | 64 */

@@ -522,7 +522,7 @@ extern "C" int wahgpu_batch_run(wahgpu_batch* B) {
     // order 2 runs two tile-by-tile passes around a scan of the items' hits,
     // order 1 (and a single query) goes query by query with the look-back
     const bool ids = B->d_rids || B->d_dense;
-    const bool two_pass = ctx->range_order == 2 && ids && B->nq > 1 && !B->capped;
+    const bool two_pass = ctx->range_order == 2 && ids && B->nq > 1;
     a.tile_major = ((ctx->range_order != 0 && !ids) || two_pass) ? 1u : 0u;
     a.pass = 0; a.item_cnt = nullptr; a.item_off = nullptr;
     a.capped = B->capped && B->d_rids ? 1u : 0u;

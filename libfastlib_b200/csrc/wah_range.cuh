@@ -109,8 +109,9 @@ struct RangeArgs {
     unsigned long long* item_cnt;
     const unsigned long long* item_off;
     // 1: every query writes at most rid_lim row ids into its own region at
-    // rid_base (query-major order; offsets within the query by a segmented
-    // look-back)
+    // rid_base (query-major order: offsets within the query by a segmented
+    // look-back; two-pass order: by the items' scan, pass 2 skipping the
+    // items whose ids lie past the limit)
     uint32_t capped;
 };
 
@@ -378,12 +379,15 @@ __global__ void __launch_bounds__(RTHREADS, 6) k_range(RangeArgs A) {
         const uint32_t g0 = k * (uint32_t)RT, g1 = min(g0 + (uint32_t)RT, GX);
         const uint32_t ng = g1 > g0 ? g1 - g0 : 0u;
         const uint32_t qi = q * A.ntiles + k;  // the item's place in query-major order
-        if (A.pass == 2u) {
-            // row ids of the two-pass order: items without hits are done
-            if (tid == 0 && k == 0) A.rid_start[q] = A.item_off[qi];
-            if (A.item_cnt[qi] == 0ull) { __syncthreads(); continue; }
-        }
         const DevQuery Q = A.queries[q];
+        if (A.pass == 2u) {
+            // row ids of the two-pass order: items without hits are done, and
+            // so (capped) are items whose ids all lie past the query's limit
+            // (offsets within the query: the scan runs in query-major order)
+            if (tid == 0 && k == 0) A.rid_start[q] = A.capped ? Q.rid_base : A.item_off[qi];
+            const bool past = A.capped && A.item_off[qi] - A.item_off[q * A.ntiles] >= Q.rid_lim;
+            if (A.item_cnt[qi] == 0ull || past) { __syncthreads(); continue; }
+        }
 
         for (uint32_t l = tid; l < RT; l += RTHREADS) S.acc[l] = ALLONES;
         for (uint32_t t = Q.t0; t < Q.t1; ++t) {
@@ -517,7 +521,7 @@ __global__ void __launch_bounds__(RTHREADS, 6) k_range(RangeArgs A) {
         uint64_t total;
         const uint64_t ex = block_exscan64(cnt, S.scan, total);
         if (A.pass == 2u) {
-            if (tid == 0) S.base = A.item_off[qi];
+            if (tid == 0) S.base = A.capped ? A.item_off[qi] - A.item_off[q * A.ntiles] : A.item_off[qi];
         } else if (warp == 0 && A.capped) {
             // the row ids before this tile within its own query
             const uint4 mine = make_uint4((uint32_t)total, (uint32_t)(total >> 32), 0u, k == 0 ? 1u : 0u);

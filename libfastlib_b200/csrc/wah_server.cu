@@ -124,9 +124,10 @@ void launch_slot(wahgpu_server* S, Slot& sl, std::vector<Request*>&& take, size_
         caps.push_back(r->rid_cap);
         rid_cap += r->rid_cap;
     }
-    // count-only batches go tile by tile so their queries share each tile's
-    // bitmap words in L2; batches with row ids go query by query
-    wahgpu_ctx_set_tuning(sl.ctx, WAHGPU_TUNE_RANGE_ORDER, rid_cap ? 0 : 1);
+    // tile by tile, so a batch's queries share each tile's bitmap words in
+    // L2: count-only batches in one pass; batches with row ids count first,
+    // then revisit only the items holding ids under each query's limit
+    wahgpu_ctx_set_tuning(sl.ctx, WAHGPU_TUNE_RANGE_ORDER, rid_cap ? 2 : 1);
     wahgpu_batch* B = nullptr;
     // row ids: each request its own region of rid_cap ids (a LIMIT), so a
     // query with many hits cannot crowd out the others of its batch

@@ -77,9 +77,12 @@ def test_server_refuses_oversized_request(gpu_ctx):
         S.close()
 
 
-def test_capped_batch_row_ids(gpu_ctx):
+@pytest.mark.parametrize("order", [0, 2])
+def test_capped_batch_row_ids(gpu_ctx, order):
     """wahgpu_batch_create_capped: every query keeps its first caps[q] row
-    ids in a region of its own; counts stay complete."""
+    ids in a region of its own; counts stay complete (query by query with
+    the segmented look-back, and tile by tile with a count pass, a scan and
+    an id pass that revisits only the items under each query's limit)."""
     import libfastlib_b200 as L
     from libfastlib_b200 import workloads as W
     n = 1_000_003
@@ -87,12 +90,17 @@ def test_capped_batch_row_ids(gpu_ctx):
     qs = W.conjunctive_queries(9, [m for _, m in cols], 64, max_terms=3)
     queries = [[cols[c][0].term(lo, hi) for c, lo, hi in q] for q in qs]
     caps = [0 if i % 5 == 0 else (1 + 97 * i) for i in range(len(queries))]
-    B = L.Batch(gpu_ctx, queries, caps=caps)
-    B.run()
-    counts = B.counts()
-    for i, q in enumerate(queries):
-        c, rids, _ = L.evaluate(gpu_ctx, q)
-        assert int(counts[i]) == c, i
-        got = B.rids(i, min(c, caps[i]))
-        assert np.array_equal(got, rids[:caps[i]]), i
-    B.close()
+    old = gpu_ctx.get_tuning(L.TUNE_RANGE_ORDER)
+    gpu_ctx.set_tuning(L.TUNE_RANGE_ORDER, order)
+    try:
+        B = L.Batch(gpu_ctx, queries, caps=caps)
+        B.run()
+        counts = B.counts()
+        for i, q in enumerate(queries):
+            c, rids, _ = L.evaluate(gpu_ctx, q)
+            assert int(counts[i]) == c, i
+            got = B.rids(i, min(c, caps[i]))
+            assert np.array_equal(got, rids[:caps[i]]), i
+        B.close()
+    finally:
+        gpu_ctx.set_tuning(L.TUNE_RANGE_ORDER, old)

@@ -41,6 +41,8 @@ constexpr int RWARPS = RTHREADS / 32;
 constexpr int RGPT = RT / RTHREADS;  // groups per thread in the epilogue
 constexpr uint32_t RDIRECT = 32;     // spans of at most this many bitmaps skip the tile lists
 constexpr int RCHK = 2;              // raw values in flight per lane in an edge-bin row check
+// the row-id epilogue stages 16 groups' ids (<= 496) in each warp's RT / RWARPS words of S.tmp
+static_assert(RGPT * RTHREADS == RT && 16 * 31 <= RT / RWARPS, "row-id staging");
 
 // per-bitmap metadata of an attached index
 struct BitmapMeta {
@@ -552,22 +554,44 @@ __global__ void __launch_bounds__(RTHREADS, 6) k_range(RangeArgs A) {
         }
         __syncthreads();
         if (A.rids) {
-            uint64_t off = S.base + ex;
             // capped: offsets are within the query; ids past its limit are
             // dropped and the rest land in its region
             const uint64_t lim = A.capped ? Q.rid_lim : A.rid_cap;
             const uint64_t rbase0 = A.capped ? Q.rid_base : 0ull;
-            for (int j = 0; j < RGPT && off < lim; ++j) {
-                const uint32_t l = l0 + j;
-                if (l >= ng) break;
-                uint32_t bits = S.acc[rsw(l)];
+            // each warp owns RGPT * 32 consecutive groups (its threads' in
+            // the count above) and writes their ids 16 groups at a time:
+            // lanes 0-15 expand a group each into the warp's part of S.tmp
+            // (free once the terms are done), then the warp stores the run
+            // of ids with consecutive lanes on consecutive slots
+            constexpr uint32_t WG = RGPT * 32;      // groups per warp
+            uint32_t* st = S.tmp + warp * WG;       // <= 16 * 31 ids per round
+            uint64_t off = S.base + __shfl_sync(0xffffffffu, ex, 0);
+            for (uint32_t r = 0; r < WG / 16u && off < lim; ++r) {
+                const uint32_t l = warp * WG + r * 16u + (lane & 15u);
+                uint32_t bits = (lane < 16u && l < ng) ? S.acc[rsw(l)] : 0u;
+                const uint32_t c = __popc(bits);
+                uint32_t x = c;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const uint32_t u = __shfl_up_sync(0xffffffffu, x, d);
+                    if (lane >= (uint32_t)d) x += u;
+                }
+                const uint32_t rt = __shfl_sync(0xffffffffu, x, 31);
+                if (rt == 0u) continue;
+                uint32_t p = x - c;
                 const uint32_t rbase = (g0 + l) * 31u;
                 while (bits) {
                     const uint32_t hb = 31u - __clz(bits);
-                    if (off < lim && rbase0 + off < A.rid_cap) A.rids[rbase0 + off] = rbase + (30u - hb);
-                    ++off;
+                    st[p++] = rbase + (30u - hb);
                     bits &= ~(1u << hb);
                 }
+                __syncwarp();
+                for (uint32_t i = lane; i < rt; i += 32u) {
+                    const uint64_t o = off + i;
+                    if (o < lim && rbase0 + o < A.rid_cap) A.rids[rbase0 + o] = st[i];
+                }
+                __syncwarp();
+                off += rt;
             }
         }
         if (A.dense && q == 0) {

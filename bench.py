@@ -232,6 +232,9 @@ def main():
     ap.add_argument("--dense-engine", type=int, default=0, choices=[0, 1, 2, 3, 4, 5],
                     help="canonical-result operators: 0 auto, 1 pipelined group-space kernel, 2 word-space merge, "
                          "3 two-pass group-space kernels, 4 single pass over CTA tiles, 5 single pass over warp tiles")
+    ap.add_argument("--only-batched", default=None,
+                    help="ROWS:QUERIES — only the batched conjunctive case (its 8 columns at that size), tile-major "
+                         "count batch run warmup + steps times (for ncu)")
     ap.add_argument("--only-range", default=None,
                     help="ROWS:QUERIES — only the binned range case at that size, tile-major count batch run "
                          "warmup+steps times (for ncu)")
@@ -256,6 +259,9 @@ def main():
 
     if args.only_range:
         run_only_range(args)
+        return
+    if args.only_batched:
+        run_only_batched(args)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -386,7 +392,7 @@ def main():
     achieved = dense_b / (dense_ms / 1e3) / 1e9 if dense_ms > 0 else None
     traffic = None
     traffic_calls = []
-    engine = dense_tuning["chosen"]["engine"] if dense_tuning else (args.dense_engine or 5)
+    engine = dense_tuning["chosen"]["engine"] if dense_tuning else (args.dense_engine or 3)
     tile = dense_tuning["chosen"]["tile_groups"] if dense_tuning else args.dense_tile
     engine_kernels = {5: "k_gone", 4: f"k_gfuse (tile {tile})", 3: "k_gop + k_gpack", 1: "k_dense",
                       2: "k_merge"}[engine]
@@ -541,6 +547,61 @@ def run_only_range(args):
         B.run()
     ms = _ev_time(stream, B.run, args.steps)
     print(json.dumps({"only_range": args.only_range, "ms_per_batch": ms, "queries_per_s": nq / ms * 1e3,
+                      "algorithmic_bytes": B.nbytes(), "GBps": B.nbytes() / ms / 1e6}))
+    ctx.set_stream(None)
+
+
+def batched_columns(ctx, n, keep_host=False):
+    """The batched workload's 8 indexed columns of n rows: 3 uint32
+    U{0..999} relic, 3 Zipf(1.1) over 1e6 ranks relic, 2 float32 Normal bin
+    512 (indexes built on the GPU); with their query metadata and, when
+    asked, host copies of the columns."""
+    import torch
+    import libfastlib_b200 as L
+    from libfastlib_b200 import workloads as W
+    cols, metas, host_cols = [], [], []
+    for c in range(3):
+        v = W.uniform_int_column(40 + c, n, 1000)
+        cols.append(L.Index.build(ctx, L.RELIC, v))
+        metas.append({"kind": "relic", "card": 1000})
+        if keep_host:
+            host_cols.append(v.cpu().numpy())
+    for c in range(3):
+        v = W.zipf_column(50 + c, n, 1.1, 1_000_000).to(torch.int32)
+        cols.append(L.Index.build(ctx, L.RELIC, v))
+        metas.append({"kind": "relic", "card": 1_000_000})
+        if keep_host:
+            host_cols.append(v.cpu().numpy())
+    for c in range(2):
+        v = W.normal_column(60 + c, n)
+        ix = L.Index.build(ctx, L.BIN, v, nbins=512)
+        cols.append(ix)
+        metas.append({"kind": "bin", "keys": ix.keys(), "nobs": ix.nbitmaps(), "max_span": 256})
+        if keep_host:
+            host_cols.append(v.cpu().numpy())
+    return cols, metas, host_cols
+
+
+def run_only_batched(args):
+    """The batched conjunctive case at a chosen size (the same 8 columns at
+    ROWS rows, QUERIES conjunctions), one count-only tile-major batch run
+    warmup + steps times; prints one JSON line."""
+    import torch
+    import libfastlib_b200 as L
+    from libfastlib_b200 import workloads as W
+    rows, nq = (int(x) for x in args.only_batched.split(":"))
+    ctx = L.Context(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    cols, metas, _ = batched_columns(ctx, rows)
+    qs = W.conjunctive_queries(4, metas, nq, max_terms=4)
+    B = L.Batch(ctx, [[cols[c].term(lo, hi) for c, lo, hi in q] for q in qs], 0)
+    ctx.set_tuning(L.TUNE_RANGE_ORDER, 1)
+    for _ in range(args.warmup):
+        B.run()
+    ms = _ev_time(stream, B.run, args.steps)
+    print(json.dumps({"only_batched": args.only_batched, "ms_per_batch": ms, "queries_per_s": nq / ms * 1e3,
                       "algorithmic_bytes": B.nbytes(), "GBps": B.nbytes() / ms / 1e6}))
     ctx.set_stream(None)
 
@@ -835,25 +896,8 @@ def range_workloads(args, ctx, stream, peak, which):
         del col
     if "batched" in which:
         n = 50_000_000
-        cols, metas, host_cols = [], [], []
         t0 = time.perf_counter()
-        for c in range(3):
-            v = W.uniform_int_column(40 + c, n, 1000)
-            cols.append(L.Index.build(ctx, L.RELIC, v))
-            metas.append({"kind": "relic", "card": 1000})
-            host_cols.append(v.cpu().numpy())
-        for c in range(3):
-            v = W.zipf_column(50 + c, n, 1.1, 1_000_000).to(torch.int32)
-            cols.append(L.Index.build(ctx, L.RELIC, v))
-            metas.append({"kind": "relic", "card": 1_000_000})
-            host_cols.append(v.cpu().numpy())
-        for c in range(2):
-            v = W.normal_column(60 + c, n)
-            ix = L.Index.build(ctx, L.BIN, v, nbins=512)
-            cols.append(ix)
-            metas.append({"kind": "bin", "keys": ix.keys(), "nobs": ix.nbitmaps(), "max_span": 256})
-            host_cols.append(v.cpu().numpy())
-        del v
+        cols, metas, host_cols = batched_columns(ctx, n, keep_host=True)
         build_s = time.perf_counter() - t0
         qs = W.conjunctive_queries(4, metas, 4096, max_terms=4)
         queries = [[cols[c].term(lo, hi) for c, lo, hi in q] for q in qs]

@@ -76,7 +76,7 @@ int64_t wahgpu_ctx_launches(wahgpu_ctx* ctx);
  * results never depend on them).  Values outside the listed set are
  * rejected with WAHGPU_EINVAL. */
 #define WAHGPU_TUNE_DENSE_TILE 1  /* groups per tile of the dense-path kernel: 1024 | 2048 | 4096 */
-#define WAHGPU_TUNE_DENSE_ENGINE 4 /* canonical-result operators: 0 auto (= 5), 1 pipelined group-space kernel, \
+#define WAHGPU_TUNE_DENSE_ENGINE 4 /* canonical-result operators: 0 auto (= 3), 1 pipelined group-space kernel, \
                                       2 word-space merge, 3 two-pass group-space kernels, \
                                       4 single-pass group-space kernel over CTA tiles, \
                                       5 single-pass group-space kernel over warp tiles */

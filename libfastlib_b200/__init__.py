@@ -52,7 +52,7 @@ RELIC, BIN = 1, 2
 TUNE_DENSE_TILE = 1
 TUNE_RANGE_ORDER = 2
 TUNE_RANGE_CTAS = 3
-TUNE_DENSE_ENGINE = 4  # 0 auto (= 5), 1 pipelined group space, 2 word space, 3 two-pass group space, 4 / 5 single pass (CTA / warp tiles)
+TUNE_DENSE_ENGINE = 4  # 0 auto (= 3), 1 pipelined group space, 2 word space, 3 two-pass group space, 4 / 5 single pass (CTA / warp tiles)
 TUNE_CUM_STRIDE = 5
 TUNE_MERGE_TILE = 6   # 0 auto, 16, 32 or 64 block-index entries per tile of the word-space merge
 TEST_WITHHOLD_TILE = 100  # failure-path test hook: a tile that never publishes its look-back record

@@ -823,13 +823,13 @@ static bool dense_in_word_space(const wahgpu_ctx* ctx, const wahgpu_bv*, const w
     return ctx->dense_engine == 2;
 }
 static bool dense_two_pass(const wahgpu_ctx* ctx) {
-    return ctx->dense_engine == 3;
+    return ctx->dense_engine == 0 || ctx->dense_engine == 3;
 }
 static bool dense_fused(const wahgpu_ctx* ctx) {
     return ctx->dense_engine == 4;
 }
 static bool dense_warp_tiles(const wahgpu_ctx* ctx) {
-    return ctx->dense_engine == 0 || ctx->dense_engine == 5;
+    return ctx->dense_engine == 5;
 }
 
 // adjustSize(0, nt) of a copy of b (src/bitvector.cpp:4086-4108): the copy

@@ -99,8 +99,8 @@ def _full_size(gpu_ctx, density):
 
 class _engine:
     """A given engine for canonical-result operators
-    (WAHGPU_TUNE_DENSE_ENGINE: 3 two-pass, 4 single-pass CTA tiles, 5
-    single-pass warp tiles, the default) and tile size
+    (WAHGPU_TUNE_DENSE_ENGINE: 3 two-pass, the default; 4 single-pass CTA
+    tiles; 5 single-pass warp tiles) and tile size
     (WAHGPU_TUNE_DENSE_TILE, used by engine 4)."""
 
     def __init__(self, ctx, engine, tile=2048):

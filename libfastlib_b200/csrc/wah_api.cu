@@ -623,15 +623,16 @@ int wg_launch_gop(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t 
     uint32_t* R = static_cast<uint32_t*>(wg_alloc(ctx, (size_t)ntiles * GT * 4));
     const uint32_t nseg = (ntiles + GSEG - 1) / GSEG;
     uint4* tiles = static_cast<uint4*>(wg_alloc(ctx, ((size_t)ntiles + nseg) * 16));
-    if (!R || !tiles) {
-        wg_free(ctx, R); wg_free(ctx, tiles);
+    uint32_t* hmask = static_cast<uint32_t*>(wg_alloc(ctx, (size_t)ntiles * 32 * 4));
+    if (!R || !tiles || !hmask) {
+        wg_free(ctx, R); wg_free(ctx, tiles); wg_free(ctx, hmask);
         return wg_fail(ctx, WAHGPU_ENOMEM, "allocation of %u tiles of result patterns failed", ntiles);
     }
     GopArgs a;
     a.xw = x->words; a.xgt = x->gt; a.nx = x->h.n;
     a.yw = y->words; a.ygt = y->gt; a.ny = y->h.n;
     a.groups = groups; a.ntiles = ntiles;
-    a.R = R; a.tiles = tiles; a.segs = tiles + ntiles;
+    a.R = R; a.tiles = tiles; a.segs = tiles + ntiles; a.hmask = hmask;
     a.out = res->words; a.obp = res->bpos; a.meta = res->meta;
     a.aval = aval; a.anb = anb;
     cudaStream_t s = ctx->stream;
@@ -662,6 +663,7 @@ int wg_launch_gop(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t 
     // stream runs after the launches above
     wg_free(ctx, R);
     wg_free(ctx, tiles);
+    wg_free(ctx, hmask);
     if (rc) return rc;
     res->h_valid = false;
     res->gt_valid = false;

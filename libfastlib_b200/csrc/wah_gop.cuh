@@ -44,6 +44,7 @@ struct GopArgs {
     uint32_t* R;          // ntiles * GT result patterns
     uint4* tiles;         // per tile: {heads, first head (GNONE: none), popcount, -}
     uint4* segs;          // per GSEG tiles (zeroed before k_gop): {heads, GNONE - first head (0: none), popcount, -}
+    uint32_t* hmask;      // per tile and lane: the lane's run heads (bit 4 j + e: group 128 j + 4 lane + e)
     uint32_t* out; uint32_t* obp; DevMeta* meta;
     uint32_t aval, anb;
 };
@@ -217,7 +218,7 @@ __global__ void __launch_bounds__(GTHREADS) k_gop(GopArgs A) {
     const uint32_t g0 = t * (uint32_t)GT, g1 = min(g0 + (uint32_t)GT, G);
     const uint32_t ng = g1 - g0;
     uint32_t* R = A.R + g0;
-    uint32_t heads = 0, first = GNONE, popc = 0;
+    uint32_t heads = 0, first = GNONE, popc = 0, hm = 0;
     uint32_t before;  // the result of the group before the current chunk
     const bool ok = gop_tile<OP>(A.xw, A.xgt, A.nx, A.yw, A.ygt, A.ny, W, g0, g1, before, [&](int j, uint4 r) {
         reinterpret_cast<uint4*>(R)[32 * j + lane] = r;
@@ -231,12 +232,17 @@ __global__ void __launch_bounds__(GTHREADS) k_gop(GopArgs A) {
             const uint32_t pos = 128u * j + 4u * lane + e;
             const uint32_t c = cls_of(rv[e]);
             if (pos < ng) {
-                if ((g0 + pos == 0u) || c == C_MIXED || c != pc) { ++heads; first = min(first, g0 + pos); }
+                if ((g0 + pos == 0u) || c == C_MIXED || c != pc) {
+                    ++heads;
+                    first = min(first, g0 + pos);
+                    hm |= 1u << (4 * j + e);
+                }
                 popc += __popc(rv[e]);
             }
             pc = c;
         }
     });
+    A.hmask[(size_t)t * 32u + lane] = hm;
     if (!ok && lane == 0) atomicExch(&A.meta->status, DEV_ERR_FORMAT);
     heads = __reduce_add_sync(0xffffffffu, heads);
     popc = __reduce_add_sync(0xffffffffu, popc);
@@ -304,71 +310,52 @@ __global__ void __launch_bounds__(GTHREADS) k_gpack(GopArgs A) {
         if (f) nxt = GNONE - f;
     }
     if (nxt == GNONE) nxt = G;
-    const uint32_t g0 = t * (uint32_t)GT, g1 = min(g0 + (uint32_t)GT, G);
-    const uint32_t ng = g1 - g0;
+    const uint32_t g0 = t * (uint32_t)GT;
     const uint4* R4 = reinterpret_cast<const uint4*>(A.R + g0);
-    uint4 rv[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) rv[j] = R4[32 * j + lane];
-    uint32_t before = g0 > 0 ? A.R[g0 - 1] : 0u;
-    uint32_t hm[8], base[8];
-    uint32_t acc = 0;  // heads before the chunk
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        const uint32_t r[4] = {rv[j].x, rv[j].y, rv[j].z, rv[j].w};
-        uint32_t pb = __shfl_up_sync(0xffffffffu, r[3], 1);
-        if (lane == 0) pb = before;
-        before = __shfl_sync(0xffffffffu, r[3], 31);
-        uint32_t pc = cls_of(pb), m = 0;
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const uint32_t pos = 128u * j + 4u * lane + e;
-            const uint32_t c = cls_of(r[e]);
-            if (pos < ng && ((g0 + pos == 0u) || c == C_MIXED || c != pc)) m |= 1u << e;
-            pc = c;
-        }
-        hm[j] = m;
-        base[j] = acc;
-        acc += __reduce_add_sync(0xffffffffu, __popc(m));
-    }
+    // the lane's heads as k_gop found them: bit 4 j + e for group 128 j + 4 lane + e
+    const uint32_t hm = A.hmask[(size_t)t * 32u + lane];
+    const uint32_t gt = (2u << lane) - 1u;  // lanes up to this one (lane 31: all)
     uint32_t later = nxt;  // the first head after the chunk
+    uint32_t rest = cnt;   // heads in the chunks before and at the current one
     bool fill = false;
 #pragma unroll
     for (int j = 7; j >= 0; --j) {
-        const uint32_t m = hm[j];
+        const uint32_t m = (hm >> (4 * j)) & 15u;
+        const uint32_t hl = __ballot_sync(0xffffffffu, m != 0u);
+        if (hl == 0u) continue;  // a chunk inside a run
+        // heads of the lanes before this one, from the bits of each lane's
+        // count (0..4); the chunk's own count
+        const uint32_t nh = __popc(m);
+        const uint32_t c0 = __ballot_sync(0xffffffffu, nh & 1u);
+        const uint32_t c1 = __ballot_sync(0xffffffffu, nh & 2u);
+        const uint32_t c2 = __ballot_sync(0xffffffffu, nh & 4u);
+        rest -= __popc(c0) + 2u * __popc(c1) + 4u * __popc(c2);
+        const uint32_t lt = gt >> 1;  // lanes before this one
+        uint32_t o = off + rest + __popc(c0 & lt) + 2u * __popc(c1 & lt) + 4u * __popc(c2 & lt);
+        // the head after this lane's last one: the first head of the
+        // nearest higher lane holding one, else the first after the chunk
         const uint32_t g = g0 + 128u * j + 4u * lane;
         const uint32_t mine = m ? g + (__ffs(m) - 1u) : GNONE;
-        uint32_t y = mine;  // first head in this lane or the lanes after it
+        const uint32_t above = hl & ~gt;
+        const uint32_t nl = __shfl_sync(0xffffffffu, mine, above ? __ffs(above) - 1u : lane);
+        const uint32_t after = above ? nl : later;
+        later = __shfl_sync(0xffffffffu, mine, __ffs(hl) - 1u);
+        if (m) {
+            const uint4 rq = R4[32 * j + lane];
+            const uint32_t r[4] = {rq.x, rq.y, rq.z, rq.w};
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t u = __shfl_down_sync(0xffffffffu, y, d);
-            if (lane + (uint32_t)d < 32u) y = min(y, u);
+            for (int e = 0; e < 4; ++e)
+                if ((m >> e) & 1u) {
+                    const uint32_t more = m >> (e + 1);
+                    const uint32_t next = more ? g + e + __ffs(more) : after;
+                    const uint32_t wd = run_word(cls_of(r[e]), next - (g + e), r[e], false);
+                    A.out[o] = wd;
+                    if ((o & 31u) == 0u) A.obp[o >> 5] = g + e;
+                    if (o == 0u) A.meta->w0 = wd;
+                    fill |= is_fill(wd);
+                    ++o;
+                }
         }
-        uint32_t after = __shfl_down_sync(0xffffffffu, y, 1);
-        if (lane == 31) after = GNONE;
-        after = min(after, later);
-        const uint32_t h = __popc(m);
-        uint32_t x = h;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t u = __shfl_up_sync(0xffffffffu, x, d);
-            if (lane >= (uint32_t)d) x += u;
-        }
-        uint32_t o = off + base[j] + x - h;
-        const uint32_t r[4] = {rv[j].x, rv[j].y, rv[j].z, rv[j].w};
-#pragma unroll
-        for (int e = 0; e < 4; ++e)
-            if ((m >> e) & 1u) {
-                const uint32_t rest = m >> (e + 1);
-                const uint32_t next = rest ? g + e + __ffs(rest) : after;
-                const uint32_t wd = run_word(cls_of(r[e]), next - (g + e), r[e], false);
-                A.out[o] = wd;
-                if ((o & 31u) == 0u) A.obp[o >> 5] = g + e;
-                if (o == 0u) A.meta->w0 = wd;
-                fill |= is_fill(wd);
-                ++o;
-            }
-        later = min(later, __shfl_sync(0xffffffffu, y, 0));
     }
     if (__any_sync(0xffffffffu, fill) && lane == 0) atomicOr(&A.meta->nfill, 1u);
 }

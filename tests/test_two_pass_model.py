@@ -76,6 +76,49 @@ def cls(v):
     return np.where(v == 0, 0, np.where(v == ALL, 1, 2))
 
 
+def gpack_lanes(head, g0, cnt, nxt):
+    """k_gpack's lane arithmetic for one tile: head[i] is True for the run
+    heads among the tile's 1024 groups (lane l of chunk j holds groups
+    128 j + 4 l .. + 3).  Chunks are taken last to first; a lane's first
+    output index is the heads of the chunks before (the tile's count minus
+    the chunks already taken) plus those of the lanes before it (from the
+    bits of each lane's 0..4 count), and the head after its last one is the
+    first head of the nearest higher lane holding one, else the first head
+    after the chunk.  Returns {group: (output index within the tile, next
+    head)}."""
+    hm = [0] * 32
+    for i in range(GT):
+        if head[i]:
+            j, rem = divmod(i, 128)
+            hm[rem // 4] |= 1 << (4 * j + rem % 4)
+    out = {}
+    later, rest = nxt, cnt
+    for j in range(7, -1, -1):
+        m = [(hm[l] >> (4 * j)) & 15 for l in range(32)]
+        hl = sum(1 << l for l in range(32) if m[l])
+        if hl == 0:
+            continue
+        nh = [bin(x).count("1") for x in m]
+        ballots = [sum(1 << l for l in range(32) if nh[l] & bit) for bit in (1, 2, 4)]
+        rest -= sum(bin(b).count("1") << k for k, b in enumerate(ballots))
+        assert rest >= 0
+        mine = [g0 + 128 * j + 4 * l + ((m[l] & -m[l]).bit_length() - 1) if m[l] else NONE for l in range(32)]
+        for l in range(32):
+            lt = (1 << l) - 1
+            o = rest + sum(bin(b & lt).count("1") << k for k, b in enumerate(ballots))
+            above = hl & ~((2 << l) - 1) & 0xFFFFFFFF
+            after = mine[(above & -above).bit_length() - 1] if above else later
+            for e in range(4):
+                if (m[l] >> e) & 1:
+                    more = m[l] >> (e + 1)
+                    g = g0 + 128 * j + 4 * l + e
+                    nx = g + ((more & -more).bit_length()) if more else after
+                    out[g] = (o, nx)
+                    o += 1
+        later = mine[(hl & -hl).bit_length() - 1]
+    return out
+
+
 def two_pass(op, wa, wb, groups):
     """Words and bpos of the engine's result (whole words only)."""
     wa, wb = np.asarray(wa, np.int64), np.asarray(wb, np.int64)
@@ -135,8 +178,11 @@ def two_pass(op, wa, wb, groups):
         if g0 == 0:
             head[0] = True
         pos = np.nonzero(head)[0]
+        lanes = gpack_lanes(np.concatenate([head, np.zeros(GT - len(head), bool)]), g0, cnt, nxt)
+        assert sorted(lanes) == [g0 + int(p) for p in pos]
         for k, p in enumerate(pos):
             nx = g0 + pos[k + 1] if k + 1 < len(pos) else nxt
+            assert lanes[g0 + int(p)] == (k, nx), (t, p)
             length = nx - (g0 + p)
             if c[p] == 2:
                 wd = r[p]

@@ -615,6 +615,10 @@ int wg_launch_gop(wahgpu_ctx* ctx, int op, wahgpu_bv* x, wahgpu_bv* y, uint32_t 
                   uint32_t anb, uint32_t aval, wahgpu_bv* res) {
     int rc = bv_reserve(res, (uint64_t)x->h.n + y->h.n);
     if (rc) return rc;
+    // the staging copies 16-byte chunks of the operands' word arrays (pool
+    // blocks, 256-byte aligned)
+    if ((reinterpret_cast<uintptr_t>(x->words) | reinterpret_cast<uintptr_t>(y->words)) & 15u)
+        return wg_fail(ctx, WAHGPU_EINVAL, "operand word arrays must be 16-byte aligned");
     rc = wg_gtile(x);
     if (rc) return rc;
     rc = wg_gtile(y);

@@ -35,7 +35,9 @@ constexpr int GTHREADS = GWARPS * 32;
 constexpr int GWPL = 33;                  // staged words per lane when counting (odd: conflict-free)
 constexpr uint32_t GNONE = 0xFFFFFFFFu;   // no head in the tile
 constexpr uint32_t GSEG = 256;            // tiles per segment of the two-level prefix
-static_assert(GT == 8 * 128 && GWPL * 32 >= GT, "tile shape");
+// staging holds a tile's <= GT words plus up to 3 before them and the
+// rest of the last 16-byte chunk
+static_assert(GT == 8 * 128 && GWPL * 32 >= GT + 4 && (GWPL * 32 * 4) % 16 == 0, "tile shape");
 
 struct GopArgs {
     const uint32_t* xw; const uint32_t* xgt; uint32_t nx;
@@ -58,7 +60,26 @@ struct GopWarp {
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Stages words [wi0, wi0 + nw) of an n-word array w (16-byte aligned) into
+// ws with both sides indexed from the 16-byte boundary a0 = wi0 & ~3:
+// ws[i] = w[a0 + i], so word wi0 + k lands at ws[k + (wi0 & 3)].  Whole
+// 16-byte chunks inside the array go as 16-byte copies (shared and global
+// addresses both 16-byte aligned: ws is, and a0 is a multiple of 4 words),
+// the at most 3 words of a chunk cut by the array's end as 4-byte ones.
+__device__ __forceinline__ void gop_stage(uint32_t* ws, const uint32_t* __restrict__ w, uint32_t wi0, uint32_t nw,
+                                          uint32_t n) {
+    const uint32_t lane = threadIdx.x & 31u;
+    if (nw == 0) return;
+    const uint32_t a0 = wi0 & ~3u, end = wi0 + nw;
+    const uint32_t nfull = min((end - a0 + 3u) / 4u, (n - a0) / 4u);
+    for (uint32_t c = lane; c < nfull; c += 32) cp_async16(ws + 4u * c, w + a0 + 4u * c);
+    for (uint32_t i = a0 + 4u * nfull + lane; i < end; i += 32) cp_async4(ws + (i - a0), w + i);
+}
 
 // Word range of one operand over the tile [g0, g1): words [wi0, wend), the
 // first starting at group s0.  gt: the operand's group-tile index (entry
@@ -128,6 +149,13 @@ __device__ __forceinline__ uint4 gop_chunk(const uint32_t* ws, const uint16_t* m
                       wpattern(ws[i2 ? i2 - 1u : 0u]), wpattern(ws[i3 ? i3 - 1u : 0u]));
 }
 
+// Staged words 4 q .. 4 q + 3: one 16-byte read when the base is 16-byte
+// aligned (al, warp-uniform), else four.
+__device__ __forceinline__ uint4 gop_ld4(const uint32_t* ws, uint32_t q, bool al) {
+    if (al) return reinterpret_cast<const uint4*>(ws)[q];
+    return make_uint4(ws[4u * q], ws[4u * q + 1u], ws[4u * q + 2u], ws[4u * q + 3u]);
+}
+
 // Result patterns of one warp's tile [g0, g1) of x OP y: both operands'
 // words over the tile are staged in shared memory at once with cp.async and
 // expanded to one 31-bit pattern per group (a word-start marker per word
@@ -148,9 +176,11 @@ __device__ __forceinline__ bool gop_tile(const uint32_t* __restrict__ xw, const 
     const uint32_t ng = g1 - g0;
     uint32_t xi0, xs0, xn, yi0, ys0, yn;
     const bool ok = gop_range(xgt, nx, g0, g1, xi0, xs0, xn) & gop_range(ygt, ny, g0, g1, yi0, ys0, yn);
-    // both operands' words in flight at once
-    for (uint32_t i = lane; i < xn; i += 32) cp_async4(&W.ws[0][i], xw + xi0 + i);
-    for (uint32_t i = lane; i < yn; i += 32) cp_async4(&W.ws[1][i], yw + yi0 + i);
+    // both operands' words in flight at once; word k of the tile at wsx[k]
+    gop_stage(W.ws[0], xw, xi0, xn, nx);
+    gop_stage(W.ws[1], yw, yi0, yn, ny);
+    const uint32_t* wsx = W.ws[0] + (xi0 & 3u);
+    const uint32_t* wsy = W.ws[1] + (yi0 & 3u);
     const bool xpure = xs0 == g0 && xn == ng, ypure = ys0 == g0 && yn == ng;
     // the result before the tile (the words covering g0 - 1)
     prev = 0;
@@ -172,11 +202,11 @@ __device__ __forceinline__ bool gop_tile(const uint32_t* __restrict__ xw, const 
 #pragma unroll
         for (int j = 1; j < 8; ++j) reinterpret_cast<uint2*>(W.mk)[32 * j + lane] = make_uint2(0u, 0u);
         __syncwarp();
-        gop_mark(W.ws[0], W.mk, xn, xs0, g0, g1);
+        gop_mark(wsx, W.mk, xn, xs0, g0, g1);
         __syncwarp();
         if (both) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) xb[j] = gop_chunk(W.ws[0], W.mk, j, xc);
+            for (int j = 0; j < 8; ++j) xb[j] = gop_chunk(wsx, W.mk, j, xc);
             __syncwarp();
 #pragma unroll
             for (int j = 0; j < 8; ++j) reinterpret_cast<uint2*>(W.mk)[32 * j + lane] = make_uint2(0u, 0u);
@@ -190,18 +220,18 @@ __device__ __forceinline__ bool gop_tile(const uint32_t* __restrict__ xw, const 
             __syncwarp();
         }
         if (xpure || both) {
-            gop_mark(W.ws[1], W.mk, yn, ys0, g0, g1);
+            gop_mark(wsy, W.mk, yn, ys0, g0, g1);
             __syncwarp();
         }
     }
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         uint4 a, b;
-        if (xpure) a = pattern4(reinterpret_cast<const uint4*>(W.ws[0])[32 * j + lane]);
+        if (xpure) a = pattern4(gop_ld4(wsx, 32 * j + lane, (xi0 & 3u) == 0u));
         else if (both) a = xb[j];
-        else a = gop_chunk(W.ws[0], W.mk, j, xc);
-        if (ypure) b = pattern4(reinterpret_cast<const uint4*>(W.ws[1])[32 * j + lane]);
-        else b = gop_chunk(W.ws[1], W.mk, j, yc);
+        else a = gop_chunk(wsx, W.mk, j, xc);
+        if (ypure) b = pattern4(gop_ld4(wsy, 32 * j + lane, (yi0 & 3u) == 0u));
+        else b = gop_chunk(wsy, W.mk, j, yc);
         f(j, make_uint4(op2<OP>(a.x, b.x), op2<OP>(a.y, b.y), op2<OP>(a.z, b.z), op2<OP>(a.w, b.w)));
     }
     return ok;

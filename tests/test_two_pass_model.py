@@ -257,3 +257,37 @@ def test_segments_span_many_tiles():
         body = ref[:-1] if ref[-1] == 0 else ref[:-2]
         words, _, _ = two_pass(op, wa, wb, ng)
         assert np.array_equal(words, body.astype(np.int64)), op
+
+
+def stage_copies(wi0, nw, n):
+    """gop_stage's copies for words [wi0, wi0 + nw) of an n-word array:
+    (shared index, global word, words) per copy."""
+    a0, end = wi0 & ~3, wi0 + nw
+    nfull = min((end - a0 + 3) // 4, (n - a0) // 4)
+    copies = [(4 * c, a0 + 4 * c, 4) for c in range(nfull)]
+    copies += [(i - a0, i, 1) for i in range(a0 + 4 * nfull, end)]
+    return a0, copies
+
+
+def test_stage_arithmetic():
+    """16-byte copies start on 16-byte boundaries on both sides, no copy
+    reads past the array, every word of the tile lands at ws[k + (wi0 & 3)]
+    and the staging buffer (33 * 32 words) is never overrun."""
+    rng = np.random.default_rng(3)
+    cases = [(w, nw, n) for n in (1, 2, 3, 4, 5, 7, 8, 1024, 1025, 1027, 5000)
+             for w in range(0, min(n, 9)) for nw in (1, 2, 3, 4, 5, n - w) if 0 < nw <= min(GT, n - w)]
+    for _ in range(3000):
+        n = int(rng.integers(1, 40000))
+        w = int(rng.integers(0, n))
+        cases.append((w, int(rng.integers(1, min(GT, n - w) + 1)), n))
+    for wi0, nw, n in cases:
+        a0, copies = stage_copies(wi0, nw, n)
+        ws = {}
+        for si, gi, k in copies:
+            if k == 4:
+                assert si % 4 == 0 and gi % 4 == 0
+            assert gi + k <= n and si + k <= 33 * 32, (wi0, nw, n)
+            for e in range(k):
+                ws[si + e] = gi + e
+        for kk in range(nw):
+            assert ws[kk + (wi0 & 3)] == wi0 + kk, (wi0, nw, n, kk)

@@ -37,6 +37,7 @@
 namespace wah {
 
 constexpr int GROWS = 8;          // 32-word rows of each operand in flight per lane
+constexpr uint32_t GSHORT = 8;    // fills up to this many groups of the tile are painted by their own lane
 
 // per warp: both operands' patterns over its tile (group g0 + i at index i)
 struct GoneWarp {

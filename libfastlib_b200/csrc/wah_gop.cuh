@@ -9,10 +9,10 @@
 //  * k_gop<OP>: one warp per tile of GT = 1024 groups (the stride of the
 //    operands' group-tile index, which gives each tile's word range).  Both
 //    operands' words over the tile are staged in shared memory at once with
-//    cp.async and expanded to one 31-bit pattern per group (each word writes
-//    its index into the groups it covers, found by a warp scan of the
-//    lengths, and each group reads its word back; an operand with one word
-//    per group is read directly); the result patterns R = a OP b are stored
+//    cp.async and expanded to one 31-bit pattern per group (a word-start
+//    marker per word and a warp max-scan find the word of every group, so a
+//    fill costs one marker whatever its length; an operand with one word per
+//    group is read directly); the result patterns R = a OP b are stored
 //    densely (4 bytes per group) and the tile's run heads (a mixed group, or
 //    a class change) are counted, with the first head's position and the
 //    popcount.  Warps never wait for one another.
@@ -51,7 +51,7 @@ struct GopArgs {
     uint32_t aval, anb;
 };
 
-// per warp: both operands' words over its tile and each group's word index
+// per warp: both operands' words over its tile and the word-start markers
 struct GopWarp {
     uint32_t ws[2][GWPL * 32];
     uint16_t mk[GT];
@@ -98,11 +98,9 @@ __device__ __forceinline__ bool gop_range(const uint32_t* __restrict__ gt, uint3
     return ok;
 }
 
-// Places one operand's staged words: every group of the tile [g0, g1) gets
-// the index + 1 of the word covering it.  The words are taken 32 at a time,
-// one per lane (a row of literals needs no scan); a literal or a fill of up
-// to GSHORT groups is placed by its own lane, a longer fill by the whole warp.
-constexpr uint32_t GSHORT = 8;
+// Places one operand's staged words: marks, at the first group of the tile
+// each word covers, the word's index + 1.  mk must be zero.  The words are
+// taken 32 at a time, one per lane; a row of literals needs no scan.
 __device__ __forceinline__ void gop_mark(const uint32_t* ws, uint16_t* mk, uint32_t nw, uint32_t s0, uint32_t g0,
                                          uint32_t g1) {
     const uint32_t lane = threadIdx.x & 31u;
@@ -126,37 +124,27 @@ __device__ __forceinline__ void gop_mark(const uint32_t* ws, uint16_t* mk, uint3
             p = carry + x - c;
             carry += __shfl_sync(0xffffffffu, x, 31);
         }
-        const uint32_t a = max(p, g0), e = min(p + c, g1);
-        const uint32_t L = (in && e > a) ? e - a : 0u;
-        const uint16_t v = (uint16_t)(k + 1u);
-        if (L == 1u) {
-            mk[a - g0] = v;
-        } else if (L <= GSHORT) {
-#pragma unroll 1
-            for (uint32_t q = a; q < a + L; ++q) mk[q - g0] = v;
-        }
-        uint32_t lm = __ballot_sync(0xffffffffu, L > GSHORT);
-        while (lm) {
-            const uint32_t src = __ffs(lm) - 1u;
-            lm &= lm - 1u;
-            const uint32_t a0 = __shfl_sync(0xffffffffu, a, src) - g0;
-            const uint32_t L0 = __shfl_sync(0xffffffffu, L, src);
-            const uint16_t v0 = (uint16_t)__shfl_sync(0xffffffffu, (uint32_t)v, src);
-            for (uint32_t q = lane; q < L0; q += 32u) mk[a0 + q] = v0;
-        }
+        if (in && p < g1 && p + c > g0) mk[max(p, g0) - g0] = (uint16_t)(k + 1u);
     }
-    // a short last tile: the groups past its end read word 0, never an
-    // index left by an earlier tile or never written
-    for (uint32_t q = (g1 - g0) + lane; q < (uint32_t)GT; q += 32u) mk[q] = 0;
 }
 
 // Patterns of chunk j (groups 128*j + 4*lane + e of the tile) of an impure
-// operand, from the word indices gop_mark placed (index 0, past a short
-// last tile's end, reads staged word 0).
-__device__ __forceinline__ uint4 gop_chunk(const uint32_t* ws, const uint16_t* mk, uint32_t j) {
+// operand; carry = the last word index + 1 seen before the chunk.
+__device__ __forceinline__ uint4 gop_chunk(const uint32_t* ws, const uint16_t* mk, uint32_t j, uint32_t& carry) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint2 m = reinterpret_cast<const uint2*>(mk)[32 * j + lane];
-    const uint32_t i0 = m.x & 0xFFFFu, i1 = m.x >> 16, i2 = m.y & 0xFFFFu, i3 = m.y >> 16;
+    const uint32_t r0 = m.x & 0xFFFFu, r1 = max(r0, m.x >> 16), r2 = max(r1, m.y & 0xFFFFu), r3 = max(r2, m.y >> 16);
+    uint32_t inc = r3;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, inc, d);
+        if (lane >= (uint32_t)d) inc = max(inc, t);
+    }
+    uint32_t ex = __shfl_up_sync(0xffffffffu, inc, 1);
+    if (lane == 0) ex = 0;
+    ex = max(ex, carry);
+    carry = max(carry, __shfl_sync(0xffffffffu, inc, 31));
+    const uint32_t i0 = max(ex, r0), i1 = max(ex, r1), i2 = max(ex, r2), i3 = max(ex, r3);  // >= 1 inside the tile
     return make_uint4(wpattern(ws[i0 ? i0 - 1u : 0u]), wpattern(ws[i1 ? i1 - 1u : 0u]),
                       wpattern(ws[i2 ? i2 - 1u : 0u]), wpattern(ws[i3 ? i3 - 1u : 0u]));
 }
@@ -170,12 +158,12 @@ __device__ __forceinline__ uint4 gop_ld4(const uint32_t* ws, uint32_t q, bool al
 
 // Result patterns of one warp's tile [g0, g1) of x OP y: both operands'
 // words over the tile are staged in shared memory at once with cp.async and
-// expanded to one 31-bit pattern per group (each word writes its index into
-// the groups it covers, found by a warp scan of the lengths, and each group
-// reads its word back; an operand with one word per group is read
+// expanded to one 31-bit pattern per group (a word-start marker per word
+// and a warp max-scan find the word of every group, so a fill costs one
+// marker whatever its length; an operand with one word per group is read
 // directly).  Calls f(j, r) for the chunks j = 0..7 in order, r holding the
 // results of groups 128 j + 4 lane + e of the tile (e = 0..3; groups past
-// g1 hold meaningless patterns and must be ignored).  prev
+// g1 hold whatever the zero-padded words give and must be ignored).  prev
 // is set to the result of group g0 - 1 (0 for g0 = 0).  Returns false for a
 // word range the metadata scan would have rejected (the patterns are then
 // meaningless).
@@ -203,32 +191,47 @@ __device__ __forceinline__ bool gop_tile(const uint32_t* __restrict__ xw, const 
     }
     cp_async_wait_all();
     __syncwarp();
-    // an impure operand is placed first (its word indices then its
-    // patterns); two impure operands share the index array one after the
-    // other, so the second one's patterns are read in a second sweep
+    uint32_t xc = 0, yc = 0;
+    // an impure operand is placed first (its markers then its patterns);
+    // two impure operands share the marker array one after the other, so
+    // the second one's patterns are read in a second sweep
     const bool both = !xpure && !ypure;
     uint4 xb[8];
     if (!xpure) {
+        reinterpret_cast<uint2*>(W.mk)[lane] = make_uint2(0u, 0u);
+#pragma unroll
+        for (int j = 1; j < 8; ++j) reinterpret_cast<uint2*>(W.mk)[32 * j + lane] = make_uint2(0u, 0u);
+        __syncwarp();
         gop_mark(wsx, W.mk, xn, xs0, g0, g1);
         __syncwarp();
         if (both) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) xb[j] = gop_chunk(wsx, W.mk, j);
+            for (int j = 0; j < 8; ++j) xb[j] = gop_chunk(wsx, W.mk, j, xc);
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < 8; ++j) reinterpret_cast<uint2*>(W.mk)[32 * j + lane] = make_uint2(0u, 0u);
             __syncwarp();
         }
     }
     if (!ypure) {
-        gop_mark(wsy, W.mk, yn, ys0, g0, g1);
-        __syncwarp();
+        if (xpure) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) reinterpret_cast<uint2*>(W.mk)[32 * j + lane] = make_uint2(0u, 0u);
+            __syncwarp();
+        }
+        if (xpure || both) {
+            gop_mark(wsy, W.mk, yn, ys0, g0, g1);
+            __syncwarp();
+        }
     }
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         uint4 a, b;
         if (xpure) a = pattern4(gop_ld4(wsx, 32 * j + lane, (xi0 & 3u) == 0u));
         else if (both) a = xb[j];
-        else a = gop_chunk(wsx, W.mk, j);
+        else a = gop_chunk(wsx, W.mk, j, xc);
         if (ypure) b = pattern4(gop_ld4(wsy, 32 * j + lane, (yi0 & 3u) == 0u));
-        else b = gop_chunk(wsy, W.mk, j);
+        else b = gop_chunk(wsy, W.mk, j, yc);
         f(j, make_uint4(op2<OP>(a.x, b.x), op2<OP>(a.y, b.y), op2<OP>(a.z, b.z), op2<OP>(a.w, b.w)));
     }
     return ok;

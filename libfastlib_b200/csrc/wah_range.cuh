@@ -458,11 +458,15 @@ __global__ void __launch_bounds__(RTHREADS, 6) k_range(RangeArgs A) {
                 sb = S.hdr[4]; nb = S.hdr[5] - sb;
             }
             const uint32_t nsel = na + nb;
-            // row checks one per warp; the bitmaps to OR in batches of up to
-            // 32 per warp (one per lane), spread over the warps
+            // row checks (the longest jobs) one per warp from warp 0; the
+            // bitmaps to OR in batches of up to 32 per warp (one per lane),
+            // spread over the warps from the one after the checks, so the
+            // warps holding a check get an OR batch last
             for (uint32_t c = warp; c < nc; c += RWARPS) warp_or_bitmap(S, I, T.cand[c], k, g0, g1, G, anb, &T);
-            const uint32_t per = min(32u, (nsel + RWARPS - 1) / RWARPS);
-            for (uint32_t j0 = warp * per; j0 < nsel; j0 += RWARPS * per) {
+            const uint32_t nfree = RWARPS - min(nc, (uint32_t)RWARPS - 1u);  // warps without a check
+            const uint32_t per = min(32u, (nsel + nfree - 1) / nfree);
+            const uint32_t wr = (warp + RWARPS - nc % RWARPS) % RWARPS;      // the warp's place in the OR order
+            for (uint32_t j0 = wr * per; j0 < nsel; j0 += RWARPS * per) {
                 const uint32_t jj = j0 + lane;
                 const bool have = lane < per && jj < nsel;
                 uint32_t b = 0;

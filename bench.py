@@ -232,6 +232,10 @@ def main():
     ap.add_argument("--dense-engine", type=int, default=0, choices=[0, 1, 2, 3, 4, 5],
                     help="canonical-result operators: 0 auto, 1 pipelined group-space kernel, 2 word-space merge, "
                          "3 two-pass group-space kernels, 4 single pass over CTA tiles, 5 single pass over warp tiles")
+    ap.add_argument("--only-relic", action="store_true",
+                    help="only the relic case (index built on the GPU), batch with row ids run warmup + steps times (for ncu)")
+    ap.add_argument("--relic-order", type=int, default=0, choices=[0, 2],
+                    help="work order of --only-relic: 0 query by query with the look-back, 2 two tile-major passes")
     ap.add_argument("--only-batched", default=None,
                     help="ROWS:QUERIES — only the batched conjunctive case (its 8 columns at that size), tile-major "
                          "count batch run warmup + steps times (for ncu)")
@@ -262,6 +266,9 @@ def main():
         return
     if args.only_batched:
         run_only_batched(args)
+        return
+    if args.only_relic:
+        run_only_relic(args)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -582,6 +589,40 @@ def batched_columns(ctx, n, keep_host=False):
     return cols, metas, host_cols
 
 
+def run_only_relic(args):
+    """The relic case built on the GPU (1M uint32 rows U[0,100), 100 ranges,
+    counts and all row ids), in the given work order (--relic-order: 0 query
+    by query with the look-back, 2 two tile-major passes); one batch run
+    warmup + steps times; prints one JSON line."""
+    import torch
+    import libfastlib_b200 as L
+    n = 1_000_000
+    vals = np.random.Generator(np.random.PCG64(42)).integers(0, 100, size=n).astype(np.uint32)
+    qrng = np.random.Generator(np.random.PCG64(7))
+    qs = []
+    while len(qs) < 100:
+        lo, hi = (int(v) for v in qrng.integers(0, 101, size=2))
+        if lo < hi:
+            qs.append((float(lo), float(hi)))
+    ctx = L.Context(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    idx = L.Index.build(ctx, L.RELIC, vals)
+    queries = [[idx.term(lo, hi)] for lo, hi in qs]
+    C = L.Batch(ctx, queries, 0)
+    C.run()
+    total = int(sum(int(c) for c in C.counts()))
+    B = L.Batch(ctx, queries, rid_cap=total)
+    ctx.set_tuning(L.TUNE_RANGE_ORDER, args.relic_order)
+    for _ in range(args.warmup):
+        B.run()
+    ms = _ev_time(stream, B.run, args.steps)
+    print(json.dumps({"only_relic": args.relic_order, "ms_per_batch": ms, "queries_per_s": len(qs) / ms * 1e3,
+                      "row_ids": total}))
+    ctx.set_stream(None)
+
+
 def run_only_batched(args):
     """The batched conjunctive case at a chosen size (the same 8 columns at
     ROWS rows, QUERIES conjunctions), one count-only tile-major batch run
@@ -748,6 +789,9 @@ def relic_workload(args, ctx, stream, peak):
     C.close()
     total = sum(counts)
     B = L.Batch(ctx, queries, rid_cap=total)
+    from libfastlib_b200 import tune
+    # query-major with the look-back, or two tile-major passes around a scan
+    best, table = tune.tune_batch(ctx, B, count_only=False, ctas=(0,), reps=2)
     for _ in range(args.warmup):
         B.run()
     torch.cuda.synchronize()
@@ -756,6 +800,7 @@ def relic_workload(args, ctx, stream, peak):
         B.run()
     g.replay()
     torch.cuda.synchronize()
+    tuned = {"order": _ORDER_NAMES[best[0]], "candidates_ms": {_ORDER_NAMES[k[0]]: round(v, 3) for k, v in table.items()}}
     flushbuf = torch.zeros(64 << 20, dtype=torch.int32, device=f"cuda:{ctx.device}")  # 256 MB > L2
     reps = max(5, min(args.steps, 50))
     ts = _ev_time_each(stream, g.replay, reps, lambda: flushbuf.add_(1))
@@ -816,12 +861,14 @@ def relic_workload(args, ctx, stream, peak):
     e2e_s = (time.perf_counter() - t0) / e_reps
     mb = B.min_bytes() + 4 * total
     gbs = mb / (ms / 1e3) / 1e9
+    ctx.set_tuning(L.TUNE_RANGE_ORDER, 1)
+    ctx.set_tuning(L.TUNE_RANGE_CTAS, 0)
     out = {
         "workload": "relic: ibis::relic over 1,000,000 uint32 rows uniform in [0,100), 100 ranges lo <= x < hi "
                     "(seeded); hit counts and ascending row ids of every query, one fused launch (CUDA graph)",
         "index_source": source,
         "queries": len(qs), "row_ids": total,
-        "queries_per_s": len(qs) / (ms / 1e3), "ms_per_batch": ms,
+        "queries_per_s": len(qs) / (ms / 1e3), "ms_per_batch": ms, "tuned": tuned,
         "one_query_per_launch_queries_per_s": len(qs) / (ms1 / 1e3),
         "e2e": {"value": len(qs) / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 4 * total + 8 * len(qs),

@@ -134,8 +134,8 @@ struct RangeShared {
     uint64_t scan[RWARPS + 1];
     uint32_t hdr[8];
     unsigned long long base;
-    DevTerm term[2];    // the term being evaluated and the next one, with their indexes
-    DevIndex index[2];
+    DevTerm term;    // the term being evaluated and its index
+    DevIndex index;
 };
 constexpr uint32_t TERM_WORDS = sizeof(DevTerm) / 4, INDEX_WORDS = sizeof(DevIndex) / 4;
 static_assert(sizeof(DevTerm) % 4 == 0 && TERM_WORDS <= 32, "a warp stages a term");
@@ -392,23 +392,18 @@ __global__ void __launch_bounds__(RTHREADS, 6) k_range(RangeArgs A) {
         }
 
         for (uint32_t l = tid; l < RT; l += RTHREADS) S.acc[l] = ALLONES;
-        // the term and its index, staged in shared memory by one warp: the
-        // first before the term loop, each later one into the other buffer
-        // by the last warp at the end of the term before it (its loads
-        // overlap that term's work; the barrier closing the term publishes it)
-        auto stage = [&](uint32_t t, uint32_t buf) {
-            const uint32_t v = lane < TERM_WORDS ? __ldg(reinterpret_cast<const uint32_t*>(A.terms + t) + lane) : 0u;
-            const uint32_t ix = __shfl_sync(0xffffffffu, v, 0);  // DevTerm::index
-            if (lane < TERM_WORDS) reinterpret_cast<uint32_t*>(&S.term[buf])[lane] = v;
-            if (lane < INDEX_WORDS)
-                reinterpret_cast<uint32_t*>(&S.index[buf])[lane] = __ldg(reinterpret_cast<const uint32_t*>(A.idx + ix) + lane);
-        };
-        if (warp == 0 && Q.t0 < Q.t1) stage(Q.t0, 0u);
-        __syncthreads();
-        uint32_t tb = 0;  // the buffer of the current term
-        for (uint32_t t = Q.t0; t < Q.t1; ++t, tb ^= 1u) {
-            const DevTerm& T = S.term[tb];
-            const DevIndex& I = S.index[tb];
+        for (uint32_t t = Q.t0; t < Q.t1; ++t) {
+            // the term and its index, staged in shared memory by warp 0
+            if (warp == 0) {
+                const uint32_t v = lane < TERM_WORDS ? __ldg(reinterpret_cast<const uint32_t*>(A.terms + t) + lane) : 0u;
+                const uint32_t ix = __shfl_sync(0xffffffffu, v, 0);  // DevTerm::index
+                if (lane < TERM_WORDS) reinterpret_cast<uint32_t*>(&S.term)[lane] = v;
+                if (lane < INDEX_WORDS)
+                    reinterpret_cast<uint32_t*>(&S.index)[lane] = __ldg(reinterpret_cast<const uint32_t*>(A.idx + ix) + lane);
+            }
+            __syncthreads();
+            const DevTerm& T = S.term;
+            const DevIndex& I = S.index;
             uint4* t4 = reinterpret_cast<uint4*>(S.tmp);
             if (T.c1) {
                 // the wholly-inside span from two cumulative rows
@@ -492,10 +487,6 @@ __global__ void __launch_bounds__(RTHREADS, 6) k_range(RangeArgs A) {
                 for (uint32_t c = warp; c < T.ncand; c += RWARPS)
                     warp_or_bitmap(S, I, T.cand[c], k, g0, g1, G, anb, &T);
             }
-            // the next term into the other buffer (last read by the term
-            // before this one, which every thread finished at its closing
-            // barrier)
-            if (warp == RWARPS - 1 && t + 1 < Q.t1) stage(t + 1, tb ^ 1u);
             __syncthreads();
             uint32_t any = 0;
             for (uint32_t l = tid; l < RT; l += RTHREADS) { const uint32_t v = S.acc[l] & S.tmp[l]; S.acc[l] = v; any |= v; }

@@ -3,7 +3,7 @@
 // all-literal loops, src/bitvector.cpp:2545-2830, 2981-3278, 3354-3619,
 // 3748-4079): one launch, operands read once, result words written once.
 //
-// k_gone<OP>: one warp per tile of GT = 1024 groups, warps claiming tiles in
+// k_gone<OP>: one warp per tile of GT = 512 groups, warps claiming tiles in
 // launch order; no shared-memory staging of words.
 //  1. paint: the warp reads each operand's words over its tile as 32-word
 //     rows (eight rows of both operands in flight per lane), finds each
@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(GTHREADS) k_gone(FuseArgs A) {
     uint32_t hm = 0;  // the lane's heads: bit 4 j + e for group 128 j + 4 lane + e
     uint32_t heads = 0, ones = 0, lasth = 0;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int j = 0; j < NCH; ++j) {
         const uint4 r = gone_chunk<OP>(W, j);
         uint32_t pb = __shfl_up_sync(0xffffffffu, r.w, 1);
         if (lane == 0) pb = before;
@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(GTHREADS) k_gone(FuseArgs A) {
         uint32_t carry = pre.y;  // the last head before the chunk (packed)
         const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll 1
-        for (int j = 0; j < 8; ++j) {
+        for (int j = 0; j < NCH; ++j) {
             const uint32_t m = (hm >> (4 * j)) & 15u;
             const uint32_t hl = __ballot_sync(0xffffffffu, m != 0u);
             if (hl == 0u) continue;  // a chunk inside a run

@@ -6,7 +6,7 @@
 // the run holds two or more groups) and one literal per mixed group.
 //
 // Two launches, no look-back and no cross-CTA waits:
-//  * k_gop<OP>: one warp per tile of GT = 1024 groups (the stride of the
+//  * k_gop<OP>: one warp per tile of GT = 512 groups (the stride of the
 //    operands' group-tile index, which gives each tile's word range).  Both
 //    operands' words over the tile are staged in shared memory at once with
 //    cp.async and expanded to one 31-bit pattern per group (a word-start
@@ -20,7 +20,7 @@
 //  * k_gpack: one warp per tile with heads re-reads R, ranks the heads and
 //    writes the words in order: a mixed head's literal, or the run word
 //    whose length reaches the next head.
-// Lanes own groups in eight chunks of four consecutive groups (group
+// Lanes own groups in NCH = 4 chunks of four consecutive groups (group
 // 128*j + 4*lane + e of the tile), so every global access of R is a
 // coalesced 16-byte vector and the chunk-major order is the group order.
 #ifndef WAH_GOP_CUH
@@ -32,12 +32,13 @@ namespace wah {
 constexpr int GT = DT;                    // groups per tile: one warp's tile (the group-tile index stride)
 constexpr int GWARPS = 4;                 // warps (tiles) per CTA
 constexpr int GTHREADS = GWARPS * 32;
-constexpr int GWPL = 33;                  // staged words per lane when counting (odd: conflict-free)
+constexpr int NCH = GT / 128;             // chunks of 128 groups (4 per lane) per tile
+constexpr int GWPL = (GT + 4 + 31) / 32;  // staged words per lane
 constexpr uint32_t GNONE = 0xFFFFFFFFu;   // no head in the tile
 constexpr uint32_t GSEG = 256;            // tiles per segment of the two-level prefix
 // staging holds a tile's <= GT words plus up to 3 before them and the
 // rest of the last 16-byte chunk
-static_assert(GT == 8 * 128 && GWPL * 32 >= GT + 4 && (GWPL * 32 * 4) % 16 == 0, "tile shape");
+static_assert(GT == NCH * 128 && NCH <= 8 && GWPL * 32 >= GT + 4 && (GWPL * 32 * 4) % 16 == 0, "tile shape");
 
 struct GopArgs {
     const uint32_t* xw; const uint32_t* xgt; uint32_t nx;
@@ -196,27 +197,27 @@ __device__ __forceinline__ bool gop_tile(const uint32_t* __restrict__ xw, const 
     // two impure operands share the marker array one after the other, so
     // the second one's patterns are read in a second sweep
     const bool both = !xpure && !ypure;
-    uint4 xb[8];
+    uint4 xb[NCH];
     if (!xpure) {
         reinterpret_cast<uint2*>(W.mk)[lane] = make_uint2(0u, 0u);
 #pragma unroll
-        for (int j = 1; j < 8; ++j) reinterpret_cast<uint2*>(W.mk)[32 * j + lane] = make_uint2(0u, 0u);
+        for (int j = 1; j < NCH; ++j) reinterpret_cast<uint2*>(W.mk)[32 * j + lane] = make_uint2(0u, 0u);
         __syncwarp();
         gop_mark(wsx, W.mk, xn, xs0, g0, g1);
         __syncwarp();
         if (both) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) xb[j] = gop_chunk(wsx, W.mk, j, xc);
+            for (int j = 0; j < NCH; ++j) xb[j] = gop_chunk(wsx, W.mk, j, xc);
             __syncwarp();
 #pragma unroll
-            for (int j = 0; j < 8; ++j) reinterpret_cast<uint2*>(W.mk)[32 * j + lane] = make_uint2(0u, 0u);
+            for (int j = 0; j < NCH; ++j) reinterpret_cast<uint2*>(W.mk)[32 * j + lane] = make_uint2(0u, 0u);
             __syncwarp();
         }
     }
     if (!ypure) {
         if (xpure) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) reinterpret_cast<uint2*>(W.mk)[32 * j + lane] = make_uint2(0u, 0u);
+            for (int j = 0; j < NCH; ++j) reinterpret_cast<uint2*>(W.mk)[32 * j + lane] = make_uint2(0u, 0u);
             __syncwarp();
         }
         if (xpure || both) {
@@ -225,7 +226,7 @@ __device__ __forceinline__ bool gop_tile(const uint32_t* __restrict__ xw, const 
         }
     }
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int j = 0; j < NCH; ++j) {
         uint4 a, b;
         if (xpure) a = pattern4(gop_ld4(wsx, 32 * j + lane, (xi0 & 3u) == 0u));
         else if (both) a = xb[j];
@@ -349,7 +350,7 @@ __global__ void __launch_bounds__(GTHREADS) k_gpack(GopArgs A) {
     uint32_t rest = cnt;   // heads in the chunks before and at the current one
     bool fill = false;
 #pragma unroll
-    for (int j = 7; j >= 0; --j) {
+    for (int j = NCH - 1; j >= 0; --j) {
         const uint32_t m = (hm >> (4 * j)) & 15u;
         const uint32_t hl = __ballot_sync(0xffffffffu, m != 0u);
         if (hl == 0u) continue;  // a chunk inside a run

@@ -1,6 +1,6 @@
 """A CPU model of the two-pass group-space engine (libfastlib_b200/csrc/
 wah_gop.cuh: k_gop, k_gpack) checked against the oracle: the word range of
-each 1024-group tile from the group-tile index, word placement by start
+each 512-group tile from the group-tile index, word placement by start
 markers and a running maximum, the dense result patterns, the run heads
 (with the group before the tile), the per-segment totals that give each
 tile its output offset and the next head after it, and the words and bpos
@@ -14,7 +14,9 @@ import oracle
 from oracle import wahgen as G
 
 ALL, H0, H1, MAXC = 0x7FFFFFFF, 0x80000000, 0xC0000000, 0x3FFFFFFF
-DT = GT = 1024          # group-tile index stride = groups per tile
+DT = GT = 512           # group-tile index stride = groups per tile
+NCH = GT // 128         # chunks of 128 groups per tile
+GWS = (GT + 4 + 31) // 32 * 32  # staged words per operand
 SEG = 256               # tiles per segment
 NONE = 0xFFFFFFFF
 
@@ -78,7 +80,7 @@ def cls(v):
 
 def gpack_lanes(head, g0, cnt, nxt):
     """k_gpack's lane arithmetic for one tile: head[i] is True for the run
-    heads among the tile's 1024 groups (lane l of chunk j holds groups
+    heads among the tile's GT groups (lane l of chunk j holds groups
     128 j + 4 l .. + 3).  Chunks are taken last to first; a lane's first
     output index is the heads of the chunks before (the tile's count minus
     the chunks already taken) plus those of the lanes before it (from the
@@ -93,7 +95,7 @@ def gpack_lanes(head, g0, cnt, nxt):
             hm[rem // 4] |= 1 << (4 * j + rem % 4)
     out = {}
     later, rest = nxt, cnt
-    for j in range(7, -1, -1):
+    for j in range(NCH - 1, -1, -1):
         m = [(hm[l] >> (4 * j)) & 15 for l in range(32)]
         hl = sum(1 << l for l in range(32) if m[l])
         if hl == 0:
@@ -224,7 +226,7 @@ def test_model_equals_oracle(seed):
     rng = np.random.default_rng(seed)
     checked = 0
     for trial in range(6):
-        ng = int(rng.integers(1, 5)) * GT + int(rng.integers(0, GT)) if trial % 3 else int(rng.integers(1, 900))
+        ng = int(rng.integers(1, 5)) * 1024 + int(rng.integers(0, 1024)) if trial % 3 else int(rng.integers(1, 900))
         wa, wb = _dense_words(rng, ng), _dense_words(rng, ng)
         if len(wa) + len(wb) <= ng:      # not the canonical-result path
             continue
@@ -272,9 +274,9 @@ def stage_copies(wi0, nw, n):
 def test_stage_arithmetic():
     """16-byte copies start on 16-byte boundaries on both sides, no copy
     reads past the array, every word of the tile lands at ws[k + (wi0 & 3)]
-    and the staging buffer (33 * 32 words) is never overrun."""
+    and the staging buffer (GWS words) is never overrun."""
     rng = np.random.default_rng(3)
-    cases = [(w, nw, n) for n in (1, 2, 3, 4, 5, 7, 8, 1024, 1025, 1027, 5000)
+    cases = [(w, nw, n) for n in (1, 2, 3, 4, 5, 7, 8, 512, 513, 515, 1024, 1025, 1027, 5000)
              for w in range(0, min(n, 9)) for nw in (1, 2, 3, 4, 5, n - w) if 0 < nw <= min(GT, n - w)]
     for _ in range(3000):
         n = int(rng.integers(1, 40000))
@@ -286,7 +288,7 @@ def test_stage_arithmetic():
         for si, gi, k in copies:
             if k == 4:
                 assert si % 4 == 0 and gi % 4 == 0
-            assert gi + k <= n and si + k <= 33 * 32, (wi0, nw, n)
+            assert gi + k <= n and si + k <= GWS, (wi0, nw, n)
             for e in range(k):
                 ws[si + e] = gi + e
         for kk in range(nw):

@@ -39,7 +39,7 @@
 
 namespace wah {
 
-constexpr int DT = 256;                   // group-tile index stride (k_gtile)
+constexpr int DT = 512;                   // group-tile index stride (k_gtile)
 constexpr uint32_t DEND = 0xFFFFFFFFu;    // slot marker: no more tiles
 constexpr uint32_t DFAST = 0xFFFFFFFFu;   // step code: 128 mixed literals
 

@@ -3,7 +3,7 @@
 // all-literal loops, src/bitvector.cpp:2545-2830, 2981-3278, 3354-3619,
 // 3748-4079): one launch, operands read once, result words written once.
 //
-// k_gone<OP>: one warp per tile of GT = 256 groups, warps claiming tiles in
+// k_gone<OP>: one warp per tile of GT = 512 groups, warps claiming tiles in
 // launch order; no shared-memory staging of words.
 //  1. paint: the warp reads each operand's words over its tile as 32-word
 //     rows (eight rows of both operands in flight per lane), finds each

@@ -6,7 +6,7 @@
 // the run holds two or more groups) and one literal per mixed group.
 //
 // Two launches, no look-back and no cross-CTA waits:
-//  * k_gop<OP>: one warp per tile of GT = 256 groups (the stride of the
+//  * k_gop<OP>: one warp per tile of GT = 512 groups (the stride of the
 //    operands' group-tile index, which gives each tile's word range).  Both
 //    operands' words over the tile are staged in shared memory at once with
 //    cp.async and expanded to one 31-bit pattern per group (a word-start
@@ -20,7 +20,7 @@
 //  * k_gpack: one warp per tile with heads re-reads R, ranks the heads and
 //    writes the words in order: a mixed head's literal, or the run word
 //    whose length reaches the next head.
-// Lanes own groups in NCH = 2 chunks of four consecutive groups (group
+// Lanes own groups in NCH = 4 chunks of four consecutive groups (group
 // 128*j + 4*lane + e of the tile), so every global access of R is a
 // coalesced 16-byte vector and the chunk-major order is the group order.
 #ifndef WAH_GOP_CUH

@@ -17,7 +17,7 @@ import oracle
 from oracle import wahgen as G
 
 ALL, H0, H1, MAXC = 0x7FFFFFFF, 0x80000000, 0xC0000000, 0x3FFFFFFF
-DT = 256
+DT = 512
 FWPT, FGPT = 8, 8
 C_ZERO, C_ONE, C_MIXED = 0, 1, 2
 
@@ -246,7 +246,7 @@ def test_model_geometric_runs():
             assert np.array_equal(got, np.asarray(want, np.uint32)), (d, op)
 
 
-def model_warp_tiles(op, groups_a, groups_b, GT=256):
+def model_warp_tiles(op, groups_a, groups_b, GT=512):
     """The words k_gone<OP> (libfastlib_b200/csrc/wah_gone.cuh) writes, from
     the operands' group patterns (its expansion is the two-pass engine's,
     checked on the GPU): per tile of GT groups the lane heads of chunks of

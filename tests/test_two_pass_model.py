@@ -1,6 +1,6 @@
 """A CPU model of the two-pass group-space engine (libfastlib_b200/csrc/
 wah_gop.cuh: k_gop, k_gpack) checked against the oracle: the word range of
-each 256-group tile from the group-tile index, word placement by start
+each 512-group tile from the group-tile index, word placement by start
 markers and a running maximum, the dense result patterns, the run heads
 (with the group before the tile), the per-segment totals that give each
 tile its output offset and the next head after it, and the words and bpos
@@ -14,7 +14,7 @@ import oracle
 from oracle import wahgen as G
 
 ALL, H0, H1, MAXC = 0x7FFFFFFF, 0x80000000, 0xC0000000, 0x3FFFFFFF
-DT = GT = 256           # group-tile index stride = groups per tile
+DT = GT = 512           # group-tile index stride = groups per tile
 NCH = GT // 128         # chunks of 128 groups per tile
 GWS = (GT + 4 + 31) // 32 * 32  # staged words per operand
 SEG = 256               # tiles per segment

@@ -198,7 +198,7 @@ struct SegRec {
 };
 
 template <int OP, bool FSM, bool UNARY, bool FLIP, int TB>
-__global__ void __launch_bounds__(MERGE_THREADS, 4) k_merge(MergeArgs A) {
+__global__ void __launch_bounds__(MERGE_THREADS, 2) k_merge(MergeArgs A) {
     constexpr int TILE_BLOCKS = TB, SEG_PER_THREAD = MCfg<TB>::SEG_PER_THREAD;
     using TileShared = wah::TileShared<TB>;
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -239,7 +239,7 @@ __device__ __forceinline__ bool gop_tile(const uint32_t* __restrict__ xw, const 
 }
 
 template <int OP>
-__global__ void __launch_bounds__(GTHREADS) k_gop(GopArgs A) {
+__global__ void __launch_bounds__(GTHREADS, 10) k_gop(GopArgs A) {
     extern __shared__ __align__(16) unsigned char gsm[];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t t = blockIdx.x * GWARPS + warp;

@@ -295,6 +295,9 @@ __global__ void __launch_bounds__(GTHREADS, 10) k_gop(GopArgs A) {
 // the lanes find it with a suffix minimum over the lanes after them, chunks
 // taken last to first.  The warp of the last tile writes the metadata.
 __global__ void __launch_bounds__(GTHREADS) k_gpack(GopArgs A) {
+    // this tile's words, from the 16-byte boundary at or below its first
+    // output index (a tile holds at most GT heads, so GT + 3 slots)
+    __shared__ __align__(16) uint32_t sout[GWARPS][GT + 4];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t t = blockIdx.x * GWARPS + warp;
     const uint32_t T = A.ntiles;
@@ -345,6 +348,8 @@ __global__ void __launch_bounds__(GTHREADS) k_gpack(GopArgs A) {
     const uint4* R4 = reinterpret_cast<const uint4*>(A.R + g0);
     // the lane's heads as k_gop found them: bit 4 j + e for group 128 j + 4 lane + e
     const uint32_t hm = A.hmask[(size_t)t * 32u + lane];
+    uint32_t* so = sout[warp];
+    const uint32_t oal = off & ~3u;
     const uint32_t gt = (2u << lane) - 1u;  // lanes up to this one (lane 31: all)
     uint32_t later = nxt;  // the first head after the chunk
     uint32_t rest = cnt;   // heads in the chunks before and at the current one
@@ -380,7 +385,7 @@ __global__ void __launch_bounds__(GTHREADS) k_gpack(GopArgs A) {
                     const uint32_t more = m >> (e + 1);
                     const uint32_t next = more ? g + e + __ffs(more) : after;
                     const uint32_t wd = run_word(cls_of(r[e]), next - (g + e), r[e], false);
-                    A.out[o] = wd;
+                    so[o - oal] = wd;
                     if ((o & 31u) == 0u) A.obp[o >> 5] = g + e;
                     if (o == 0u) A.meta->w0 = wd;
                     fill |= is_fill(wd);
@@ -389,6 +394,20 @@ __global__ void __launch_bounds__(GTHREADS) k_gpack(GopArgs A) {
         }
     }
     if (__any_sync(0xffffffffu, fill) && lane == 0) atomicOr(&A.meta->nfill, 1u);
+    // the tile's words leave as 16-byte stores (the output array is a pool
+    // block, 16-byte aligned), the ragged ends word by word
+    __syncwarp();
+    const uint32_t end = off + cnt;
+    for (uint32_t v = lane; 4u * v < end - oal; v += 32u) {
+        const uint32_t gi = oal + 4u * v;
+        if (gi >= off && gi + 4u <= end) {
+            *reinterpret_cast<uint4*>(A.out + gi) = *reinterpret_cast<const uint4*>(so + 4u * v);
+        } else {
+#pragma unroll
+            for (uint32_t e = 0; e < 4u; ++e)
+                if (gi + e >= off && gi + e < end) A.out[gi + e] = so[4u * v + e];
+        }
+    }
 }
 
 }  // namespace wah

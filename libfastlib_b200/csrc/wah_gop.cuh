@@ -130,21 +130,20 @@ __device__ __forceinline__ void gop_mark(const uint32_t* ws, uint16_t* mk, uint3
 }
 
 // Patterns of chunk j (groups 128*j + 4*lane + e of the tile) of an impure
-// operand; carry = the last word index + 1 seen before the chunk.
+// operand; carry = the last word index + 1 seen before the chunk (markers,
+// word index + 1 at a word's first group, grow with the group).
 __device__ __forceinline__ uint4 gop_chunk(const uint32_t* ws, const uint16_t* mk, uint32_t j, uint32_t& carry) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint2 m = reinterpret_cast<const uint2*>(mk)[32 * j + lane];
     const uint32_t r0 = m.x & 0xFFFFu, r1 = max(r0, m.x >> 16), r2 = max(r1, m.y & 0xFFFFu), r3 = max(r2, m.y >> 16);
-    uint32_t inc = r3;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, inc, d);
-        if (lane >= (uint32_t)d) inc = max(inc, t);
-    }
-    uint32_t ex = __shfl_up_sync(0xffffffffu, inc, 1);
-    if (lane == 0) ex = 0;
-    ex = max(ex, carry);
-    carry = max(carry, __shfl_sync(0xffffffffu, inc, 31));
+    // markers grow with the group, so the largest one before this lane is
+    // the last one of the nearest lower lane holding any
+    const uint32_t nz = __ballot_sync(0xffffffffu, r3 != 0u);
+    const uint32_t below = nz & ((1u << lane) - 1u);
+    const uint32_t lo = __shfl_sync(0xffffffffu, r3, below ? 31u - __clz(below) : lane);
+    const uint32_t hi = __shfl_sync(0xffffffffu, r3, nz ? 31u - __clz(nz) : 0u);
+    const uint32_t ex = below ? lo : carry;
+    if (nz) carry = hi;
     const uint32_t i0 = max(ex, r0), i1 = max(ex, r1), i2 = max(ex, r2), i3 = max(ex, r3);  // >= 1 inside the tile
     return make_uint4(wpattern(ws[i0 ? i0 - 1u : 0u]), wpattern(ws[i1 ? i1 - 1u : 0u]),
                       wpattern(ws[i2 ? i2 - 1u : 0u]), wpattern(ws[i3 ? i3 - 1u : 0u]));

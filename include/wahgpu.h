@@ -86,7 +86,7 @@ int64_t wahgpu_ctx_launches(wahgpu_ctx* ctx);
                                      only the tiles holding ids under each query's limit) */
 #define WAHGPU_TUNE_RANGE_CTAS 3  /* resident CTAs per SM of the persistent range launch: 0 (all that fit) .. 32 */
 #define WAHGPU_TUNE_CUM_STRIDE 5  /* bitmaps per cumulative row of indexes built or attached later: 0 auto, 1 none, >= 2 that stride */
-#define WAHGPU_TUNE_MERGE_TILE 6  /* block-index entries per tile of the word-space merge: 0 auto (8..64, sized so the tiles fill whole waves of resident CTAs), 16 | 32 | 64 */
+#define WAHGPU_TUNE_MERGE_TILE 6  /* block-index entries per tile of the word-space merge: 0 auto (by operand size), 16 | 32 | 64 */
 /* Failure-path test hooks (no counterpart in the reference; never needed in
  * normal use).  WAHGPU_TEST_WITHHOLD_TILE = t: in the next operator call on
  * the single-pass group-space engine, tile t never publishes its look-back

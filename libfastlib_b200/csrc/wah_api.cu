@@ -489,38 +489,15 @@ static void launch_merge_tb(const wahgpu_ctx* ctx, int op, bool fsm, bool unary,
     }
 #undef WG_MERGE_OP
 }
-// Resident CTAs of the merge kernel on the device for tiles of 16 / 32 / 64
-// entries (queried once per context).
-static uint64_t merge_slots(wahgpu_ctx* ctx, int i) {
-    if (!ctx->merge_slots[i]) {
-        int n = 0;
-        if (i == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_merge<OP_AND, true, false, false, 16>, MERGE_THREADS, sizeof(TileShared<16>));
-        else if (i == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_merge<OP_AND, true, false, false, 32>, MERGE_THREADS, sizeof(TileShared<32>));
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_merge<OP_AND, true, false, false, 64>, MERGE_THREADS, sizeof(TileShared<64>));
-        cudaGetLastError();
-        ctx->merge_slots[i] = (uint32_t)std::max(1, n) * (uint32_t)std::max(1, ctx->sm_count);
-    }
-    return ctx->merge_slots[i];
-}
-// Block-index entries per merge tile and the kernel (16, 32 or 64 entries
-// at most) that holds them: the context's setting, else the fewest entries
-// per tile (at least 8) that fill one wave of resident CTAs when the
-// operands fit one, else the tile that spreads them over whole waves of the
-// 64-entry kernel (a last wave mostly empty would cost a whole tile's time).
-static uint32_t merge_plan(wahgpu_ctx* ctx, uint32_t nblocks, uint32_t& kernel_tb) {
-    if (ctx->merge_tile) { kernel_tb = ctx->merge_tile; return ctx->merge_tile; }
-    const uint32_t T[3] = {16, 32, 64};
-    for (int i = 0; i < 3; ++i) {
-        const uint64_t slots = merge_slots(ctx, i);
-        if ((uint64_t)nblocks <= T[i] * slots) {
-            kernel_tb = T[i];
-            return (uint32_t)std::min<uint64_t>(T[i], std::max<uint64_t>(8, (nblocks + slots - 1) / slots));
-        }
-    }
-    const uint64_t slots = merge_slots(ctx, 2);
-    const uint64_t waves = ((uint64_t)nblocks + 64 * slots - 1) / (64 * slots);
-    kernel_tb = 64;
-    return (uint32_t)std::min<uint64_t>(64, (nblocks + waves * slots - 1) / (waves * slots));
+// Block-index entries per merge tile: the context's setting, else by the
+// operands' size: the largest of 64 / 32 / 16 that still gives about two
+// tiles per SM, so small operands spread over the GPU in short tiles.
+static uint32_t merge_tile_blocks(const wahgpu_ctx* ctx, uint32_t nblocks) {
+    if (ctx->merge_tile) return ctx->merge_tile;
+    const uint64_t want = 2ull * (uint64_t)ctx->sm_count;
+    if ((uint64_t)nblocks >= want * 64u) return 64;
+    if ((uint64_t)nblocks >= want * 32u) return 32;
+    return 16;
 }
 
 // Merge launch: x OP y, or a (complemented) copy of x when y == nullptr.
@@ -533,8 +510,7 @@ int wg_launch_merge(wahgpu_ctx* ctx, int op, bool fsm, bool unary, bool flip,
     int rc = bv_reserve(res, need);
     if (rc) return rc;
     const uint32_t nblk = unary ? nbx : nbx + nby;
-    uint32_t ktb = 64;
-    const uint32_t tb = merge_plan(ctx, nblk, ktb);
+    const uint32_t tb = merge_tile_blocks(ctx, nblk);
     uint32_t ntiles = (nblk + tb - 1) / tb;
     if (ntiles == 0) ntiles = 1;
     TileRec* recs; LaunchSync* sync;
@@ -545,12 +521,12 @@ int wg_launch_merge(wahgpu_ctx* ctx, int op, bool fsm, bool unary, bool flip,
     a.yw = y ? y->words : x->words; a.ybp = y ? y->bpos : x->bpos; a.ny = ny; a.nby = nby;
     a.groups = groups;
     a.out = res->words; a.obp = res->bpos; a.meta = res->meta;
-    a.recs = recs; a.sync = sync; a.ntiles = ntiles; a.tb = tb;
+    a.recs = recs; a.sync = sync; a.ntiles = ntiles;
     a.aval = aval; a.anb = anb;
     CUDA_TRY(ctx, cudaMemsetAsync(res->meta, 0, sizeof(DevMeta), ctx->stream));
     dim3 g(ntiles);
-    if (ktb == 16) launch_merge_tb<16>(ctx, op, fsm, unary, flip, g, ctx->stream, a);
-    else if (ktb == 32) launch_merge_tb<32>(ctx, op, fsm, unary, flip, g, ctx->stream, a);
+    if (tb == 16) launch_merge_tb<16>(ctx, op, fsm, unary, flip, g, ctx->stream, a);
+    else if (tb == 32) launch_merge_tb<32>(ctx, op, fsm, unary, flip, g, ctx->stream, a);
     else launch_merge_tb<64>(ctx, op, fsm, unary, flip, g, ctx->stream, a);
     ctx->launches++;
     CUDA_TRY(ctx, cudaGetLastError());

@@ -32,7 +32,6 @@ struct wahgpu_ctx {
     uint32_t range_order = 1;           // WAHGPU_TUNE_RANGE_ORDER
     uint32_t range_ctas = 0;            // WAHGPU_TUNE_RANGE_CTAS (0: as many as fit)
     uint32_t merge_tile = 0;            // WAHGPU_TUNE_MERGE_TILE (0: by operand size)
-    uint32_t merge_slots[3] = {0, 0, 0};  // resident merge CTAs on the device, tiles of 16 / 32 / 64 entries
     uint32_t cum_stride = 0;            // WAHGPU_TUNE_CUM_STRIDE (0 auto, 1 none)
     // failure-path test hooks (WAHGPU_TEST_*): the tile of the next
     // single-pass operator launch that never publishes its look-back record

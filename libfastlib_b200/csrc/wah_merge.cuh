@@ -5,11 +5,10 @@
 //
 // Work split.  Every operand carries a block-position index bpos[k] = group
 // position where word 32k starts (bpos[nblocks] = total groups).  The CTA for
-// tile t takes the t-th run of tb entries of the sorted union of the
+// tile t takes the t-th run of TILE_BLOCKS entries of the sorted union of the
 // two indexes (a merge path over bpos arrays only, found with a 32-way warp
 // search), so each CTA gets a group interval [Pa, Pb) holding at most
-// 32*(tb+2) words of both operands (tb at most the kernel's TB, chosen at
-// launch so the tiles fill whole waves of resident CTAs).  Both Pa and Pb are word
+// 32*(TILE_BLOCKS+2) words of both operands.  Both Pa and Pb are word
 // boundaries of one operand, hence segment boundaries.
 //
 // Segments.  Inside the tile the word ends of x and y are merged again (per
@@ -55,7 +54,6 @@ struct MergeArgs {
     TileRec* recs;
     LaunchSync* sync;
     uint32_t ntiles;
-    uint32_t tb;          // block-index entries per tile (<= the kernel's TB)
     uint32_t aval, anb;   // result active word (already combined)
 };
 
@@ -201,8 +199,7 @@ struct SegRec {
 
 template <int OP, bool FSM, bool UNARY, bool FLIP, int TB>
 __global__ void __launch_bounds__(MERGE_THREADS, 2) k_merge(MergeArgs A) {
-    constexpr int SEG_PER_THREAD = MCfg<TB>::SEG_PER_THREAD;
-    const uint32_t TILE_BLOCKS = min(A.tb, (uint32_t)TB);  // a tile holds at most 32 * (TB + 2) words
+    constexpr int TILE_BLOCKS = TB, SEG_PER_THREAD = MCfg<TB>::SEG_PER_THREAD;
     using TileShared = wah::TileShared<TB>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TileShared& S = *reinterpret_cast<TileShared*>(smem_raw);
@@ -231,7 +228,7 @@ __global__ void __launch_bounds__(MERGE_THREADS, 2) k_merge(MergeArgs A) {
         }
     } else if (warp < 2) {
         const uint32_t dtot = A.nbx + A.nby;
-        const uint32_t d = min((t + warp) * TILE_BLOCKS, dtot);
+        const uint32_t d = min((t + warp) * (uint32_t)TILE_BLOCKS, dtot);
         const uint32_t kx = warp_merge_split(A.xbp, A.nbx, A.ybp, A.nby, d);
         const uint32_t ky = d - kx;
         if (lane == 0) {

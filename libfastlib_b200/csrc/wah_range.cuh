@@ -165,13 +165,10 @@ __device__ __forceinline__ double col_value(const void* vals, uint32_t vtype, ui
     return (double)__ldg(reinterpret_cast<const uint32_t*>(vals) + row);
 }
 
-// One warp ORs bitmap b's words for the tile [g0, g1) into S.tmp.  With
-// check != nullptr the bitmap's rows are instead tested against the term's
-// comparison on the raw column and only passing rows are set.  The virtual
-// group G holds the active bits.
+// One warp ORs bitmap b's words for the tile [g0, g1) into S.tmp (the
+// virtual group G holds the active bits).
 __device__ __forceinline__ void warp_or_bitmap(RangeShared& S, const DevIndex& I, uint32_t b, uint32_t k,
-                                               uint32_t g0, uint32_t g1, uint32_t G, uint32_t anb,
-                                               const DevTerm* check) {
+                                               uint32_t g0, uint32_t g1, uint32_t G, uint32_t anb) {
     const uint32_t lane = threadIdx.x & 31u;
     const BitmapMeta m = I.bm[b];
     const uint32_t* tix = I.tiles + ((size_t)b * (I.ntiles + 1) + k) * 2;
@@ -213,31 +210,8 @@ __device__ __forceinline__ void warp_or_bitmap(RangeShared& S, const DevIndex& I
                 const uint32_t a = max(p, g0), e = min(p + c, g1);
                 const uint32_t pat = wpattern(wd);
                 for (uint32_t g = a; g < e; ++g) {
-                    if (!check) {
-                        if (pat == ALLONES) S.tmp[rsw(g - g0)] = ALLONES;
-                        else atomicOr(&S.tmp[rsw(g - g0)], pat);
-                    } else {
-                        // the rows of the group's 1 bits, RCHK raw values
-                        // loaded at once (one memory latency per RCHK rows)
-                        uint32_t bits = pat, set = 0;
-                        const uint32_t* raw = reinterpret_cast<const uint32_t*>(I.values);
-                        while (bits) {
-                            uint32_t hb[RCHK], v[RCHK];
-#pragma unroll
-                            for (int k = 0; k < RCHK; ++k) {
-                                hb[k] = bits ? 31u - __clz(bits) : 32u;
-                                if (bits) bits &= ~(1u << hb[k]);
-                            }
-#pragma unroll
-                            for (int k = 0; k < RCHK; ++k)  // every column type is 4 bytes a row
-                                v[k] = hb[k] < 32u ? __ldg(raw + g * 31u + (30u - hb[k])) : 0u;
-#pragma unroll
-                            for (int k = 0; k < RCHK; ++k)
-                                if (hb[k] < 32u && pass_cmp(raw_value(v[k], I.vtype), check->lop, check->lo, check->rop, check->hi))
-                                    set |= 1u << hb[k];
-                        }
-                        if (set) atomicOr(&S.tmp[rsw(g - g0)], set);
-                    }
+                    if (pat == ALLONES) S.tmp[rsw(g - g0)] = ALLONES;
+                    else atomicOr(&S.tmp[rsw(g - g0)], pat);
                 }
             }
         }
@@ -246,19 +220,107 @@ __device__ __forceinline__ void warp_or_bitmap(RangeShared& S, const DevIndex& I
     // virtual group G when the bitmap covers every row)
     const uint32_t Gb = m.groups;
     if (lane == 0 && m.anb > 0 && Gb >= g0 && Gb < g1) {
-        uint32_t pat = (m.aval & ((1u << m.anb) - 1u)) << (31u - m.anb);
-        if (check) {
-            uint32_t bits = pat, set = 0;
-            while (bits) {
-                const uint32_t hb = 31u - __clz(bits);
-                const uint32_t row = Gb * 31u + (30u - hb);
-                if (pass_cmp(col_value(I.values, I.vtype, row), check->lop, check->lo, check->rop, check->hi))
-                    set |= 1u << hb;
-                bits &= ~(1u << hb);
-            }
-            pat = set;
-        }
+        const uint32_t pat = (m.aval & ((1u << m.anb) - 1u)) << (31u - m.anb);
         if (pat) atomicOr(&S.tmp[rsw(Gb - g0)], pat);
+    }
+}
+
+// An edge bin's row check by one warp: the bin's rows in the tile [g0, g1)
+// whose raw values pass the term's comparison are OR'ed into S.tmp.  The
+// bin's words are taken 128 at a time; the first set row of every literal
+// of the batch has its raw value loaded before any is compared (one memory
+// latency per batch for the usual one-row literals of a sparse bin), the
+// other rows of a literal and the rows of 1-fills RCHK at a time after.
+__device__ __forceinline__ void warp_check_bitmap(RangeShared& S, const DevIndex& I, uint32_t b, uint32_t k,
+                                                  uint32_t g0, uint32_t g1, const DevTerm& T) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const BitmapMeta m = I.bm[b];
+    const uint32_t* tix = I.tiles + ((size_t)b * (I.ntiles + 1) + k) * 2;
+    const uint32_t i0 = __ldg(tix), s0 = __ldg(tix + 1);
+    const uint32_t in1 = __ldg(tix + 2), sn1 = __ldg(tix + 3);
+    const uint32_t i1 = min(sn1 < g1 ? in1 + 1u : in1, m.n);
+    const uint32_t* w = I.words + m.wstart;
+    const uint32_t* raw = reinterpret_cast<const uint32_t*>(I.values);  // every column type is 4 bytes a row
+    uint32_t carry = s0;
+    for (uint32_t base0 = i0; base0 < i1; base0 += 128) {
+        uint32_t wv[4], pv[4], cv[4], v0[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t i = base0 + 32u * j + lane;
+            wv[j] = i < i1 ? __ldg(w + i) : 0u;
+        }
+        // each row's first group per word
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t base = base0 + 32u * j;
+            pv[j] = 0; cv[j] = 0;
+            if (base < i1) {
+                const bool in = base + lane < i1;
+                const uint32_t wd = wv[j];
+                const uint32_t c = in ? wgroups(wd) : 0u;
+                if (__ballot_sync(0xffffffffu, in && is_fill(wd)) == 0u) {
+                    pv[j] = carry + lane;
+                    carry += __popc(__ballot_sync(0xffffffffu, in));
+                } else {
+                    uint32_t x = c;
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1) { uint32_t t = __shfl_up_sync(0xffffffffu, x, d); if (lane >= (uint32_t)d) x += t; }
+                    pv[j] = carry + x - c;
+                    carry += __shfl_sync(0xffffffffu, x, 31);
+                }
+                cv[j] = c;
+            }
+        }
+        // the first set row of every literal in the tile, all loads in flight
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t wd = wv[j];
+            const bool lit = cv[j] == 1u && !is_fill(wd) && wd != 0u && pv[j] >= g0 && pv[j] < g1;
+            v0[j] = lit ? __ldg(raw + pv[j] * 31u + (__clz(wd) - 1u)) : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t wd = wv[j], c = cv[j], p = pv[j];
+            if (c == 0u || wd == 0u || (is_fill(wd) && wd < HEADER1)) continue;
+            const bool lit = c == 1u && !is_fill(wd);
+            const uint32_t a = max(p, g0), e = min(p + c, g1);
+            for (uint32_t g = a; g < e; ++g) {
+                uint32_t bits = wpattern(wd), set = 0;
+                if (lit) {
+                    const uint32_t hb = 31u - __clz(bits);
+                    if (pass_cmp(raw_value(v0[j], I.vtype), T.lop, T.lo, T.rop, T.hi)) set |= 1u << hb;
+                    bits &= ~(1u << hb);
+                }
+                while (bits) {
+                    uint32_t hb[RCHK], v[RCHK];
+#pragma unroll
+                    for (int q = 0; q < RCHK; ++q) {
+                        hb[q] = bits ? 31u - __clz(bits) : 32u;
+                        if (bits) bits &= ~(1u << hb[q]);
+                    }
+#pragma unroll
+                    for (int q = 0; q < RCHK; ++q)
+                        v[q] = hb[q] < 32u ? __ldg(raw + g * 31u + (30u - hb[q])) : 0u;
+#pragma unroll
+                    for (int q = 0; q < RCHK; ++q)
+                        if (hb[q] < 32u && pass_cmp(raw_value(v[q], I.vtype), T.lop, T.lo, T.rop, T.hi))
+                            set |= 1u << hb[q];
+                }
+                if (set) atomicOr(&S.tmp[rsw(g - g0)], set);
+            }
+        }
+    }
+    // the bitmap's active bits form the group after its whole words
+    const uint32_t Gb = m.groups;
+    if (lane == 0 && m.anb > 0 && Gb >= g0 && Gb < g1) {
+        uint32_t bits = (m.aval & ((1u << m.anb) - 1u)) << (31u - m.anb), set = 0;
+        while (bits) {
+            const uint32_t hb = 31u - __clz(bits);
+            const uint32_t row = Gb * 31u + (30u - hb);
+            if (pass_cmp(col_value(I.values, I.vtype, row), T.lop, T.lo, T.rop, T.hi)) set |= 1u << hb;
+            bits &= ~(1u << hb);
+        }
+        if (set) atomicOr(&S.tmp[rsw(Gb - g0)], set);
     }
 }
 
@@ -317,7 +379,7 @@ __device__ __forceinline__ void lanes_or_bitmaps(RangeShared& S, const DevIndex&
     while (lm) {
         const uint32_t src = __ffs(lm) - 1u;
         lm &= lm - 1u;
-        warp_or_bitmap(S, I, __shfl_sync(0xffffffffu, b, src), k, g0, g1, G, anb, nullptr);
+        warp_or_bitmap(S, I, __shfl_sync(0xffffffffu, b, src), k, g0, g1, G, anb);
     }
 }
 
@@ -462,7 +524,7 @@ __global__ void __launch_bounds__(RTHREADS, 6) k_range(RangeArgs A) {
             // bitmaps to OR in batches of up to 32 per warp (one per lane),
             // spread over the warps from the one after the checks, so the
             // warps holding a check get an OR batch last
-            for (uint32_t c = warp; c < nc; c += RWARPS) warp_or_bitmap(S, I, T.cand[c], k, g0, g1, G, anb, &T);
+            for (uint32_t c = warp; c < nc; c += RWARPS) warp_check_bitmap(S, I, T.cand[c], k, g0, g1, T);
             const uint32_t nfree = RWARPS - min(nc, (uint32_t)RWARPS - 1u);  // warps without a check
             const uint32_t per = min(32u, (nsel + nfree - 1) / nfree);
             const uint32_t wr = (warp + RWARPS - nc % RWARPS) % RWARPS;      // the warp's place in the OR order
@@ -485,7 +547,7 @@ __global__ void __launch_bounds__(RTHREADS, 6) k_range(RangeArgs A) {
                 __syncthreads();
                 // edge bitmaps: rows checked against the raw values
                 for (uint32_t c = warp; c < T.ncand; c += RWARPS)
-                    warp_or_bitmap(S, I, T.cand[c], k, g0, g1, G, anb, &T);
+                    warp_check_bitmap(S, I, T.cand[c], k, g0, g1, T);
             }
             __syncthreads();
             uint32_t any = 0;

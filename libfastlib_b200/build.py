@@ -28,20 +28,34 @@ def _stale(target, deps):
     return any(os.path.getmtime(p) > t for p in deps)
 
 
+UNITS = ["wah_api", "wah_index", "wah_build", "wah_server", "wah_noalloc", "wah_idxfile"]
+
+
 def build_lib(force: bool = False, verbose: bool = False) -> str:
+    """Compiles the translation units in parallel (one nvcc each, objects
+    under _build/) and links them into libwahgpu.so."""
+    from concurrent.futures import ThreadPoolExecutor
     out = os.path.join(HERE, "libwahgpu.so")
     deps = _sources() + [os.path.join(ROOT, "include", "wahgpu.h")]
     if not force and not _stale(out, deps):
         return out
-    cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-O3",
-           "-shared", "-I" + os.path.join(ROOT, "include"),
-           "-o", out, os.path.join(HERE, "csrc", "wah_api.cu"),
-           os.path.join(HERE, "csrc", "wah_index.cu"), os.path.join(HERE, "csrc", "wah_build.cu"),
-           os.path.join(HERE, "csrc", "wah_server.cu"),
-           os.path.join(HERE, "csrc", "wah_noalloc.cu"), os.path.join(HERE, "csrc", "wah_idxfile.cu")]
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    flags = ["-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-O3",
+             "-I" + os.path.join(ROOT, "include")]
+    cmds = [[NVCC, *flags, "-c", "-o", os.path.join(objdir, u + ".o"), os.path.join(HERE, "csrc", u + ".cu")]
+            for u in UNITS]
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        for c in cmds:
+            print(" ".join(c))
+    with ThreadPoolExecutor(len(cmds)) as ex:
+        for r in list(ex.map(lambda c: subprocess.run(c), cmds)):
+            if r.returncode:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
+    link = [NVCC, *ARCH, "-shared", "-o", out, *[os.path.join(objdir, u + ".o") for u in UNITS]]
+    if verbose:
+        print(" ".join(link))
+    subprocess.run(link, check=True)
     return out
 
 

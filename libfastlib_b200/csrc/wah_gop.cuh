@@ -302,6 +302,14 @@ __global__ void __launch_bounds__(GTHREADS) k_gpack(GopArgs A) {
     const uint32_t T = A.ntiles;
     if (t >= T) return;
     const uint32_t G = A.groups;
+    // the tile's result patterns and head masks, loaded first so their
+    // round trip overlaps the prefix and next-head loads below
+    const uint32_t g0 = t * (uint32_t)GT;
+    const uint4* R4 = reinterpret_cast<const uint4*>(A.R + g0);
+    const uint32_t hm = A.hmask[(size_t)t * 32u + lane];
+    uint4 rqs[NCH];
+#pragma unroll
+    for (int j = 0; j < NCH; ++j) rqs[j] = R4[32 * j + lane];
     const uint32_t sg = t / GSEG, nseg = (T + GSEG - 1) / GSEG;
     uint32_t off = 0;
     for (uint32_t i = lane; i < sg; i += 32) off += A.segs[i].x;
@@ -343,10 +351,7 @@ __global__ void __launch_bounds__(GTHREADS) k_gpack(GopArgs A) {
         if (f) nxt = GNONE - f;
     }
     if (nxt == GNONE) nxt = G;
-    const uint32_t g0 = t * (uint32_t)GT;
-    const uint4* R4 = reinterpret_cast<const uint4*>(A.R + g0);
-    // the lane's heads as k_gop found them: bit 4 j + e for group 128 j + 4 lane + e
-    const uint32_t hm = A.hmask[(size_t)t * 32u + lane];
+    // hm: the lane's heads as k_gop found them (bit 4 j + e for group 128 j + 4 lane + e)
     uint32_t* so = sout[warp];
     const uint32_t oal = off & ~3u;
     const uint32_t gt = (2u << lane) - 1u;  // lanes up to this one (lane 31: all)
@@ -376,7 +381,7 @@ __global__ void __launch_bounds__(GTHREADS) k_gpack(GopArgs A) {
         const uint32_t after = above ? nl : later;
         later = __shfl_sync(0xffffffffu, mine, __ffs(hl) - 1u);
         if (m) {
-            const uint4 rq = R4[32 * j + lane];
+            const uint4 rq = rqs[j];
             const uint32_t r[4] = {rq.x, rq.y, rq.z, rq.w};
 #pragma unroll
             for (int e = 0; e < 4; ++e)

@@ -154,14 +154,16 @@ struct TileShared {
     uint32_t warp_agg[MERGE_THREADS / 32][4];
     uint32_t tile_prefix[4];
     uint32_t hdr[16];  // tile geometry broadcast
+    // seg_transfer for every (step, xb, yb, fits_x, fits_y): entry
+    // 16 * step + 8 xb + 4 yb + 2 fits_x + fits_y
+    uint32_t trans_tab[80];
 };
 
-// Loads words [g0, g1) of an operand into shared memory and computes the end
-// position of each word from the block positions.  g0 is a multiple of 32.
-__device__ __forceinline__ void load_range(const uint32_t* __restrict__ w, const uint32_t* __restrict__ bp,
-                                           uint32_t g0, uint32_t g1, uint32_t* sw, uint32_t* se) {
+// Starts copying words [g0, g1) of an operand into shared memory (128-bit
+// loads: g0 is 32-word aligned, buffers are 256-byte aligned).  The caller
+// waits with a block barrier before reading sw.
+__device__ __forceinline__ void load_words(const uint32_t* __restrict__ w, uint32_t g0, uint32_t g1, uint32_t* sw) {
     const uint32_t n = g1 - g0;
-    // words: 128-bit loads (g0 is 32-word aligned, buffers are 256-byte aligned)
     const uint32_t n4 = n / 4u;
     const uint4* w4 = reinterpret_cast<const uint4*>(w + g0);
     for (uint32_t i = threadIdx.x; i < n4; i += MERGE_THREADS) {
@@ -169,11 +171,20 @@ __device__ __forceinline__ void load_range(const uint32_t* __restrict__ w, const
         reinterpret_cast<uint4*>(sw)[i] = v;
     }
     for (uint32_t i = n4 * 4u + threadIdx.x; i < n; i += MERGE_THREADS) sw[i] = __ldg(w + g0 + i);
-    __syncthreads();
-    // end positions: one warp per 32-word block, inclusive scan of counts
+}
+
+// End position of each staged word from the block positions: one warp per
+// 32-word block, inclusive scan of the group counts.  bpv[r] holds the
+// block position of block warp + r * (MERGE_THREADS / 32), loaded before the
+// barrier that made sw readable (so its latency overlaps the word loads).
+template <int NR>
+__device__ __forceinline__ void word_ends(const uint32_t* sw, uint32_t* se, uint32_t n, const uint32_t (&bpv)[NR]) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t nblk = (n + 31u) / 32u;
-    for (uint32_t b = warp; b < nblk; b += MERGE_THREADS / 32) {
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        const uint32_t b = warp + (uint32_t)r * (MERGE_THREADS / 32);
+        if (b >= nblk) break;
         const uint32_t i = b * 32u + lane;
         uint32_t c = i < n ? wgroups(sw[i]) : 0u;
 #pragma unroll
@@ -181,7 +192,18 @@ __device__ __forceinline__ void load_range(const uint32_t* __restrict__ w, const
             uint32_t t = __shfl_up_sync(0xffffffffu, c, d);
             if (lane >= (uint32_t)d) c += t;
         }
-        if (i < n) se[i] = __ldg(bp + (g0 / 32u) + b) + c;
+        if (i < n) se[i] = bpv[r] + c;
+    }
+}
+// Block positions for word_ends (lane values; every lane loads the same entry).
+template <int NR>
+__device__ __forceinline__ void load_bpos(const uint32_t* __restrict__ bp, uint32_t g0, uint32_t n, uint32_t (&bpv)[NR]) {
+    const uint32_t warp = threadIdx.x >> 5;
+    const uint32_t nblk = (n + 31u) / 32u;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        const uint32_t b = warp + (uint32_t)r * (MERGE_THREADS / 32);
+        bpv[r] = b < nblk ? __ldg(bp + (g0 / 32u) + b) : 0u;
     }
 }
 
@@ -205,10 +227,14 @@ __global__ void __launch_bounds__(MERGE_THREADS, 2) k_merge(MergeArgs A) {
     TileShared& S = *reinterpret_cast<TileShared*>(smem_raw);
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
 
-    // ---- claim a tile and the launch epoch
-    if (tid == 0) {
-        S.hdr[0] = claim_tile(A.sync);
-        S.hdr[1] = ld_cg(&A.sync->epoch);
+    // ---- claim a tile and read the launch epoch (two threads, so the two
+    // round trips overlap; the epoch only changes after the last CTA of the
+    // previous launch on this stream finished)
+    if (tid == 0) S.hdr[0] = claim_tile(A.sync);
+    if (tid == 32) S.hdr[1] = ld_cg(&A.sync->epoch);
+    if (FSM && tid >= 64 && tid < 64 + 80) {
+        const uint32_t e = tid - 64;
+        S.trans_tab[e] = seg_transfer(e >> 4, (e >> 3) & 1u, (e >> 2) & 1u, (e >> 1) & 1u, e & 1u);
     }
     __syncthreads();
     const uint32_t t = S.hdr[0];
@@ -260,8 +286,16 @@ __global__ void __launch_bounds__(MERGE_THREADS, 2) k_merge(MergeArgs A) {
         if (gy0 > A.ny) gy0 = gy1 = A.ny;
     }
     const uint32_t hx = gx1 - gx0, hy = gy1 - gy0;
-    if (hx) load_range(A.xw, A.xbp, gx0, gx1, S.wx, S.ex);
-    if (!UNARY && hy) load_range(A.yw, A.ybp, gy0, gy1, S.wy, S.ey);
+    // both operands' words and block positions in flight together
+    constexpr int NR = (TILE_BLOCKS + 2 + MERGE_THREADS / 32 - 1) / (MERGE_THREADS / 32);
+    uint32_t bpx[NR], bpy[NR];
+    load_words(A.xw, gx0, gx1, S.wx);
+    if (!UNARY) load_words(A.yw, gy0, gy1, S.wy);
+    load_bpos(A.xbp, gx0, hx, bpx);
+    if (!UNARY) load_bpos(A.ybp, gy0, hy, bpy);
+    __syncthreads();
+    word_ends(S.wx, S.ex, hx, bpx);
+    if (!UNARY) word_ends(S.wy, S.ey, hy, bpy);
     __syncthreads();
 
     // ---- events of this tile: word ends in (Pa, Pb]; four threads search
@@ -354,7 +388,8 @@ __global__ void __launch_bounds__(MERGE_THREADS, 2) k_merge(MergeArgs A) {
                         const uint32_t xe2 = xendk(kx), ye2 = yendk(ky);
                         const bool xb = (pos == xstart(kx)), yb = (pos == ystart(ky));
                         const uint32_t sel = select_step(OP, xw_, xe2 - pos, yw_, ye2 - pos);
-                        trans = seg_transfer(sel, xb, yb, xe2 <= ye2, ye2 <= xe2);
+                        trans = S.trans_tab[16u * sel + (xb ? 8u : 0u) + (yb ? 4u : 0u) +
+                                            (xe2 <= ye2 ? 2u : 0u) + (ye2 <= xe2 ? 1u : 0u)];
                     }
                     const uint32_t len = segend - pos;
                     agg.popc += (cls == C_MIXED) ? __popc(val) : (cls == C_ONE ? len * 31u : 0u);

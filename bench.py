@@ -9,9 +9,11 @@ pairs in turn, so each operand is evicted between its uses.
 
 Metric: WAH-op bandwidth in GB/s, counting 4 bytes per serialized word of
 both operands and of the result (the algorithmic bytes).  `value` is device
-time with operands resident in HBM; `e2e` goes through the C ABI with host
-buffers (pinned), each call uploading its operands and reading back the
-result words and cnt().
+time with operands resident in HBM, the step's independent calls spread over
+--streams contexts (a stream each) and replayed as one graph; `e2e` goes
+through the C ABI with host buffers (pinned), each call uploading its
+operands and reading back the result words and cnt(), the calls shared by
+--e2e-threads host threads with a context each.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -262,6 +264,8 @@ def main():
     ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--streams", type=int, default=4,
+                    help="contexts (one stream each) the device-timed step's independent calls are spread over")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--e2e-threads", type=int, default=4,
                     help="host threads (one context each) sharing the end-to-end leg's calls")
@@ -355,31 +359,85 @@ def main():
             dense_tuning = {"chosen": {"engine": best[0], "tile_groups": best[1]},
                             "candidates_ms_per_step": {f"engine {e} tile {t}": round(v, 4) for (e, t), v in table.items()}}
 
+    # The step's calls are independent of one another, so they are spread
+    # over --streams contexts (a stream and look-back scratch each; every
+    # context holds its own copies of the operands it works on), as a caller
+    # with several streams would issue them: the calls sorted by operand
+    # size and dealt round-robin, so every stream gets a share of the dense,
+    # medium and small calls and the small calls' latency overlaps the
+    # others' work.  The step is captured as one graph that forks from the
+    # timing stream to the contexts' streams and joins back.
+    nstreams = max(1, min(args.streams, len(OPS) * len(dev)))
+    order = sorted(((op, i) for op in OPS for i in range(len(dev))),
+                   key=lambda c: -(dev[c[1]][0].nwords() + dev[c[1]][1].nwords()))
+    lanes = []  # (context, stream, calls, operands, results)
+    for k in range(nstreams):
+        calls_k = order[k::nstreams]
+        if k == 0:
+            lanes.append((ctx, stream, calls_k, dev, {(op, i): res[i][op] for op, i in calls_k}))
+            continue
+        c = L.Context(local)
+        for key in (L.TUNE_DENSE_TILE, L.TUNE_DENSE_ENGINE, L.TUNE_MERGE_TILE):
+            c.set_tuning(key, ctx.get_tuning(key))
+        s_k = torch.cuda.Stream()
+        c.set_stream(s_k.cuda_stream)
+        dv = {}
+        for _, i in calls_k:
+            if i not in dv:
+                dv[i] = (c.bitvector(pairs[i][0]), c.bitvector(pairs[i][1]))
+                dv[i][0].size(); dv[i][1].size()
+        rs = {(op, i): c.empty(len(pairs[i][0]) + len(pairs[i][1])) for op, i in calls_k}
+        lanes.append((c, s_k, calls_k, dv, rs))
+
+    def step_streams():
+        if nstreams == 1:
+            step()
+            return
+        fork = torch.cuda.Event()
+        fork.record(stream)
+        for _c, s_k, _k, _d, _r in lanes[1:]:
+            s_k.wait_event(fork)
+        for _c, _s, calls_k, dv, rs in lanes:
+            for op, i in calls_k:
+                dv[i][0].binop_into(op, dv[i][1], rs[(op, i)])
+        for _c, s_k, _k, _d, _r in lanes[1:]:
+            j = torch.cuda.Event()
+            j.record(s_k)
+            stream.wait_event(j)
+
+    def all_launches():
+        return sum(l[0].launches for l in lanes)
+
     clk = ClockSampler(local)
     if not args.only:
         clk.start()
         time.sleep(1.0)  # nvidia-smi needs a moment before its first sample
-    l_step0 = ctx.launches
-    step()
-    launches_per_step = ctx.launches - l_step0
+    step_streams()  # first use: one-time per-operand indexes on each context
+    l_step0 = all_launches()
+    step_streams()
+    launches_per_step = all_launches() - l_step0
     for _ in range(args.warmup):
-        step()
+        step_streams()
     torch.cuda.synchronize()
-    res_lens = [res[i][op].nwords() + 1 + (1 if (NBITS % 31) else 0) for op in OPS for i in range(len(dev))]
+    result_of = {}
+    for _c, _s, calls_k, _d, rs in lanes:
+        for key in calls_k:
+            result_of[key] = rs[key]
+    res_lens = [result_of[(op, i)].nwords() + 1 + (1 if (NBITS % 31) else 0) for op in OPS for i in range(len(dev))]
     nbytes = algorithmic_bytes(pairs, res_lens)
 
     # the step as one CUDA graph (the library enqueues without host syncs once
     # operand metadata is known and scratch is sized)
     graph = torch.cuda.CUDAGraph()
     with torch.cuda.graph(graph, stream=stream):
-        step()
+        step_streams()
     for _ in range(args.warmup):
         graph.replay()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    l0 = ctx.launches
+    l0 = all_launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
@@ -387,7 +445,7 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     # kernels per step were counted while capturing; replays launch the same set
-    launches = (ctx.launches - l0) + args.steps * launches_per_step
+    launches = (all_launches() - l0) + args.steps * launches_per_step
     clocks = clk.stop()
     ms = max_over_ranks(e0.elapsed_time(e1), f"cuda:{local}")
     if world > 1:
@@ -550,6 +608,9 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": _config(world),
+            "device_streams": {"streams": nstreams,
+                               "how": "the step's independent calls dealt round-robin by operand size over "
+                                      "contexts with a stream each, one graph forking and joining them"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if achieved else None, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": engine_kernels + " (+ the metadata memset), per-call CUDA events over the "

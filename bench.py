@@ -167,11 +167,12 @@ def algorithmic_bytes(pairs, res_lens):
     return tot
 
 
-def copy_only_bound(pinned, h2d: int, d2h: int, nbytes: int, device: int, reps: int = 3) -> dict:
+def copy_only_bound(pinned, uploads, h2d: int, d2h: int, nbytes: int, device: int, reps: int = 3) -> dict:
     """The end-to-end rate the step's host<->device copies alone allow: the
-    step's operand words uploaded from pinned host memory on one stream while
-    a buffer of its result bytes comes back on another (no kernels), timed
-    with CUDA events; value = the step's algorithmic bytes / that time."""
+    operand pairs the step uploads (pair indices `uploads`, from pinned host
+    memory) on one stream while a buffer of its result bytes comes back on
+    another (no kernels), timed with CUDA events; value = the step's
+    algorithmic bytes / that time."""
     import torch
     dev = f"cuda:{device}"
     up, down = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
@@ -188,10 +189,10 @@ def copy_only_bound(pinned, h2d: int, d2h: int, nbytes: int, device: int, reps: 
         up.wait_event(e0)
         down.wait_event(e0)
         with torch.cuda.stream(up):
-            for _op in OPS:  # the step uploads each pair once per operator
-                for (_, _, ta, tb), (da, db) in zip(pinned, dst):
-                    da.copy_(ta.view(torch.int32), non_blocking=True)
-                    db.copy_(tb.view(torch.int32), non_blocking=True)
+            for i in uploads:
+                _, _, ta, tb = pinned[i]
+                dst[i][0].copy_(ta.view(torch.int32), non_blocking=True)
+                dst[i][1].copy_(tb.view(torch.int32), non_blocking=True)
             e1.record(up)
         with torch.cuda.stream(down):
             back.copy_(back_dev, non_blocking=True)
@@ -201,7 +202,7 @@ def copy_only_bound(pinned, h2d: int, d2h: int, nbytes: int, device: int, reps: 
         best = ms if best is None else min(best, ms)
     return {"value": nbytes / (best * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": best,
             "h2d_bytes": h2d, "d2h_bytes": d2h,
-            "how": "uploads of every call's operands and one readback of the step's result bytes, "
+            "how": "the step's operand uploads and one readback of its result bytes, "
                    "on two streams, no kernels (best of 3, CUDA events)"}
 
 
@@ -451,6 +452,13 @@ def main():
     if world > 1:
         dist.barrier()
     value = whole_job_rate(nbytes, args.steps, ms, world)
+    # the extra contexts of the step and their operand copies are released
+    # here, so the legs below run with the device as they would alone
+    graph.reset()
+    for lane in lanes[1:]:
+        lane[0].close()
+    lanes = lanes[:1]
+    torch.cuda.synchronize()
     if args.only:
         if rank == 0:
             print(json.dumps({"only": args.only, "value": value, "unit": "GB/s", "ms_per_call": ms / args.steps,
@@ -512,10 +520,16 @@ def main():
         except Exception:
             traffic = None
 
-    # end to end through the C ABI with host (pinned) buffers: the step's
-    # calls are shared by E2E_THREADS host threads, each with its own
-    # context (stream), as a multi-threaded caller would use the library, so
-    # one call's upload overlaps another's readback and kernels
+    # end to end through the C ABI with host (pinned) buffers: every step
+    # uploads the step's operand pairs from pinned host memory, runs the four
+    # operators on each pair's device copies (as a caller holding
+    # ibis::bitvector objects applies several operators to them) and reads
+    # every result's words and cnt() back.  The work is shared by
+    # E2E_THREADS host threads, each with its own context (stream), so one
+    # upload overlaps another's readback and kernels: a unit is a pair and
+    # the operators run on it (the two largest pairs' operators split over
+    # two units, each uploading the pair), units dealt largest first to the
+    # least-loaded thread.
     import ctypes
     pinned = []
     for a, b in pairs:
@@ -526,24 +540,42 @@ def main():
     for c in ectx[1:]:  # the launch shapes the device-side leg ran with (tuned or given)
         for key in (L.TUNE_DENSE_TILE, L.TUNE_DENSE_ENGINE, L.TUNE_MERGE_TILE):
             c.set_tuning(key, ctx.get_tuning(key))
-    outbufs = [[torch.empty(len(a) + len(b) + 4, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
-                for a, b in pairs] for _ in ectx]
-    calls = [(op, i) for op in OPS for i in range(len(pinned))]
+    sizes = [len(a) + len(b) for a, b in pairs]
+    big = sorted(range(len(pairs)), key=lambda i: -sizes[i])[:2]
+    units = []
+    for i in range(len(pairs)):
+        if i in big and len(OPS) > 1:
+            h = len(OPS) // 2
+            units += [(i, OPS[:h]), (i, OPS[h:])]
+        else:
+            units.append((i, list(OPS)))
+    cost = lambda u: sizes[u[0]] * (1 + len(u[1]) / 2)  # upload + results (about half an operand each)
+    load = [0.0] * len(ectx)
+    assign = [[] for _ in ectx]
+    for u in sorted(units, key=lambda u: -cost(u)):
+        k = min(range(len(ectx)), key=lambda j: load[j])
+        assign[k].append(u)
+        load[k] += cost(u)
+    outbufs = [{(i, op): torch.empty(sizes[i] + 4, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+                for i, ops in assign[k] for op in ops} for k in range(len(ectx))]
 
     def e2e_calls(k, out):
         c, h2d, d2h = ectx[k], 0, 0
         try:
-            for op, i in calls[k::len(ectx)]:
+            for i, ops in assign[k]:
                 a, b = pinned[i][0], pinned[i][1]
                 A = c.bitvector(a)
                 B = c.bitvector(b)
-                R = A._binop(op, B, False)
-                buf = outbufs[k][i]
-                n = c.check(c.lib.wahgpu_bv_write(R.h, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), len(buf)))
-                R.cnt()
                 h2d += 4 * (len(a) + len(b))
-                d2h += 4 * n
-                del A, B, R
+                for op in ops:
+                    R = A._binop(op, B, False)
+                    buf = outbufs[k][(i, op)]
+                    n = c.check(c.lib.wahgpu_bv_write(R.h, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                                      len(buf)))
+                    R.cnt()
+                    d2h += 4 * n
+                    del R
+                del A, B
             out[k] = (h2d, d2h)
         except BaseException as e:  # surfaced by the caller
             out[k] = e
@@ -573,7 +605,11 @@ def main():
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(max(q0.elapsed_time(q1), (time.perf_counter() - t0) * 1e3), f"cuda:{local}")
     e2e_value = whole_job_rate(nbytes, args.e2e_steps, e2e_ms, world)
-    copy_bound = copy_only_bound(pinned, h2d, d2h, nbytes, local)
+    copy_bound = copy_only_bound(pinned, [u[0] for a_k in assign for u in a_k], h2d, d2h, nbytes, local)
+    for c in ectx[1:]:  # the end-to-end leg's extra contexts, released before the legs below
+        c.close()
+    del pinned, outbufs
+    torch.cuda.synchronize()
 
     cpu = None
     if rank == 0 and world == 1:

@@ -502,7 +502,7 @@ public:
 
 /* ibis::countQuery over named columns.  A WHERE clause combines range
  * conditions — "a >= 3", "2.5 <= b < 7", "c between 1 and 4", "d = 5",
- * "d != 5", "e in (1, 4, 9)" (a qDiscreteRange, as an OR of equalities) —
+ * "d != 5", "e in (1, 4, 9)" or "e in (1 4 9)" (a qDiscreteRange, as an OR of equalities) —
  * with AND, OR, NOT (also &&, ||, !) and parentheses, as
  * countQuery::doEvaluate does with its LOGICAL_AND / OR / NOT nodes over
  * qContinuousRange leaves (src/countQuery.cpp:929-1036): an AND of ranges
@@ -655,7 +655,8 @@ private:
         const auto& T = toks_;
         if (i >= T.size()) throw error(WAHGPU_EINVAL, "missing condition");
         if (!nums_[i] && i + 2 < T.size() && lower(T[i + 1]) == "in" && T[i + 2] == "(") {
-            // x in (v1, v2, ...): qDiscreteRange as an OR of equalities
+            // x in (v1, v2, ...) or x in (v1 v2 ...): qDiscreteRange as an
+            // OR of equalities
             const index* c = column(T[i]);
             std::vector<int> kids;
             size_t k = i + 3;
@@ -663,6 +664,7 @@ private:
                 if (k >= T.size() || !nums_[k]) throw error(WAHGPU_EINVAL, "bad IN list");
                 kids.push_back(leaf(c, WAHGPU_CMP_LE, vals_[k], WAHGPU_CMP_LE, vals_[k]));
                 if (k + 1 < T.size() && T[k + 1] == ",") { k += 2; continue; }
+                if (k + 1 < T.size() && nums_[k + 1]) { k += 1; continue; }
                 if (k + 1 < T.size() && T[k + 1] == ")") break;
                 throw error(WAHGPU_EINVAL, "bad IN list");
             }

@@ -108,7 +108,8 @@ class _Parser:
 
         if (kind(i) == "name" and kind(i + 1) == "name" and str(val(i + 1)).lower() == "in"
                 and kind(i + 2) == "op" and val(i + 2) == "("):
-            # x in (v1, v2, ...): qDiscreteRange as an OR of equalities
+            # x in (v1, v2, ...) or x in (v1 v2 ...): qDiscreteRange as an
+            # OR of equalities
             idx, k, vals = self._col(val(i)), i + 3, []
             while True:
                 if kind(k) != "num":
@@ -116,6 +117,9 @@ class _Parser:
                 vals.append(val(k))
                 if kind(k + 1) == "op" and val(k + 1) == ",":
                     k += 2
+                    continue
+                if kind(k + 1) == "num":
+                    k += 1
                     continue
                 if kind(k + 1) == "op" and val(k + 1) == ")":
                     break

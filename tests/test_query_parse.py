@@ -36,6 +36,8 @@ def leaf(*t):
     ("b in (2) and not a in (1, 2)",
      ("and", [leaf("b", CMP_LE, 2.0, CMP_LE, 2.0),
               ("not", ("or", [leaf("a", CMP_LE, 1.0, CMP_LE, 1.0), leaf("a", CMP_LE, 2.0, CMP_LE, 2.0)]))])),
+    # the reference's own test queries write IN lists without commas
+    ("a in (1 2)", ("or", [leaf("a", CMP_LE, 1.0, CMP_LE, 1.0), leaf("a", CMP_LE, 2.0, CMP_LE, 2.0)])),
     ("!(a >= 3) || (b < 1 && a > 2)",
      ("or", [("not", leaf("a", CMP_LE, 3.0, CMP_NONE, None)),
              ("and", [leaf("b", CMP_NONE, None, CMP_LT, 1.0), leaf("a", CMP_LT, 2.0, CMP_NONE, None)])])),
@@ -45,7 +47,7 @@ def test_trees(clause, tree):
 
 
 @pytest.mark.parametrize("clause", ["c < 3", "a < 5 or", "(a < 3", "a between 1 4", "a <", "a < 3 b < 4", "a @ 3",
-                                    "a in (1, 2", "a in ()", "a in (1 2)"])
+                                    "a in (1, 2", "a in ()", "a in (1 2", "a in (1 , , 2)"])
 def test_refused(clause):
     with pytest.raises(QueryError):
         parse(clause, COLS)

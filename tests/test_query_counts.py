@@ -25,7 +25,7 @@ FIXTURE = os.path.join(HERE, "golden", "query_counts.json")
 # Strict lower bounds below zero: the reference's count leaves out the row
 # whose value is 0 (98 of the 99 values 0..98 in each case); a
 # qContinuousRange "-3 < x < 99" holds for 0, and so does every evaluation
-# here.  Recorded as a deviation of the reference's WHERE parser, not
+# here.  Where the reference loses that row was not traced; it is not
 # reproduced.
 REFERENCE_DROPS_ZERO = {"-3 < i0 < 99", "-4 < i1 < 99", "-5 < i2 < 99"}
 

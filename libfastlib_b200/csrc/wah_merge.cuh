@@ -288,6 +288,10 @@ __global__ void __launch_bounds__(MERGE_THREADS, 2) k_merge(MergeArgs A) {
     const uint32_t hx = gx1 - gx0, hy = gy1 - gy0;
     // both operands' words and block positions in flight together
     constexpr int NR = (TILE_BLOCKS + 2 + MERGE_THREADS / 32 - 1) / (MERGE_THREADS / 32);
+    // a tile holds at most TILE_BLOCKS + 1 blocks of an operand (the merge
+    // path's TILE_BLOCKS entries and the block holding Pa); NR rows of warps
+    // cover them
+    static_assert(NR * (MERGE_THREADS / 32) >= TILE_BLOCKS + 2, "block-position registers");
     uint32_t bpx[NR], bpy[NR];
     load_words(A.xw, gx0, gx1, S.wx);
     if (!UNARY) load_words(A.yw, gy0, gy1, S.wy);

@@ -11,9 +11,10 @@ Metric: WAH-op bandwidth in GB/s, counting 4 bytes per serialized word of
 both operands and of the result (the algorithmic bytes).  `value` is device
 time with operands resident in HBM, the step's independent calls spread over
 --streams contexts (a stream each) and replayed as one graph; `e2e` goes
-through the C ABI with host buffers (pinned), each call uploading its
-operands and reading back the result words and cnt(), the calls shared by
---e2e-threads host threads with a context each.
+through the C ABI with host buffers (pinned): every step uploads the operand
+pairs, runs the four operators on each pair's device copies and reads back
+every result's words and cnt(), the work shared by --e2e-threads host
+threads with a context each.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 

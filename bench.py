@@ -626,6 +626,11 @@ def main():
             secs, lens = cpu_port(host, 1)
             cpu = {"value": algorithmic_bytes(host, lens) / secs / 1e9, "unit": "GB/s", "cores": 1,
                    "kind": "port", "sample": "1 pass of the 20 operator calls (C oracle)"}
+        # the device results' serialized lengths against the CPU leg's, call
+        # by call (both in operator-major order)
+        same = [int(x) for x in lens] == [int(x) for x in res_lens]
+        cpu["result_lengths_equal"] = same
+        assert same, "serialized result lengths differ from the CPU leg's"
 
     extra = {}
     which = (args.workloads.split(",") if args.workloads is not None

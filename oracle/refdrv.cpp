@@ -518,6 +518,29 @@ int main(int argc, char** argv) {
                 fastbit_iapi_free_all();
             }
             wr32(ierr < 0 ? 1u : 0u);
+        } else if (kind == 14) {
+            // relic::construct over uint32 values, then per query
+            // relic::evaluate of  lo lop x rop hi  (0: no bound, 1: <, 2: <=)
+            // (src/irelic.cpp:879, 1827; qContinuousRange src/qExpr.h:259-280):
+            // the count and the row ids
+            const uint32_t nrows = rd32();
+            ibis::array_t<uint32_t> vals(nrows);
+            for (uint32_t i = 0; i < nrows; ++i) vals[i] = rd32();
+            ibis::relic rel(0);
+            rel.construct(vals);
+            const ibis::qExpr::COMPARE cmp[3] = {ibis::qExpr::OP_UNDEFINED, ibis::qExpr::OP_LT, ibis::qExpr::OP_LE};
+            const uint32_t nq = rd32();
+            for (uint32_t q = 0; q < nq; ++q) {
+                const double lo = rdf64(), hi = rdf64();
+                const uint32_t lop = rd32(), rop = rd32();
+                if (lop > 2 || rop > 2) exit(3);
+                ibis::qContinuousRange expr(lo, cmp[lop], "x", cmp[rop], hi);
+                ibis::bitvector hits;
+                const long c = rel.evaluate(expr, hits);
+                std::vector<uint32_t> rids;
+                if (c > 0) rids_of(hits, rids);
+                wr32(c < 0 ? 1u : 0u); wr32(c < 0 ? 0u : (uint32_t)c); wrv(rids);
+            }
         } else {
             fprintf(stderr, "refdrv: unknown request %u\n", kind);
             return 4;

@@ -124,6 +124,26 @@ def relic_triple(values):
     return _triple(d, 0)[0]
 
 
+def relic_compare(values, queries):
+    """Request 14: relic::construct over uint32 values, then per query
+    (lo, lop, hi, rop) -- lo lop x rop hi with 0 = no bound, 1 = <, 2 = <= --
+    relic::evaluate's count and row ids.  Returns [(count, rids), ...]."""
+    v = np.ascontiguousarray(values, np.uint32)
+    req = [struct.pack("<II", 14, len(v)), v.tobytes(), struct.pack("<I", len(queries))]
+    for lo, lop, hi, rop in queries:
+        req.append(struct.pack("<ddII", float(lo), float(hi), int(lop), int(rop)))
+    d = _run(b"".join(req))
+    res, p = [], 0
+    for _ in range(len(queries)):
+        st, c, n = struct.unpack_from("<III", d, p)
+        p += 12
+        if st:
+            raise RuntimeError("relic::evaluate failed")
+        res.append((c, np.frombuffer(d, np.uint32, n, p).copy()))
+        p += 4 * n
+    return res
+
+
 def bin_index(values, nbins: int, queries=()):
     """Request 9: the reference's own bin index
     (fastbit_iapi_build_index "<binning nbins=N equal_weight/>" then

@@ -1,6 +1,6 @@
 """The reference driver's query requests (oracle/reference.py), on the CPU:
 the in-memory C API on attached index triples (request 12), relic
-evaluation (request 13) and the appendFill-built operator pairs
+evaluation (requests 13 and 14) and the appendFill-built operator pairs
 (request 11) give the answers of a double-precision scan or of the C
 oracle, with one thread and with several.  These requests time the
 reference in bench.py and pin the GPU's answers at full size, so they are
@@ -57,6 +57,35 @@ def test_relic_timed_counts():
         secs, counts = R.relic_timed(v, qs, nthreads=nth, reps=2)
         assert secs > 0
         assert counts == [int(np.sum((v >= lo) & (v < hi))) for lo, hi in qs]
+
+
+def test_relic_every_comparison_pair_equals_the_scan():
+    """Request 14: the reference's relic::evaluate for every operator pair
+    the GPU tests use (x < b, a < x <= b, a <= x, a <= x <= b, a < x < b),
+    with bounds below, inside and above the values, whole and halfway
+    between keys, negative strict lower bounds among them, gives exactly
+    the double-precision scan that the GPU's range results are compared
+    with (count and row ids)."""
+    rng = np.random.default_rng(14)
+    n = 50_003
+    v = rng.integers(0, 500, size=n).astype(np.uint32)
+    v[:10] = 0  # the value 0 is present, for the negative strict bounds
+    f = v.astype(np.float64)
+    pairs = [(0, 1), (1, 2), (2, 0), (2, 2), (1, 1)]
+    qs = [(-3.0, 1, 99.0, 1), (-0.5, 1, 0.5, 2), (0.0, 1, 10.0, 1), (-5.0, 2, 0.0, 2)]
+    for k in range(80):
+        lo, hi = sorted(rng.integers(-5, 505, 2).astype(float) + rng.choice([0.0, 0.5]))
+        lop, rop = pairs[k % len(pairs)]
+        qs.append((lo, lop, hi, rop))
+    got = R.relic_compare(v, qs)
+    for (lo, lop, hi, rop), (cnt, rids) in zip(qs, got):
+        m = np.ones(n, bool)
+        if lop == 1: m &= lo < f
+        if lop == 2: m &= lo <= f
+        if rop == 1: m &= f < hi
+        if rop == 2: m &= f <= hi
+        assert cnt == int(m.sum()), (lo, lop, hi, rop)
+        assert np.array_equal(rids, np.flatnonzero(m).astype(np.uint32)), (lo, lop, hi, rop)
 
 
 @pytest.mark.parametrize("density", [1e-3, 0.1, 0.5])
